@@ -1,0 +1,359 @@
+"""Throughput of the random-field path on B200: Mpoints/s of one blended field.
+
+Workload (default): a 512^3 deck (re-fitted to 513^3) with exponential
+correlation, anisotropic correlation lengths (40, 20, 10) at spacing 1,
+lognormal marginal (mean 1, CV 0.3), 2x2x2 tiles with overlap 2 l, padded
+periodic generation in FP32 with the FP64 spectral normalisation.  One step
+generates one complete field (8 tiles x 3 passes).  Synthetic: the field is
+drawn from seeded Philox normals; nothing is read from disk.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scarl|reference]
+
+N > 1: one process per GPU (torchrun), independent replicas (the path does
+not shard across GPUs), weak scaling.  --impl reference times the CPU
+restatement of the same path on the host cores (tile sample).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpoints/s per field vs plain GPU path at rel-L2≤1e-5 vs FP64; FFT % HBM roofline"
+
+# the 512^3 deck: xMax 512, corrL (40,20,10), ppcl (41,21,11) -> spacing 1
+DECK = dict(xMinGlob=(0, 0, 0), xMaxGlob=(512, 512, 512), corrL=(40, 20, 10),
+            overlap=(2, 2, 2), pointsPerCorrL=(41, 21, 11), corrMod=3, margiFirst=2,
+            avg=1.0, std_dev=0.3, seedBase=0, nu=0.5)
+TOPO = (2, 2, 2)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+
+    FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id):
+        self.bus = (bus_id or "").lower()
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            with open(self.path) as fh:
+                for line in fh:
+                    f = [x.strip() for x in line.split(",")]
+                    if len(f) < 10:
+                        continue
+                    if self.bus and self.bus[-12:] not in f[1].lower():
+                        continue
+                    rows.append(f)
+            os.unlink(self.path)
+        except Exception:
+            return None
+        if not rows:
+            return None
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[2]) for r in rows if num(r[2]) is not None]
+        mx = [num(r[3]) for r in rows if num(r[3]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[6:10]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def layout_of(S):
+    s = S.make_sample(**DECK)
+    return s, S.sample_layout(s, 1, 8, TOPO)
+
+
+def pass_bytes(lay, dtype_bytes=4):
+    """Algorithmic HBM bytes per launch of each pass, averaged over tiles.
+    Pass 1 writes the z-transformed half spectrum (its input is synthesised in
+    registers); pass 2 reads it and writes the y-pruned rows; pass 3 reads
+    those and writes the tile's points into the field (plus the re-read of
+    points an earlier tile already wrote)."""
+    Np, No, T = [int(v) for v in lay["Np"]], [int(v) for v in lay["Np_ovlp"]], lay["topo"]
+    P = [1 << (2 * n - 1).bit_length() for n in Np]
+    Hx = P[0] // 2 + 1
+    c = 2 * dtype_bytes
+    b1 = Hx * P[1] * Np[2] * c
+    b2 = Hx * P[1] * Np[2] * c + Hx * Np[1] * Np[2] * c
+    # points of a tile that an earlier tile already wrote (read-modify-write)
+    nb = int(T[0] * T[1] * T[2])
+    reread = 0
+    for r in range(nb):
+        pos = [r % T[0], (r // T[0]) % T[1], r // (T[0] * T[1])]
+        own = 1
+        for d in range(3):
+            own *= Np[d] - (No[d] if pos[d] > 0 and No[d] >= 2 else 0)
+        reread += Np[0] * Np[1] * Np[2] - own
+    b3 = Hx * Np[1] * Np[2] * c + Np[0] * Np[1] * Np[2] * dtype_bytes + reread * dtype_bytes // nb
+    return {"k_gen_z": b1, "k_mid_y": b2, "k_c2r_x": b3}, P
+
+
+def cpu_sample(lay, steps, warmup, stride=8):
+    """The oracle (CPU restatement, OpenMP) on every stride-th line of each
+    pass of tile 0: per step, 1/stride of one tile's work."""
+    from oracle import oracle as O
+    Np = [int(v) for v in lay["Np"]]
+    P = [1 << (2 * n - 1).bit_length() for n in Np]
+    dx = [float(v) for v in lay["xStep"]]
+    norm = O.spectrum_sum(DECK["corrMod"], DECK["nu"], P, dx, DECK["corrL"])
+    out = __import__("numpy").zeros(Np, order="F")
+    for _ in range(warmup):
+        O.gen_padded_stream(Np, P, dx, DECK["corrL"], DECK["corrMod"], DECK["nu"], norm, 1, 0,
+                            stride, out)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.gen_padded_stream(Np, P, dx, DECK["corrL"], DECK["corrMod"], DECK["nu"], norm, 1, 0,
+                            stride, out)
+    dt = (time.perf_counter() - t0) / steps
+    nb = int(lay["nb_tiles"])
+    field_points = int(lay["L"][0]) * int(lay["L"][1]) * int(lay["L"][2])
+    # one tile accounts for field_points / nb points; the sample is 1/stride tile
+    mpts = (field_points / nb) / (dt * stride) / 1e6
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": round(mpts, 4), "unit": "Mpoints/s", "cores": cores, "kind": "port",
+            "sample": f"oracle (C, FP64, OpenMP) on every {stride}th line of the three passes of "
+                      f"tile 0 of {nb}; {dt:.3f} s per sample, scaled x{stride} to one tile and "
+                      f"by 1/{nb} of the {field_points}-point field"}, dt
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import scarl_b200 as S
+    _, lay = layout_of(S)
+    base, dt = cpu_sample(lay, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": base["value"], "unit": "Mpoints/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": config_of(lay),
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "Mpoints/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_of(lay):
+    return {"workload": "512^3 deck -> 513^3 field, exponential, l=(40,20,10), lognormal mean 1 "
+                        "CV 0.3, 2x2x2 tiles, overlap 2l, padded periodic C2R FP32",
+            "global_points": [int(v) for v in lay["L"]], "tile_points": [int(v) for v in lay["Np"]],
+            "overlap_points": [int(v) for v in lay["Np_ovlp"]], "tiles": [int(v) for v in lay["topo"]],
+            "padded_grid": [1 << (2 * int(n) - 1).bit_length() for n in lay["Np"]],
+            "l2": "working set larger than L2 (1.3 GB intermediate, 0.54 GB field)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="scarl", choices=["scarl", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    import scarl_b200 as S
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    ctx = S.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    sample, lay = layout_of(S)
+    sample.seedBase = 1000 * rank  # independent replica per rank
+    L = [int(v) for v in lay["L"]]
+    npts = L[0] * L[1] * L[2]
+    field = torch.empty(npts, dtype=torch.float32, device="cuda")
+
+    def step(out=field, dtype=S.F32):
+        S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=dtype, nb_procs=8,
+                          topo=TOPO, out=out)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident output, CUDA events on the launch stream
+    launches0 = ctx.counters()["launches"]
+    props = torch.cuda.get_device_properties(local)
+    bus = getattr(props, "pci_bus_id", None)
+    if bus is None:
+        bus = "%08x:%02x:%02x.0" % (getattr(props, "pci_domain_id", 0), getattr(props, "pci_bus_id", 0),
+                                     getattr(props, "pci_device_id", 0))
+    clk = Clocks(str(bus))
+    clk.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = ctx.counters()["launches"] - launches0
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * npts / (ms * 1e-3) / 1e6
+
+    # ---- per-kernel device times (separate, profiled steps)
+    ctx.profile(True)
+    ctx.profile_reset()
+    nprof = max(2, min(5, args.steps))
+    for _ in range(nprof):
+        step()
+    torch.cuda.synchronize()
+    stats = ctx.profile_stats()
+    ctx.profile(False)
+    pb, P = pass_bytes(lay)
+    peak, peak_kind = load_peaks()
+    kern = {}
+    for k, (tot, n) in stats.items():
+        avg = tot / max(n, 1)
+        b = pb.get(k)
+        kern[k] = {"launches": n, "avg_ms": round(avg, 4), "share": None,
+                   "gbs": round(b / (avg * 1e-3) / 1e9, 1) if b else None}
+    tot_all = sum(v[0] for v in stats.values()) or 1.0
+    for k, (tot, n) in stats.items():
+        kern[k]["share"] = round(tot / tot_all, 4)
+    dom = max((k for k in kern if k in pb), key=lambda k: stats[k][0]) if kern else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if dom and os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(dom)
+        except Exception:
+            traffic = None
+    roof = None
+    if dom:
+        ach = kern[dom]["gbs"]
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": traffic,
+                "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_launch": pb[dom]}
+
+    # ---- accuracy of the FP32 field against the FP64 path (same seed)
+    f64 = torch.empty(npts, dtype=torch.float64, device="cuda")
+    step(out=f64, dtype=S.F64)
+    step()
+    torch.cuda.synchronize()
+    rel = float(torch.linalg.vector_norm(field.double() - f64) / torch.linalg.vector_norm(f64))
+    del f64
+
+    # ---- end to end through the C ABI with a pinned host buffer
+    host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
+    hnp = host.numpy()
+    ctx.set_stream(0)  # library-owned stream; host calls synchronise inside
+    S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, out=hnp)
+    c0 = ctx.counters()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, out=hnp)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    c1 = ctx.counters()
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": round(world * npts / e2e_s / 1e6, 2), "unit": "Mpoints/s",
+           "h2d_bytes_per_step": (c1["h2d_bytes"] - c0["h2d_bytes"]) // args.steps,
+           "d2h_bytes_per_step": (c1["d2h_bytes"] - c0["d2h_bytes"]) // args.steps,
+           "ms_per_step": round(e2e_s * 1e3, 3)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _ = cpu_sample(lay, 1, 0)
+
+    if dist is not None:
+        dist.barrier()
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpoints/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (Philox normals, seeded per rank)", "config": config_of(lay),
+                "rel_l2_vs_fp64": rel, "roofline": roof, "kernels": kern,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

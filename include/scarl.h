@@ -1,0 +1,257 @@
+/*
+ * scarl.h -- C ABI of scarl_b200, a B200 (sm_100a) implementation of the
+ * ScaRL random-field path: spectral generation on a padded periodic grid (or
+ * the reference's DCT-III generator), partition-of-unity blending of
+ * overlapping subdomain tiles, the marginal transform, and the Stat_ScaRL
+ * moment / covariance estimators.
+ *
+ * Conventions
+ *  - Arrays are column-major (Fortran order, x fastest), as in ScaRL.
+ *  - Every call returns an int status (SCARL_OK = 0); the library never exits
+ *    or traps.  scarl_last_error(ctx) holds the message of the last failure.
+ *  - Field pointers may be host memory (pageable or pinned) or device memory
+ *    of the context's GPU; the library detects which and copies as needed.
+ *  - Device work runs on the context's stream (its own, or one set with
+ *    scarl_ctx_set_stream).  Calls with host pointers return after the
+ *    results are in host memory; calls with device pointers return after the
+ *    work is enqueued (use scarl_sync).
+ *  - One context per host thread.  Contexts own all device scratch memory
+ *    (grown on demand up to the budget given at creation, then reused).
+ *  - Functions marked [host] compute on the CPU and need no GPU; they accept
+ *    ctx == NULL.
+ */
+#ifndef SCARL_H
+#define SCARL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define SCARL_OK 0
+#define SCARL_EINVAL 1       /* invalid argument (verify_inputs rules, sizes) */
+#define SCARL_ENOMEM 2       /* device memory budget or allocation exhausted */
+#define SCARL_EDEVICE 3      /* CUDA error */
+#define SCARL_ETIMEOUT 4     /* a bounded device wait expired */
+#define SCARL_EUNSUPPORTED 5 /* valid in the reference but not provided here */
+#define SCARL_EIO 6          /* file could not be read */
+
+/* ---- enumerations: values of SRC_F/constants_ScaRL.f90:12-19 ---- */
+#define SCARL_FFT 1          /* gen_meth: FFT with localization */
+#define SCARL_FFT_MPI 2      /* gen_meth: slab FFTW-MPI (layout only here) */
+#define SCARL_CM_GAUSSIAN 1
+#define SCARL_CM_VON_KARMAN 2
+#define SCARL_CM_EXPONENTIAL 3 /* no counterpart in the reference */
+#define SCARL_FOM_GAUSSIAN 1
+#define SCARL_FOM_LOGNORMAL 2
+
+/* ---- precisions ---- */
+#define SCARL_F32 4
+#define SCARL_F64 8
+
+/* ---- generators for scarl_generate_sample ---- */
+#define SCARL_GEN_DCT 1      /* gen_std_gauss_FFT, SRC_F/fftw_ScaRL.f90:261 */
+#define SCARL_GEN_SHINO 2    /* gen_std_gauss_Shino_FFT, SRC_F/fftw_ScaRL.f90:157 */
+#define SCARL_GEN_PADDED 3   /* padded periodic C2R, normalised spectra */
+
+typedef struct scarl_ctx scarl_ctx;
+
+/* One deck entry: the 11 per-sample lines of input_ScaRL.txt
+ * (SRC_F/read_input.f90:257-299), plus the von Karman order nu. */
+typedef struct {
+  char name[256];
+  double xMinGlob[3];
+  double xMaxGlob[3];
+  double corrL[3];
+  double overlap[3];      /* in correlation lengths */
+  int pointsPerCorrL[3];
+  int corrMod;
+  int margiFirst;
+  double avg;
+  double std_dev;
+  int seedBase;
+  double nu;              /* von Karman smoothness (0.5 = exponential) */
+} scarl_sample;
+
+/* Index maps of one sample (SRC_F/main_ScaRL.f90:100-176). */
+typedef struct {
+  int L[3];               /* global points after the re-fit of :176 */
+  int Np[3];              /* points per tile */
+  int Np_ovlp[3];         /* overlap points */
+  int topo_shape[3];      /* tiles per axis */
+  int nb_tiles;           /* product(topo_shape) */
+  double xStep[3];
+} scarl_layout;
+
+/* Geometry of one tile (SRC_F/main_ScaRL.f90:455-468). */
+typedef struct {
+  int topo_pos[3];
+  int pos_0[3];           /* 1-based, like the reference */
+  int pos_N[3];
+  double coord_0[3];
+  double coord_N[3];
+  double xRange[3];
+} scarl_tile;
+
+/* Options of scarl_generate_sample; zero-initialise for the defaults. */
+typedef struct {
+  int generator;          /* SCARL_GEN_*, 0 = SCARL_GEN_PADDED */
+  int dtype;              /* SCARL_F32 / SCARL_F64, 0 = SCARL_F32 */
+  int nb_procs;           /* tiles requested (mpirun -np), 0 = 1 */
+  int topo_shape[3];      /* explicit topology (extra_config_ScaRL.txt); 0 = decide */
+  int pad[3];             /* padded grid per axis, 0 = 2^ceil(log2(2 Np)) */
+  int no_spectral_normalisation; /* 1 = raw Riemann-sum amplitudes */
+  int normalize_field;    /* 1 = normalize_field (disabled in the reference) */
+  uint32_t stream;        /* realisation stream (ensembles), 0 by default */
+  const double* phiK;     /* DCT generator: injected phases, nb x (Np/2)^3 */
+} scarl_gen_opts;
+
+/* ------------------------------------------------------------------ */
+/* Context                                                             */
+/* ------------------------------------------------------------------ */
+int scarl_ctx_create(int device, size_t budget_bytes, scarl_ctx** ctx);
+int scarl_ctx_destroy(scarl_ctx* ctx);
+const char* scarl_last_error(const scarl_ctx* ctx);
+int scarl_ctx_set_stream(scarl_ctx* ctx, void* cuda_stream);
+int scarl_sync(scarl_ctx* ctx);
+/* Kernels launched and bytes copied host->device / device->host by this
+ * context since its creation. */
+int scarl_counters(scarl_ctx* ctx, long long* launches, unsigned long long* h2d_bytes,
+                   unsigned long long* d2h_bytes);
+/* Per-kernel device time (CUDA events around each launch) while enabled;
+ * enable = 2 clears the accumulated times. */
+int scarl_profile(scarl_ctx* ctx, int enable);
+int scarl_profile_read(scarl_ctx* ctx, int idx, char* name, size_t name_len,
+                       double* total_ms, long long* launches);
+const char* scarl_version(void);
+
+/* ------------------------------------------------------------------ */
+/* [host] Index maps, topology, weights (bit-exact restatements)       */
+/* ------------------------------------------------------------------ */
+/* SRC_F/main_ScaRL.f90:271-340 (verify_inputs): 0 or SCARL_EINVAL with the
+ * reference's message in msg.  corrMod 2/3 are accepted (new models). */
+int scarl_verify_inputs(const scarl_sample* s, int gen_meth, char* msg, size_t msg_len);
+/* SRC_F/main_ScaRL.f90:788-897 (decide_topo_shape, localization branch). */
+int scarl_decide_topo_shape(int nb_procs, const int L[3], const int Np_ovlp[3],
+                            long long pointsPerBlockIdeal, int topo_shape[3]);
+/* SRC_F/main_ScaRL.f90:747-782 (get_topo_pos / get_topo_rank). */
+int scarl_get_topo_pos(int rank, const int topo_shape[3], int topo_pos[3]);
+int scarl_get_topo_rank(const int topo_shape[3], const int topo_pos[3]);
+/* SRC_F/main_ScaRL.f90:100-176: xStep, L, Np_ovlp, topology, Np, re-fitted L.
+ * topo_shape_in = NULL decides the topology for nb_procs tiles. */
+int scarl_sample_layout(const scarl_sample* s, int gen_meth, int nb_procs,
+                        const int* topo_shape_in, scarl_layout* out);
+/* SRC_F/main_ScaRL.f90:455-459 (pos_0, pos_N, coord_0, coord_N, xRange). */
+int scarl_tile_geometry(const scarl_layout* lay, const double xMinGlob[3], int rank,
+                        scarl_tile* out);
+/* SRC_F/main_ScaRL.f90:1236-1294: the Np[0]*Np[1]*Np[2] weight array. */
+int scarl_unity_partition_weights(const int Np[3], const int Np_ovlp[3], int partitionType,
+                                  const int topo_pos[3], const int topo_shape[3], double* w);
+/* SRC_F/fftw_ScaRL.f90:194 and SRC_F/spectra_ScaRL.f90:44-56: padded grid,
+ * spectrum box and delta_k of the Shino generator (k_cut clamped to k_max). */
+int scarl_shino_sizes(const int Np[3], const double xRange[3], const double corrL[3],
+                      int sz_c[3], int sz_Sk[3], double delta_k[3]);
+
+/* ------------------------------------------------------------------ */
+/* [host] Input decks (SRC_F/read_input.f90)                           */
+/* ------------------------------------------------------------------ */
+/* read_config_ScaRL :26-102; a missing file gives the defaults of :74-83. */
+int scarl_read_config(const char* path, int* gen_meth, int* c_info_file, int* d_sample,
+                      int* one_file, int* one_hdf_ds, char* input_file, size_t len);
+/* read_extra_config_ScaRL :108-149; *found = 0 when the file is absent. */
+int scarl_read_extra_config(const char* path, int* found, int topo_shape[3]);
+/* read_input_ScaRL :159-348.  Call with samples = NULL to get the count. */
+int scarl_read_input(const char* path, char* output_folder, size_t folder_len,
+                     int* nSamples, scarl_sample* samples, int max_samples);
+/* read_input_SEM :354-559 (random.spec + domains.txt in folder). */
+int scarl_read_input_sem(const char* folder, char* output_folder, size_t folder_len,
+                         int* nSamples, scarl_sample* samples, int max_samples);
+
+/* ------------------------------------------------------------------ */
+/* Generation                                                          */
+/* ------------------------------------------------------------------ */
+/* Drop-in for gen_std_gauss_FFT (SRC_F/fftw_ScaRL.f90:261-418), FP64.
+ * data_real_3D: Np[0]*Np[1]*Np[2] doubles (caller-allocated, overwritten).
+ * phiK / gammaK: the (Np/2)^3 phase and amplitude arrays the reference draws
+ * with random_number (:364-367); phiK = NULL draws Philox uniforms keyed by
+ * seed + rank, gammaK = NULL uses 1 (the reference's :367).  corrMod must be
+ * SCARL_CM_GAUSSIAN (the only model of this routine). */
+int scarl_gen_std_gauss_fft(scarl_ctx* ctx, double* data_real_3D, const int Np[3],
+                            const double xRange[3], const double corrL[3], int corrMod,
+                            int seed, int rank, const double* phiK, const double* gammaK);
+
+/* Drop-in for gen_std_gauss_Shino_FFT + build_Sk_mtx (SRC_F/fftw_ScaRL.f90:
+ * 157-255, SRC_F/spectra_ScaRL.f90:10-142), FP64: Park-Miller phases from
+ * seed + 1000000, the reference's amplitude and scaling, padded grid
+ * 2^ceil(log2(2 Np)), real part cropped to Np.  The quadrant placement uses
+ * the full first axis of the spectrum box (the reference's :204 halves it). */
+int scarl_gen_std_gauss_shino_fft(scarl_ctx* ctx, double* data_real_3D, const int Np[3],
+                                  const double xRange[3], const double corrL[3],
+                                  const int pointsPerCorrL[3], int corrMod, int seed, int rank);
+
+/* Padded periodic method, one tile, no blending: Np[0]*Np[1]*Np[2] values of
+ * dtype written to out.  Grid spacing xStep, padded grid pad (0 entries =
+ * 2^ceil(log2(2 Np))).  corrMod 1/2/3 with nu for 2.  normalise = 1 scales
+ * the spectrum so the periodic field has unit variance (FP64 sum on the
+ * GPU).  xi = NULL draws Philox normals keyed by (seed, stream); otherwise xi
+ * holds (P0/2+1)*P1*P2 pairs (re, im) of dtype, mode index kx fastest. */
+int scarl_gen_padded(scarl_ctx* ctx, void* out, int dtype, const int Np[3], const int pad[3],
+                     const double xStep[3], const double corrL[3], int corrMod, double nu,
+                     int normalise, uint64_t seed, uint32_t stream, const void* xi);
+
+/* One deck sample end to end on the GPU (SRC_F/main_ScaRL.f90:95-214 +
+ * create_fields :345-583 without file output): layout, every tile generated,
+ * PoU-weighted, overlap-summed and assembled into the global field
+ * L[0]*L[1]*L[2] (layout from scarl_sample_layout), marginal transformed.
+ * global: dtype values. */
+int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen_opts* opts,
+                          void* global);
+
+/* ------------------------------------------------------------------ */
+/* Post steps (device kernels; FP64 fields in place)                   */
+/* ------------------------------------------------------------------ */
+/* apply_UnityPartition_mtx (SRC_F/main_ScaRL.f90:1216-1301), bit-exact. */
+int scarl_apply_unity_partition(scarl_ctx* ctx, double* field, const int Np[3],
+                                const int Np_ovlp[3], int partitionType, const int topo_pos[3],
+                                const int topo_shape[3]);
+/* add_overlap (SRC_F/main_ScaRL.f90:984-1210) over every tile at once:
+ * tiles holds nb = prod(topo_shape) consecutive Np blocks in rank order;
+ * each block receives its neighbours' overlap regions, bit-exact. */
+int scarl_add_overlap(scarl_ctx* ctx, double* tiles, const int Np[3], const int Np_ovlp[3],
+                      const int topo_shape[3]);
+/* multiVariateTransformation (SRC_F/main_ScaRL.f90:1355-1395). */
+int scarl_multivariate_transformation(scarl_ctx* ctx, void* field, int dtype, long long n,
+                                      double avg, double std_dev, int margiFirst);
+/* normalize_field (SRC_F/main_ScaRL.f90:903-953) on an assembled global
+ * field (every point counted once): standardise, FP64 sums on the GPU. */
+int scarl_normalize_field(scarl_ctx* ctx, void* field, int dtype, long long n, double* avg,
+                          double* std_dev);
+
+/* ------------------------------------------------------------------ */
+/* Estimators (Stat_ScaRL), FP64 accumulation on the GPU               */
+/* ------------------------------------------------------------------ */
+/* calculate_average_and_stdVar_MPI (SRC_F/Stat_ScaRL/statistics_RF.f90:
+ * 18-174): field is xNTotal x Nmc; per-realisation and global mean and
+ * population standard deviation sqrt(E[x^2] - E[x]^2). */
+int scarl_moments(scarl_ctx* ctx, const void* field, int dtype, long long xNTotal, int Nmc,
+                  double* evntAvg, double* evntStdDev, double* globalAvg,
+                  double* globalStdDev);
+/* rebuild_Sk_FFT + rebuild_Sk (statistics_RF.f90:180-462) for one field
+ * L[0]*L[1]*L[2]: per direction the circular autocovariance of the
+ * standardised, Tukey-windowed field averaged over lines, first floor(L/2)
+ * lags kept.  SkTot receives floor(L0/2)+floor(L1/2)+floor(L2/2) values.
+ * tukey_literal = 1 reproduces the reference's window (single-precision
+ * r_tukey, taper formula over every ratio > r); 0 the standard Tukey window. */
+int scarl_rebuild_sk(scarl_ctx* ctx, const void* field, int dtype, const int L[3], double avg,
+                     double stdDev, int tukey_literal, double* SkTot);
+/* [host] rebuild_corrL (statistics_RF.f90:468-486). */
+int scarl_rebuild_corrL(const double* SkTot, const int L[3], const double xStep[3],
+                        double corrL_out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

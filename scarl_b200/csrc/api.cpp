@@ -1,0 +1,1262 @@
+// api.cpp -- the C ABI of scarl_b200 (include/scarl.h): contexts, device
+// workspace, cached per-grid plans (twiddles, spectrum tables and the FP64
+// spectral normalisation), host<->device staging, and the dispatch of every
+// entry point onto the sm_100a kernels.  No CPU fallback: every numerical
+// entry point runs on the GPU or returns an error.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/scarl.h"
+#include "host_maps.h"
+#include "scarl_internal.h"
+
+using namespace scarl;
+
+namespace {
+
+constexpr double kPiRef = 3.1415926535898;  // SRC_F/constants_ScaRL.f90:5
+
+struct Buf {
+  void* p = nullptr;
+  size_t n = 0;
+};
+
+struct PaddedPlan {
+  int dt = 4;
+  int amp = AMP_SEPARABLE;
+  double expo = 0.0;
+  double norm = 1.0;
+  Buf tabs;
+  const void* t[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+struct Mark {
+  std::string name;
+  cudaEvent_t a, b;
+};
+
+}  // namespace
+
+struct scarl_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  size_t budget = 0, used = 0;
+  std::string err;
+  Buf work, tile, stage_out, stage_in, stage_in2, tabs, dtabs, part, t1, t2, sk, pmpw;
+  void* pin = nullptr;
+  size_t pin_n = 0;
+  cudaEvent_t pin_ev = nullptr;
+  std::map<std::string, PaddedPlan> plans;
+  std::map<long long, Buf> twiddles;
+  std::map<int, Buf> dct_tabs;
+  bool profile = false;
+  long long launches = 0;
+  unsigned long long h2d = 0, d2h = 0;
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::string> porder;
+  std::map<std::string, std::pair<double, long long>> pstats;
+};
+
+namespace {
+
+int fail(scarl_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(ctx, SCARL_EDEVICE, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define RC(call)                     \
+  do {                               \
+    int r_ = (call);                 \
+    if (r_ != SCARL_OK) return r_;   \
+  } while (0)
+
+int ensure(scarl_ctx* ctx, Buf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.n >= bytes) return SCARL_OK;
+  const size_t want = bytes;
+  if (ctx->used - b.n + want > ctx->budget)
+    return fail(ctx, SCARL_ENOMEM, "device memory budget exceeded (" + std::to_string(want) + " bytes requested)");
+  if (b.p) {
+    cudaFree(b.p);
+    ctx->used -= b.n;
+    b.p = nullptr;
+    b.n = 0;
+  }
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    return fail(ctx, SCARL_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  b.n = want;
+  ctx->used += want;
+  return SCARL_OK;
+}
+
+void release(scarl_ctx* ctx, Buf& b) {
+  if (b.p) {
+    cudaFree(b.p);
+    ctx->used -= b.n;
+  }
+  b.p = nullptr;
+  b.n = 0;
+}
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Pinned host staging for small tables; waits for the previous upload.
+int pinned(scarl_ctx* ctx, size_t bytes, void** out) {
+  if (ctx->pin_ev) CK(cudaEventSynchronize(ctx->pin_ev));
+  if (ctx->pin_n < bytes) {
+    if (ctx->pin) cudaFreeHost(ctx->pin);
+    ctx->pin = nullptr;
+    ctx->pin_n = 0;
+    CK(cudaMallocHost(&ctx->pin, bytes));
+    ctx->pin_n = bytes;
+  }
+  *out = ctx->pin;
+  return SCARL_OK;
+}
+
+int upload_pinned(scarl_ctx* ctx, void* dst, size_t bytes) {
+  CK(cudaMemcpyAsync(dst, ctx->pin, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += bytes;
+  if (!ctx->pin_ev) CK(cudaEventCreateWithFlags(&ctx->pin_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ctx->pin_ev, ctx->stream));
+  return SCARL_OK;
+}
+
+// ---- profiling: events around each launch while enabled ----
+cudaEvent_t pool_event(scarl_ctx* ctx) {
+  if (!ctx->pool.empty()) {
+    cudaEvent_t e = ctx->pool.back();
+    ctx->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct Prof {
+  scarl_ctx* c;
+  bool on;
+  Mark m;
+  Prof(scarl_ctx* ctx, const char* name, int nlaunch = 1) : c(ctx), on(ctx->profile) {
+    c->launches += nlaunch;
+    if (on) {
+      m.name = name;
+      m.a = pool_event(c);
+      m.b = pool_event(c);
+      cudaEventRecord(m.a, c->stream);
+    }
+  }
+  ~Prof() {
+    if (on) {
+      cudaEventRecord(m.b, c->stream);
+      c->marks.push_back(m);
+    }
+  }
+};
+
+void flush_marks(scarl_ctx* ctx) {
+  if (ctx->marks.empty()) return;
+  cudaEventSynchronize(ctx->marks.back().b);
+  for (Mark& m : ctx->marks) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, m.a, m.b);
+    auto it = ctx->pstats.find(m.name);
+    if (it == ctx->pstats.end()) {
+      ctx->porder.push_back(m.name);
+      ctx->pstats[m.name] = {0.0, 0};
+    }
+    ctx->pstats[m.name].first += ms;
+    ctx->pstats[m.name].second += 1;
+    ctx->pool.push_back(m.a);
+    ctx->pool.push_back(m.b);
+  }
+  ctx->marks.clear();
+}
+
+int begin(scarl_ctx* ctx) {
+  if (!ctx) return SCARL_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  return SCARL_OK;
+}
+
+// Output destination on the device: the caller's pointer or the staging
+// buffer, copied back by finish_out.
+int out_dev(scarl_ctx* ctx, void* user, size_t bytes, void** dev, bool* host) {
+  if (!user) return fail(ctx, SCARL_EINVAL, "null output pointer");
+  *host = !is_device_ptr(user);
+  if (!*host) {
+    *dev = user;
+    return SCARL_OK;
+  }
+  RC(ensure(ctx, ctx->stage_out, bytes));
+  *dev = ctx->stage_out.p;
+  return SCARL_OK;
+}
+
+int finish_out(scarl_ctx* ctx, void* user, const void* dev, size_t bytes, bool host) {
+  if (host) {
+    CK(cudaMemcpyAsync(user, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->d2h += bytes;
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  CK(cudaGetLastError());
+  return SCARL_OK;
+}
+
+// Input on the device: the caller's pointer or a copy in buf.
+int in_dev(scarl_ctx* ctx, Buf& buf, const void* user, size_t bytes, const void** dev) {
+  if (!user) {
+    *dev = nullptr;
+    return SCARL_OK;
+  }
+  if (is_device_ptr(user)) {
+    *dev = user;
+    return SCARL_OK;
+  }
+  RC(ensure(ctx, buf, bytes));
+  CK(cudaMemcpyAsync(buf.p, user, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += bytes;
+  *dev = buf.p;
+  return SCARL_OK;
+}
+
+bool pow2(int n) { return n >= 2 && (n & (n - 1)) == 0; }
+int default_pad(int Np) {
+  int p = 1;
+  while (p < 2 * Np) p <<= 1;
+  return p;
+}
+int round_up(int a, int m) { return (a + m - 1) / m * m; }
+
+// e^{2 pi i m / P}, m < P, rounded from long double.
+int twiddles(scarl_ctx* ctx, int P, int dt, const void** out) {
+  const long long key = (long long)P * 16 + dt;
+  auto it = ctx->twiddles.find(key);
+  if (it != ctx->twiddles.end()) {
+    *out = it->second.p;
+    return SCARL_OK;
+  }
+  Buf b;
+  RC(ensure(ctx, b, (size_t)P * 2 * dt));
+  std::vector<double> d(2 * (size_t)P);
+  const long double pi = 3.14159265358979323846264338327950288L;
+  for (int m = 0; m < P; ++m) {
+    const long double a = 2.0L * pi * (long double)m / (long double)P;
+    d[2 * m] = (double)cosl(a);
+    d[2 * m + 1] = (double)sinl(a);
+  }
+  if (dt == 8) {
+    CK(cudaMemcpy(b.p, d.data(), d.size() * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(d.begin(), d.end());
+    CK(cudaMemcpy(b.p, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+  }
+  ctx->twiddles[key] = b;
+  *out = b.p;
+  return SCARL_OK;
+}
+
+double freq(int k, int P, double dx) {
+  const int s = (2 * k <= P) ? k : k - P;
+  return (double)s / ((double)P * dx);
+}
+
+// Spectrum tables and the FP64 spectral normalisation of one padded grid.
+int padded_plan(scarl_ctx* ctx, int dt, const int P[3], const double dx[3],
+                const double corrL[3], int corrMod, double nu, int normalise,
+                PaddedPlan** out) {
+  char key[512];
+  std::snprintf(key, sizeof key, "%d|%d,%d,%d|%a,%a,%a|%a,%a,%a|%d|%a|%d", dt, P[0], P[1], P[2],
+                dx[0], dx[1], dx[2], corrL[0], corrL[1], corrL[2], corrMod, nu, normalise);
+  auto it = ctx->plans.find(key);
+  if (it != ctx->plans.end()) {
+    *out = &it->second;
+    return SCARL_OK;
+  }
+  PaddedPlan pl;
+  pl.dt = dt;
+  const int Hx = P[0] / 2 + 1;
+  const int n[3] = {Hx, P[1], P[2]};
+  std::vector<double> r[3];
+  double craw2 = 0.0;
+  if (corrMod == SCARL_CM_GAUSSIAN) {
+    pl.amp = AMP_SEPARABLE;
+    for (int d = 0; d < 3; ++d) {
+      const double dk = 1.0 / ((double)P[d] * dx[d]);
+      r[d].resize(n[d]);
+      for (int k = 0; k < n[d]; ++k) {
+        const double f = freq(k, P[d], dx[d]);
+        r[d][k] = std::sqrt(corrL[d] * dk) * std::exp(-M_PI * corrL[d] * corrL[d] * f * f / 2.0);
+      }
+    }
+  } else {
+    const double v = (corrMod == SCARL_CM_EXPONENTIAL) ? 0.5 : nu;
+    const double sc = std::tgamma(v) / (2.0 * std::sqrt(M_PI) * std::tgamma(v + 0.5));
+    double a[3], dk3 = 1.0;
+    for (int d = 0; d < 3; ++d) {
+      a[d] = corrL[d] * sc;
+      dk3 *= 1.0 / ((double)P[d] * dx[d]);
+    }
+    const double C = 8.0 * std::pow(M_PI, 1.5) * std::tgamma(v + 1.5) / std::tgamma(v) * a[0] * a[1] * a[2];
+    craw2 = C * dk3;
+    pl.expo = -(v + 1.5) / 2.0;
+    pl.amp = (v == 0.5) ? AMP_RECIP : AMP_POW;
+    for (int d = 0; d < 3; ++d) {
+      r[d].resize(n[d]);
+      for (int k = 0; k < n[d]; ++k) {
+        const double f = freq(k, P[d], dx[d]);
+        r[d][k] = 4.0 * M_PI * M_PI * a[d] * a[d] * f * f;
+      }
+    }
+  }
+  // FP64 normalisation sum on the GPU over the full periodic grid.
+  double norm = 1.0;
+  if (normalise) {
+    Buf t64;
+    const size_t tot = (size_t)n[0] + n[1] + n[2];
+    RC(ensure(ctx, t64, tot * 8));
+    std::vector<double> h;
+    h.insert(h.end(), r[0].begin(), r[0].end());
+    h.insert(h.end(), r[1].begin(), r[1].end());
+    h.insert(h.end(), r[2].begin(), r[2].end());
+    CK(cudaMemcpy(t64.p, h.data(), tot * 8, cudaMemcpyHostToDevice));
+    const double* d0 = (const double*)t64.p;
+    const double* d1 = d0 + n[0];
+    const double* d2 = d1 + n[1];
+    GenArgs ga;
+    std::memset(&ga, 0, sizeof ga);
+    for (int d = 0; d < 3; ++d) ga.P[d] = P[d];
+    ga.Hx = Hx;
+    ga.amp = pl.amp;
+    ga.expo = pl.expo;
+    ga.qx = d0; ga.qy = d1; ga.qz = d2;
+    const int nb = spectrum_sum_blocks();
+    RC(ensure(ctx, ctx->part, (size_t)nb * 8));
+    {
+      Prof pr(ctx, "spectrum_sum");
+      CK(launch_spectrum_sum(ga, d0, d1, d2, craw2, (double*)ctx->part.p, nb, ctx->stream));
+    }
+    std::vector<double> parts(nb);
+    CK(cudaMemcpyAsync(parts.data(), ctx->part.p, (size_t)nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    release(ctx, t64);
+    norm = 0.0;
+    for (double p : parts) norm += p;
+    if (!(norm > 0.0)) return fail(ctx, SCARL_EINVAL, "spectrum sums to zero on this grid");
+  }
+  pl.norm = norm;
+  // Device tables in the pass precision.
+  const double inv = 1.0 / std::sqrt(norm);
+  std::vector<double> tab;
+  std::vector<size_t> off(6, 0);
+  auto push = [&](int slot, const std::vector<double>& v) {
+    off[slot] = tab.size();
+    tab.insert(tab.end(), v.begin(), v.end());
+  };
+  std::vector<double> ax(Hx);
+  for (int k = 0; k < Hx; ++k) {
+    const double g = (k == 0 || 2 * k == P[0]) ? 1.0 : M_SQRT1_2;
+    ax[k] = (pl.amp == AMP_SEPARABLE ? r[0][k] : std::sqrt(craw2)) * g * inv;
+  }
+  push(0, ax);
+  if (pl.amp == AMP_SEPARABLE) {
+    push(1, r[1]);
+    push(2, r[2]);
+  } else {
+    push(3, r[0]);
+    push(4, r[1]);
+    push(5, r[2]);
+  }
+  RC(ensure(ctx, pl.tabs, tab.size() * dt));
+  if (dt == 8) {
+    CK(cudaMemcpy(pl.tabs.p, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(tab.begin(), tab.end());
+    CK(cudaMemcpy(pl.tabs.p, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+  }
+  for (int s = 0; s < 6; ++s) pl.t[s] = (const char*)pl.tabs.p + off[s] * dt;
+  if (pl.amp == AMP_SEPARABLE) pl.t[3] = pl.t[4] = pl.t[5] = nullptr;
+  else pl.t[1] = pl.t[2] = nullptr;
+  auto ins = ctx->plans.emplace(key, pl);
+  *out = &ins.first->second;
+  return SCARL_OK;
+}
+
+int pm_powers(scarl_ctx* ctx, const uint32_t** out) {
+  if (!ctx->pmpw.p) {
+    RC(ensure(ctx, ctx->pmpw, 64 * 4));
+    uint32_t h[64];
+    uint64_t b = 16807;
+    for (int i = 0; i < 64; ++i) {
+      h[i] = (uint32_t)b;
+      b = (b * b) % 2147483647ull;
+    }
+    CK(cudaMemcpy(ctx->pmpw.p, h, sizeof h, cudaMemcpyHostToDevice));
+  }
+  *out = (const uint32_t*)ctx->pmpw.p;
+  return SCARL_OK;
+}
+
+// One Park-Miller step with Schrage's factorisation (SRC_F/normal_ScaRL.f90:827-833).
+int32_t schrage(int32_t seed) {
+  int32_t k = seed / 127773;
+  seed = 16807 * (seed - k * 127773) - k * 2836;
+  if (seed < 0) seed += 2147483647;
+  return seed;
+}
+
+int run_passes(scarl_ctx* ctx, int dt, const GenArgs& a) {
+  {
+    Prof p(ctx, "k_gen_z");
+    CK(launch_gen_pass(dt, 1, a, ctx->stream));
+  }
+  {
+    Prof p(ctx, "k_mid_y");
+    CK(launch_gen_pass(dt, 2, a, ctx->stream));
+  }
+  {
+    Prof p(ctx, "k_c2r_x");
+    CK(launch_gen_pass(dt, 3, a, ctx->stream));
+  }
+  return SCARL_OK;
+}
+
+int check_grid(scarl_ctx* ctx, const int P[3], const int Np[3]) {
+  for (int d = 0; d < 3; ++d) {
+    if (Np[d] < 1) return fail(ctx, SCARL_EINVAL, "Np must be >= 1");
+    if (!pow2(P[d]) || P[d] < 8 || P[d] > 2048)
+      return fail(ctx, SCARL_EUNSUPPORTED, "padded grid must be a power of two in [8, 2048]");
+    if (P[d] < Np[d]) return fail(ctx, SCARL_EINVAL, "padded grid smaller than the tile");
+  }
+  return SCARL_OK;
+}
+
+// Common GenArgs of the padded passes for one tile.
+int gen_args(scarl_ctx* ctx, int dt, const int P[3], const int Np[3], GenArgs* a) {
+  std::memset(a, 0, sizeof *a);
+  for (int d = 0; d < 3; ++d) {
+    a->P[d] = P[d];
+    a->Nout[d] = Np[d];
+  }
+  a->Hx = P[0] / 2 + 1;
+  a->Hpad = round_up(a->Hx, 16);
+  const size_t wbytes = (size_t)a->Hpad * P[1] * Np[2] * 2 * dt;
+  RC(ensure(ctx, ctx->work, wbytes));
+  a->work = ctx->work.p;
+  RC(twiddles(ctx, P[2], dt, &a->tw_z));
+  RC(twiddles(ctx, P[1], dt, &a->tw_y));
+  RC(twiddles(ctx, P[0], dt, &a->tw_x));
+  return SCARL_OK;
+}
+
+void set_plan(GenArgs* a, const PaddedPlan* pl) {
+  a->spec = SPEC_PHILOX;
+  a->amp = pl->amp;
+  a->expo = pl->expo;
+  a->ax = pl->t[0];
+  a->ay = pl->t[1];
+  a->az = pl->t[2];
+  a->qx = pl->t[3];
+  a->qy = pl->t[4];
+  a->qz = pl->t[5];
+}
+
+// Marginal parameters exactly as SRC_F/main_ScaRL.f90:1371-1389.
+int marginal_params(scarl_ctx* ctx, int margiFirst, double avg, double std_dev, double* s,
+                    double* mu) {
+  double nv, na;
+  if (margiFirst == SCARL_FOM_GAUSSIAN) {
+    nv = std_dev * std_dev;
+    na = avg;
+  } else if (margiFirst == SCARL_FOM_LOGNORMAL) {
+    if (avg <= 0.0)
+      return fail(ctx, SCARL_EINVAL, "ERROR - when using lognormal fieldAvg should be a positive number");
+    const double cv = std_dev / avg;
+    nv = std::log(1.0 + cv * cv);
+    na = std::log(avg) - nv / 2.0;
+  } else {
+    return fail(ctx, SCARL_EINVAL, "First-order marginal not detected");
+  }
+  *s = std::sqrt(nv);
+  *mu = na;
+  return SCARL_OK;
+}
+
+// Blend tables of every tile: per tile, per axis lo[Np], hi[Np] (doubles)
+// then flags[Np] (bytes), uploaded once.
+struct BlendTabs {
+  size_t dbl_off[64][3];
+  size_t flag_off[64][3];
+};
+
+int upload_blend_tables(scarl_ctx* ctx, const scarl_layout& lay, int partitionType,
+                        std::vector<BlendAxis>* axes) {
+  const int nb = lay.nb_tiles;
+  size_t nd = 0, nf = 0;
+  for (int d = 0; d < 3; ++d) {
+    nd += 2 * (size_t)lay.Np[d];
+    nf += (size_t)lay.Np[d];
+  }
+  const size_t dbytes = nd * 8 * nb;
+  const size_t fbytes = round_up((int)(nf * nb), 16);
+  const size_t total = dbytes + fbytes;
+  void* hp;
+  RC(pinned(ctx, total, &hp));
+  RC(ensure(ctx, ctx->tabs, total));
+  double* hd = (double*)hp;
+  uint8_t* hf = (uint8_t*)hp + dbytes;
+  const char* dbase = (const char*)ctx->tabs.p;
+  axes->resize((size_t)nb * 3);
+  size_t od = 0, of = 0;
+  for (int r = 0; r < nb; ++r) {
+    int pos[3];
+    get_topo_pos(r, lay.topo_shape, pos);
+    for (int d = 0; d < 3; ++d) {
+      const int Np = lay.Np[d];
+      pou_axis_tables(Np, lay.Np_ovlp[d], pos[d], lay.topo_shape[d], partitionType, hd + od, hd + od + Np);
+      blend_axis_flags(Np, lay.Np_ovlp[d], pos[d], lay.topo_shape[d], hf + of);
+      BlendAxis& ax = (*axes)[(size_t)r * 3 + d];
+      ax.lo = (const double*)(dbase + od * 8);
+      ax.hi = (const double*)(dbase + (od + Np) * 8);
+      ax.flags = (const uint8_t*)(dbase + dbytes + of);
+      od += 2 * (size_t)Np;
+      of += (size_t)Np;
+    }
+  }
+  RC(upload_pinned(ctx, ctx->tabs.p, total));
+  return SCARL_OK;
+}
+
+int dct_table(scarl_ctx* ctx, int N, const double** out) {
+  auto it = ctx->dct_tabs.find(N);
+  if (it != ctx->dct_tabs.end()) {
+    *out = (const double*)it->second.p;
+    return SCARL_OK;
+  }
+  Buf b;
+  RC(ensure(ctx, b, (size_t)4 * N * 8));
+  std::vector<double> c(4 * (size_t)N);
+  for (int m = 0; m < 4 * N; ++m) c[m] = std::cos(M_PI * (double)m / (2.0 * (double)N));
+  CK(cudaMemcpy(b.p, c.data(), c.size() * 8, cudaMemcpyHostToDevice));
+  ctx->dct_tabs[N] = b;
+  *out = (const double*)b.p;
+  return SCARL_OK;
+}
+
+// gen_std_gauss_FFT on the device into dev_out (Np doubles).
+int dct_tile(scarl_ctx* ctx, double* dev_out, const int Np[3], const double xRange[3],
+             const double corrL[3], const double* phi_dev, const double* gamma_dev,
+             uint32_t key) {
+  DctArgs a;
+  std::memset(&a, 0, sizeof a);
+  size_t ktot = 1, t1n, t2n;
+  std::vector<double> ex;
+  for (int d = 0; d < 3; ++d) {
+    a.Np[d] = Np[d];
+    a.K[d] = Np[d] / 2;
+    a.corrL[d] = corrL[d];
+    ktot *= (size_t)a.K[d];
+  }
+  t1n = (size_t)Np[0] * a.K[1] * a.K[2];
+  t2n = (size_t)Np[0] * Np[1] * a.K[2];
+  // per-axis exp(-PI k^2) factors, SRC_F/fftw_ScaRL.f90:300-326
+  std::vector<double> h;
+  size_t off[3];
+  for (int d = 0; d < 3; ++d) {
+    off[d] = h.size();
+    const double delta_x = xRange[d] / (double)(Np[d] - 1);
+    const double k_max = 1.0 / delta_x;
+    const double dk = k_max / (double)(Np[d] - 1);
+    for (int i = 0; i < a.K[d]; ++i) {
+      const double kp = (double)i * dk / corrL[d];
+      h.push_back(std::exp(-kPiRef * (kp * kp)));
+    }
+  }
+  h.push_back(0.0);
+  void* hp;
+  RC(pinned(ctx, h.size() * 8, &hp));
+  std::memcpy(hp, h.data(), h.size() * 8);
+  RC(ensure(ctx, ctx->dtabs, h.size() * 8));
+  RC(upload_pinned(ctx, ctx->dtabs.p, h.size() * 8));
+  const double* dt = (const double*)ctx->dtabs.p;
+  a.cx = dt + off[0];
+  a.cy = dt + off[1];
+  a.cz = dt + off[2];
+  RC(ensure(ctx, ctx->sk, std::max<size_t>(ktot, 1) * 8));
+  RC(ensure(ctx, ctx->t1, std::max<size_t>(t1n, 1) * 8));
+  RC(ensure(ctx, ctx->t2, std::max<size_t>(t2n, 1) * 8));
+  a.sk = (double*)ctx->sk.p;
+  a.t1 = (double*)ctx->t1.p;
+  a.t2 = (double*)ctx->t2.p;
+  a.out = dev_out;
+  a.phi = phi_dev;
+  a.gamma = gamma_dev;
+  a.k0 = key;
+  a.k1 = 0;
+  a.stream = 0;
+  for (int d = 0; d < 3; ++d) RC(dct_table(ctx, Np[d], &a.ctab[d]));
+  Prof p(ctx, "k_dct_literal", 4);
+  CK(launch_dct_literal(a, ctx->stream));
+  return SCARL_OK;
+}
+
+// Literal Shino GenArgs for one tile (SRC_F/fftw_ScaRL.f90:157-255).
+int shino_args(scarl_ctx* ctx, const int Np[3], const double xRange[3], const double corrL[3],
+               int seed, GenArgs* a) {
+  int sz_c[3], sz[3];
+  double dk[3];
+  shino_sizes(Np, xRange, corrL, sz_c, sz, dk);
+  RC(check_grid(ctx, sz_c, Np));
+  RC(gen_args(ctx, 8, sz_c, Np, a));
+  a->spec = SPEC_SHINO;
+  for (int d = 0; d < 3; ++d) {
+    a->sz[d] = sz[d];
+    a->de[d] = ((kPiRef * kPiRef) / 2.0) * (dk[d] * dk[d]);
+  }
+  a->shino_scale = std::sqrt(8.0);
+  a->shino_f = 2.0 * std::sqrt((dk[0] * dk[1]) * dk[2]);
+  const int32_t s0 = (int32_t)((uint32_t)seed + 1000000u);
+  a->pm_s1 = (uint32_t)schrage(s0);
+  RC(pm_powers(ctx, &a->pm_pw));
+  return SCARL_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* scarl_version(void) { return "scarl_b200 0.1 (sm_100a)"; }
+
+int scarl_ctx_create(int device, size_t budget_bytes, scarl_ctx** out) {
+  if (!out) return SCARL_EINVAL;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return SCARL_EDEVICE;
+  }
+  if (device < 0 || device >= n) return SCARL_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return SCARL_EDEVICE;
+  scarl_ctx* c = new scarl_ctx();
+  c->device = device;
+  if (budget_bytes == 0) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    budget_bytes = fr / 10 * 9;
+  }
+  c->budget = budget_bytes;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return SCARL_EDEVICE;
+  }
+  c->own_stream = true;
+  *out = c;
+  return SCARL_OK;
+}
+
+int scarl_ctx_destroy(scarl_ctx* ctx) {
+  if (!ctx) return SCARL_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  flush_marks(ctx);
+  for (Buf* b : {&ctx->work, &ctx->tile, &ctx->stage_out, &ctx->stage_in, &ctx->stage_in2,
+                 &ctx->tabs, &ctx->dtabs, &ctx->part, &ctx->t1, &ctx->t2, &ctx->sk, &ctx->pmpw})
+    release(ctx, *b);
+  for (auto& kv : ctx->plans) release(ctx, kv.second.tabs);
+  for (auto& kv : ctx->twiddles) release(ctx, kv.second);
+  for (auto& kv : ctx->dct_tabs) release(ctx, kv.second);
+  for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
+  if (ctx->pin_ev) cudaEventDestroy(ctx->pin_ev);
+  if (ctx->pin) cudaFreeHost(ctx->pin);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return SCARL_OK;
+}
+
+const char* scarl_last_error(const scarl_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int scarl_ctx_set_stream(scarl_ctx* ctx, void* s) {
+  RC(begin(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  if (s) {
+    ctx->stream = (cudaStream_t)s;
+    ctx->own_stream = false;
+  } else {
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  return SCARL_OK;
+}
+
+int scarl_sync(scarl_ctx* ctx) {
+  RC(begin(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  return SCARL_OK;
+}
+
+int scarl_counters(scarl_ctx* ctx, long long* launches, unsigned long long* h2d_bytes,
+                   unsigned long long* d2h_bytes) {
+  if (!ctx) return SCARL_EINVAL;
+  if (launches) *launches = ctx->launches;
+  if (h2d_bytes) *h2d_bytes = ctx->h2d;
+  if (d2h_bytes) *d2h_bytes = ctx->d2h;
+  return SCARL_OK;
+}
+
+int scarl_profile(scarl_ctx* ctx, int enable) {
+  RC(begin(ctx));
+  flush_marks(ctx);
+  if (enable == 2) {  // reset
+    ctx->pstats.clear();
+    ctx->porder.clear();
+    return SCARL_OK;
+  }
+  ctx->profile = enable != 0;
+  return SCARL_OK;
+}
+
+int scarl_profile_read(scarl_ctx* ctx, int idx, char* name, size_t name_len, double* total_ms,
+                       long long* launches) {
+  RC(begin(ctx));
+  flush_marks(ctx);
+  if (idx < 0 || idx >= (int)ctx->porder.size()) return SCARL_EINVAL;
+  const std::string& k = ctx->porder[idx];
+  if (name && name_len) std::snprintf(name, name_len, "%s", k.c_str());
+  if (total_ms) *total_ms = ctx->pstats[k].first;
+  if (launches) *launches = ctx->pstats[k].second;
+  return SCARL_OK;
+}
+
+// ---- host-only ----
+int scarl_verify_inputs(const scarl_sample* s, int gen_meth, char* msg, size_t len) {
+  if (!s) return SCARL_EINVAL;
+  return verify_inputs(s, gen_meth, msg, len);
+}
+
+int scarl_decide_topo_shape(int nb_procs, const int L[3], const int Np_ovlp[3],
+                            long long ppbi, int topo[3]) {
+  if (nb_procs < 1 || !L || !Np_ovlp || !topo) return SCARL_EINVAL;
+  decide_topo_shape(nb_procs, L, Np_ovlp, ppbi, topo);
+  return SCARL_OK;
+}
+
+int scarl_get_topo_pos(int rank, const int shape[3], int pos[3]) {
+  if (!shape || !pos || shape[0] < 1 || shape[1] < 1 || shape[2] < 1) return SCARL_EINVAL;
+  get_topo_pos(rank, shape, pos);
+  return SCARL_OK;
+}
+
+int scarl_get_topo_rank(const int shape[3], const int pos[3]) {
+  if (!shape || !pos) return -1;
+  return get_topo_rank(shape, pos);
+}
+
+int scarl_sample_layout(const scarl_sample* s, int gen_meth, int nb_procs, const int* topo_in,
+                        scarl_layout* out) {
+  if (!s || !out) return SCARL_EINVAL;
+  return sample_layout(s, gen_meth, nb_procs, topo_in, out);
+}
+
+int scarl_tile_geometry(const scarl_layout* lay, const double xMin[3], int rank, scarl_tile* t) {
+  if (!lay || !xMin || !t || rank < 0 || rank >= lay->nb_tiles) return SCARL_EINVAL;
+  tile_geometry(lay, xMin, rank, t);
+  return SCARL_OK;
+}
+
+int scarl_unity_partition_weights(const int Np[3], const int No[3], int partitionType,
+                                  const int pos[3], const int shape[3], double* w) {
+  if (!Np || !No || !pos || !shape || !w) return SCARL_EINVAL;
+  unity_partition_weights(Np, No, partitionType, pos, shape, w);
+  return SCARL_OK;
+}
+
+int scarl_shino_sizes(const int Np[3], const double xRange[3], const double corrL[3],
+                      int sz_c[3], int sz_Sk[3], double delta_k[3]) {
+  if (!Np || !xRange || !corrL || !sz_c || !sz_Sk || !delta_k) return SCARL_EINVAL;
+  shino_sizes(Np, xRange, corrL, sz_c, sz_Sk, delta_k);
+  return SCARL_OK;
+}
+
+int scarl_read_config(const char* path, int* gen_meth, int* c_info_file, int* d_sample,
+                      int* one_file, int* one_hdf_ds, char* input_file, size_t len) {
+  if (!path || !gen_meth || !c_info_file || !d_sample || !one_file || !one_hdf_ds) return SCARL_EINVAL;
+  return read_config(path, gen_meth, c_info_file, d_sample, one_file, one_hdf_ds, input_file, len);
+}
+
+int scarl_read_extra_config(const char* path, int* found, int topo[3]) {
+  if (!path || !found || !topo) return SCARL_EINVAL;
+  return read_extra_config(path, found, topo);
+}
+
+int scarl_read_input(const char* path, char* folder, size_t flen, int* nSamples,
+                     scarl_sample* samples, int max_samples) {
+  if (!path || !nSamples) return SCARL_EINVAL;
+  return read_input(path, folder, flen, nSamples, samples, max_samples);
+}
+
+int scarl_read_input_sem(const char* folder, char* out_folder, size_t flen, int* nSamples,
+                         scarl_sample* samples, int max_samples) {
+  if (!nSamples) return SCARL_EINVAL;
+  return read_input_sem(folder, out_folder, flen, nSamples, samples, max_samples);
+}
+
+int scarl_rebuild_corrL(const double* SkTot, const int L[3], const double xStep[3],
+                        double corrL_out[3]) {
+  if (!SkTot || !L || !xStep || !corrL_out) return SCARL_EINVAL;
+  int off = 0;
+  for (int d = 0; d < 3; ++d) {
+    const int nk = L[d] / 2;
+    if (nk < 1) return SCARL_EINVAL;
+    double s = 0.0;
+    for (int t = 0; t < nk; ++t) s += SkTot[off + t];
+    corrL_out[d] = 2.0 * (s - ((SkTot[off] + SkTot[off + nk - 1]) / 2.0)) * xStep[d];
+    off += nk;
+  }
+  return SCARL_OK;
+}
+
+// ---- generation ----
+int scarl_gen_std_gauss_fft(scarl_ctx* ctx, double* data, const int Np[3], const double xRange[3],
+                            const double corrL[3], int corrMod, int seed, int rank,
+                            const double* phiK, const double* gammaK) {
+  RC(begin(ctx));
+  if (!data || !Np || !xRange || !corrL) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (corrMod != SCARL_CM_GAUSSIAN) return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
+  for (int d = 0; d < 3; ++d)
+    if (Np[d] < 2) return fail(ctx, SCARL_EINVAL, "Np must be >= 2");
+  const size_t n = (size_t)Np[0] * Np[1] * Np[2];
+  const size_t nk = (size_t)(Np[0] / 2) * (Np[1] / 2) * (Np[2] / 2);
+  void* dev;
+  bool host;
+  RC(out_dev(ctx, data, n * 8, &dev, &host));
+  const void *phi = nullptr, *gam = nullptr;
+  RC(in_dev(ctx, ctx->stage_in, phiK, nk * 8, &phi));
+  RC(in_dev(ctx, ctx->stage_in2, gammaK, nk * 8, &gam));
+  RC(dct_tile(ctx, (double*)dev, Np, xRange, corrL, (const double*)phi, (const double*)gam,
+              (uint32_t)((uint32_t)seed + (uint32_t)rank)));
+  return finish_out(ctx, data, dev, n * 8, host);
+}
+
+int scarl_gen_std_gauss_shino_fft(scarl_ctx* ctx, double* data, const int Np[3],
+                                  const double xRange[3], const double corrL[3],
+                                  const int ppcl[3], int corrMod, int seed, int rank) {
+  (void)ppcl;
+  (void)rank;
+  RC(begin(ctx));
+  if (!data || !Np || !xRange || !corrL) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (corrMod != SCARL_CM_GAUSSIAN)
+    return fail(ctx, SCARL_EUNSUPPORTED, "the Shino generator has only the Gaussian model (SRC_F/spectra_ScaRL.f90:119-137 is commented out)");
+  for (int d = 0; d < 3; ++d)
+    if (Np[d] < 2 || !(corrL[d] > 0.0)) return fail(ctx, SCARL_EINVAL, "Np >= 2 and corrL > 0 required");
+  const size_t n = (size_t)Np[0] * Np[1] * Np[2];
+  void* dev;
+  bool host;
+  RC(out_dev(ctx, data, n * 8, &dev, &host));
+  GenArgs a;
+  RC(shino_args(ctx, Np, xRange, corrL, seed, &a));
+  a.epi.mode = 0;
+  a.epi.out = dev;
+  RC(run_passes(ctx, 8, a));
+  return finish_out(ctx, data, dev, n * 8, host);
+}
+
+int scarl_gen_padded(scarl_ctx* ctx, void* out, int dtype, const int Np[3], const int pad[3],
+                     const double xStep[3], const double corrL[3], int corrMod, double nu,
+                     int normalise, uint64_t seed, uint32_t stream, const void* xi) {
+  RC(begin(ctx));
+  if (!out || !Np || !xStep || !corrL) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  if (corrMod < 1 || corrMod > 3) return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
+  if (corrMod == SCARL_CM_VON_KARMAN && !(nu > 0.0)) return fail(ctx, SCARL_EINVAL, "nu must be > 0");
+  int P[3];
+  for (int d = 0; d < 3; ++d) {
+    P[d] = (pad && pad[d] > 0) ? pad[d] : default_pad(Np[d]);
+    if (!(xStep[d] > 0.0) || !(corrL[d] > 0.0)) return fail(ctx, SCARL_EINVAL, "xStep and corrL must be > 0");
+  }
+  RC(check_grid(ctx, P, Np));
+  const size_t n = (size_t)Np[0] * Np[1] * Np[2];
+  void* dev;
+  bool host;
+  RC(out_dev(ctx, out, n * dtype, &dev, &host));
+  PaddedPlan* pl;
+  RC(padded_plan(ctx, dtype, P, xStep, corrL, corrMod, nu, normalise, &pl));
+  GenArgs a;
+  RC(gen_args(ctx, dtype, P, Np, &a));
+  set_plan(&a, pl);
+  a.k0 = (uint32_t)seed;
+  a.k1 = (uint32_t)(seed >> 32);
+  a.stream = stream;
+  if (xi) {
+    const size_t nm = (size_t)a.Hx * P[1] * P[2];
+    RC(in_dev(ctx, ctx->stage_in, xi, nm * 2 * dtype, &a.xi));
+    a.spec = SPEC_INJECT;
+  }
+  a.epi.mode = 0;
+  a.epi.out = dev;
+  RC(run_passes(ctx, dtype, a));
+  return finish_out(ctx, out, dev, n * dtype, host);
+}
+
+int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen_opts* o_in,
+                          void* global) {
+  RC(begin(ctx));
+  if (!s || !global) return fail(ctx, SCARL_EINVAL, "null argument");
+  scarl_gen_opts o;
+  std::memset(&o, 0, sizeof o);
+  if (o_in) o = *o_in;
+  const int gen = o.generator ? o.generator : SCARL_GEN_PADDED;
+  const int dt = o.dtype ? o.dtype : SCARL_F32;
+  if (dt != SCARL_F32 && dt != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  if (gen != SCARL_GEN_PADDED && dt != SCARL_F64)
+    return fail(ctx, SCARL_EUNSUPPORTED, "the reference generators (DCT, Shino) run in FP64 only");
+  char msg[256];
+  if (verify_inputs(s, SCARL_FFT, msg, sizeof msg) != SCARL_OK) return fail(ctx, SCARL_EINVAL, msg);
+  if (gen != SCARL_GEN_PADDED && s->corrMod != SCARL_CM_GAUSSIAN)
+    return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
+  const int nb_procs = o.nb_procs > 0 ? o.nb_procs : 1;
+  const bool topo_given = o.topo_shape[0] > 0 && o.topo_shape[1] > 0 && o.topo_shape[2] > 0;
+  scarl_layout lay;
+  if (sample_layout(s, SCARL_FFT, nb_procs, topo_given ? o.topo_shape : nullptr, &lay) != SCARL_OK)
+    return fail(ctx, SCARL_EINVAL, "ERROR! procs grid dimensions do not agree with the total number of procs");
+  for (int d = 0; d < 3; ++d)
+    if (lay.Np_ovlp[d] < 0) return fail(ctx, SCARL_EUNSUPPORTED, "negative overlap (discontinuous mesh) is not supported");
+  if (lay.nb_tiles > 4096) return fail(ctx, SCARL_EINVAL, "too many tiles");
+  const size_t ng = (size_t)lay.L[0] * lay.L[1] * lay.L[2];
+  void* dev;
+  bool host;
+  RC(out_dev(ctx, global, ng * dt, &dev, &host));
+  if (s->std_dev == 0.0) {  // write_constant_field, SRC_F/main_ScaRL.f90:145-155
+    if (dt == 8) {
+      CK(cudaMemsetAsync(dev, 0, ng * 8, ctx->stream));
+      RC(launch_marginal(8, dev, (int64_t)ng, 1, 0.0, s->avg, ctx->stream) == cudaSuccess ? SCARL_OK : SCARL_EDEVICE);
+    } else {
+      CK(cudaMemsetAsync(dev, 0, ng * 4, ctx->stream));
+      RC(launch_marginal(4, dev, (int64_t)ng, 1, 0.0, s->avg, ctx->stream) == cudaSuccess ? SCARL_OK : SCARL_EDEVICE);
+    }
+    return finish_out(ctx, global, dev, ng * dt, host);
+  }
+  double ms, mmu;
+  RC(marginal_params(ctx, s->margiFirst, s->avg, s->std_dev, &ms, &mmu));
+  std::vector<BlendAxis> axes;
+  RC(upload_blend_tables(ctx, lay, 1, &axes));
+  Epilogue epi;
+  std::memset(&epi, 0, sizeof epi);
+  epi.mode = 1;
+  epi.out = dev;
+  for (int d = 0; d < 3; ++d) epi.L[d] = lay.L[d];
+  epi.marginal = o.normalize_field ? 0 : s->margiFirst;
+  epi.ms = ms;
+  epi.mmu = mmu;
+  epi.apply_pou = 1;
+  const size_t ntile = (size_t)lay.Np[0] * lay.Np[1] * lay.Np[2];
+  const size_t nk = (size_t)(lay.Np[0] / 2) * (lay.Np[1] / 2) * (lay.Np[2] / 2);
+  PaddedPlan* pl = nullptr;
+  int P[3];
+  if (gen == SCARL_GEN_PADDED) {
+    for (int d = 0; d < 3; ++d) P[d] = o.pad[d] > 0 ? o.pad[d] : default_pad(lay.Np[d]);
+    RC(check_grid(ctx, P, lay.Np));
+    for (int d = 0; d < 3; ++d)
+      if (!(s->corrL[d] > 0.0)) return fail(ctx, SCARL_EINVAL, "corrL must be > 0");
+    RC(padded_plan(ctx, dt, P, lay.xStep, s->corrL, s->corrMod, s->nu, !o.no_spectral_normalisation, &pl));
+  }
+  if (gen == SCARL_GEN_DCT) {
+    for (int d = 0; d < 3; ++d)
+      if (lay.Np[d] < 2) return fail(ctx, SCARL_EINVAL, "Np must be >= 2");
+    RC(ensure(ctx, ctx->tile, ntile * 8));
+  }
+  const void* phi_all = nullptr;
+  if (gen == SCARL_GEN_DCT && o.phiK)
+    RC(in_dev(ctx, ctx->stage_in, o.phiK, nk * lay.nb_tiles * 8, &phi_all));
+  for (int r = 0; r < lay.nb_tiles; ++r) {
+    scarl_tile t;
+    tile_geometry(&lay, s->xMinGlob, r, &t);
+    const int32_t seedStart = (int32_t)((uint32_t)s->seedBase + 1u + (uint32_t)r);
+    Epilogue e = epi;
+    for (int d = 0; d < 3; ++d) {
+      e.off[d] = t.pos_0[d] - 1;
+      e.ax[d] = axes[(size_t)r * 3 + d];
+    }
+    if (gen == SCARL_GEN_PADDED) {
+      GenArgs a;
+      RC(gen_args(ctx, dt, P, lay.Np, &a));
+      set_plan(&a, pl);
+      a.k0 = (uint32_t)seedStart;
+      a.k1 = 0;
+      a.stream = o.stream;
+      a.epi = e;
+      RC(run_passes(ctx, dt, a));
+    } else if (gen == SCARL_GEN_SHINO) {
+      GenArgs a;
+      RC(shino_args(ctx, lay.Np, t.xRange, s->corrL, seedStart, &a));
+      a.epi = e;
+      RC(run_passes(ctx, 8, a));
+    } else {
+      const double* phi = phi_all ? (const double*)phi_all + nk * r : nullptr;
+      RC(dct_tile(ctx, (double*)ctx->tile.p, lay.Np, t.xRange, s->corrL, phi, nullptr, (uint32_t)seedStart));
+      Prof p(ctx, "k_blend_tile");
+      CK(launch_blend_tile(8, ctx->tile.p, lay.Np, e, ctx->stream));
+    }
+  }
+  if (o.normalize_field) {
+    double avg, sd;
+    RC(scarl_normalize_field(ctx, dev, dt, (long long)ng, &avg, &sd));
+    Prof p(ctx, "k_marginal");
+    CK(launch_marginal(dt, dev, (int64_t)ng, s->margiFirst, ms, mmu, ctx->stream));
+  }
+  return finish_out(ctx, global, dev, ng * dt, host);
+}
+
+// ---- post steps ----
+int scarl_apply_unity_partition(scarl_ctx* ctx, double* field, const int Np[3],
+                                const int No[3], int partitionType, const int pos[3],
+                                const int shape[3]) {
+  RC(begin(ctx));
+  if (!field || !Np || !No || !pos || !shape) return fail(ctx, SCARL_EINVAL, "null argument");
+  const size_t n = (size_t)Np[0] * Np[1] * Np[2];
+  void* dev;
+  bool host = !is_device_ptr(field);
+  if (host) {
+    RC(ensure(ctx, ctx->stage_out, n * 8));
+    dev = ctx->stage_out.p;
+    CK(cudaMemcpyAsync(dev, field, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h2d += n * 8;
+  } else {
+    dev = field;
+  }
+  const size_t nd = 2 * ((size_t)Np[0] + Np[1] + Np[2]);
+  void* hp;
+  RC(pinned(ctx, nd * 8, &hp));
+  RC(ensure(ctx, ctx->tabs, nd * 8));
+  double* h = (double*)hp;
+  BlendAxis ax[3];
+  size_t od = 0;
+  for (int d = 0; d < 3; ++d) {
+    pou_axis_tables(Np[d], No[d], pos[d], shape[d], partitionType, h + od, h + od + Np[d]);
+    ax[d].lo = (const double*)ctx->tabs.p + od;
+    ax[d].hi = (const double*)ctx->tabs.p + od + Np[d];
+    ax[d].flags = nullptr;
+    od += 2 * (size_t)Np[d];
+  }
+  RC(upload_pinned(ctx, ctx->tabs.p, nd * 8));
+  {
+    Prof p(ctx, "k_apply_pou");
+    CK(launch_apply_pou(8, dev, Np, ax, ctx->stream));
+  }
+  return finish_out(ctx, field, dev, n * 8, host);
+}
+
+int scarl_add_overlap(scarl_ctx* ctx, double* tiles, const int Np[3], const int No[3],
+                      const int shape[3]) {
+  RC(begin(ctx));
+  if (!tiles || !Np || !No || !shape) return fail(ctx, SCARL_EINVAL, "null argument");
+  for (int d = 0; d < 3; ++d)
+    if (shape[d] < 1 || No[d] > Np[d] || No[d] < 0) return fail(ctx, SCARL_EINVAL, "invalid topology or overlap");
+  const size_t n = (size_t)Np[0] * Np[1] * Np[2] * shape[0] * shape[1] * shape[2];
+  RC(ensure(ctx, ctx->tile, n * 8));
+  void* dev;
+  bool host = !is_device_ptr(tiles);
+  if (host) {
+    RC(ensure(ctx, ctx->stage_out, n * 8));
+    dev = ctx->stage_out.p;
+    CK(cudaMemcpyAsync(dev, tiles, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    dev = tiles;
+  }
+  CK(cudaMemcpyAsync(ctx->tile.p, dev, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  {
+    Prof p(ctx, "k_add_overlap");
+    CK(launch_add_overlap((const double*)ctx->tile.p, (double*)dev, Np, No, shape, ctx->stream));
+  }
+  return finish_out(ctx, tiles, dev, n * 8, host);
+}
+
+int scarl_multivariate_transformation(scarl_ctx* ctx, void* field, int dtype, long long n,
+                                      double avg, double std_dev, int margiFirst) {
+  RC(begin(ctx));
+  if (!field || n < 0) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  double ms, mu;
+  RC(marginal_params(ctx, margiFirst, avg, std_dev, &ms, &mu));
+  void* dev;
+  bool host = !is_device_ptr(field);
+  if (host) {
+    RC(ensure(ctx, ctx->stage_out, (size_t)n * dtype));
+    dev = ctx->stage_out.p;
+    CK(cudaMemcpyAsync(dev, field, (size_t)n * dtype, cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    dev = field;
+  }
+  {
+    Prof p(ctx, "k_marginal");
+    CK(launch_marginal(dtype, dev, n, margiFirst, ms, mu, ctx->stream));
+  }
+  return finish_out(ctx, field, dev, (size_t)n * dtype, host);
+}
+
+static int sums(scarl_ctx* ctx, const void* dev, int dtype, long long xN, int nmc,
+                std::vector<double>* s, std::vector<double>* s2) {
+  const int nb = sums_blocks(xN);
+  RC(ensure(ctx, ctx->part, (size_t)nb * nmc * 2 * 8));
+  {
+    Prof p(ctx, "k_sums");
+    CK(launch_sums(dtype, dev, xN, nmc, (double*)ctx->part.p, nb, ctx->stream));
+  }
+  std::vector<double> h((size_t)nb * nmc * 2);
+  CK(cudaMemcpyAsync(h.data(), ctx->part.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  s->assign(nmc, 0.0);
+  s2->assign(nmc, 0.0);
+  for (int e = 0; e < nmc; ++e)
+    for (int b = 0; b < nb; ++b) {
+      (*s)[e] += h[((size_t)e * nb + b) * 2];
+      (*s2)[e] += h[((size_t)e * nb + b) * 2 + 1];
+    }
+  return SCARL_OK;
+}
+
+int scarl_normalize_field(scarl_ctx* ctx, void* field, int dtype, long long n, double* avg,
+                          double* sd) {
+  RC(begin(ctx));
+  if (!field || n <= 0) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  void* dev;
+  bool host = !is_device_ptr(field);
+  if (host) {
+    RC(ensure(ctx, ctx->stage_out, (size_t)n * dtype));
+    dev = ctx->stage_out.p;
+    CK(cudaMemcpyAsync(dev, field, (size_t)n * dtype, cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    dev = field;
+  }
+  std::vector<double> s, s2;
+  RC(sums(ctx, dev, dtype, n, 1, &s, &s2));
+  const double a = s[0] / (double)n;
+  {
+    Prof p(ctx, "k_affine");
+    CK(launch_affine(dtype, dev, n, a, 1.0, ctx->stream));
+  }
+  RC(sums(ctx, dev, dtype, n, 1, &s, &s2));
+  const double sdv = std::sqrt(s2[0] / (double)n);
+  {
+    Prof p(ctx, "k_affine");
+    CK(launch_affine(dtype, dev, n, 0.0, sdv, ctx->stream));
+  }
+  if (avg) *avg = a;
+  if (sd) *sd = sdv;
+  return finish_out(ctx, field, dev, (size_t)n * dtype, host);
+}
+
+// ---- estimators ----
+int scarl_moments(scarl_ctx* ctx, const void* field, int dtype, long long xN, int nmc,
+                  double* evntAvg, double* evntStd, double* gAvg, double* gStd) {
+  RC(begin(ctx));
+  if (!field || xN <= 0 || nmc <= 0) return fail(ctx, SCARL_EINVAL, "invalid argument");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  const void* dev;
+  RC(in_dev(ctx, ctx->stage_in, field, (size_t)xN * nmc * dtype, &dev));
+  std::vector<double> s, s2;
+  RC(sums(ctx, dev, dtype, xN, nmc, &s, &s2));
+  double S = 0.0, S2 = 0.0;
+  for (int e = 0; e < nmc; ++e) {
+    const double a = s[e] / (double)xN;
+    if (evntAvg) evntAvg[e] = a;
+    if (evntStd) evntStd[e] = std::sqrt(s2[e] / (double)xN - a * a);
+    S += s[e];
+    S2 += s2[e];
+  }
+  const double ga = S / (double)(xN * nmc);
+  if (gAvg) *gAvg = ga;
+  if (gStd) *gStd = std::sqrt(S2 / (double)(xN * nmc) - ga * ga);
+  return SCARL_OK;
+}
+
+int scarl_rebuild_sk(scarl_ctx* ctx, const void* field, int dtype, const int L[3], double avg,
+                     double stdDev, int tukey_literal, double* SkTot) {
+  RC(begin(ctx));
+  if (!field || !L || !SkTot) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  for (int d = 0; d < 3; ++d)
+    if (L[d] < 2 || L[d] > 4096) return fail(ctx, SCARL_EUNSUPPORTED, "line length must be in [2, 4096]");
+  if (!(stdDev > 0.0)) return fail(ctx, SCARL_EINVAL, "stdDev must be > 0");
+  const size_t n = (size_t)L[0] * L[1] * L[2];
+  const void* dev;
+  RC(in_dev(ctx, ctx->stage_in, field, n * dtype, &dev));
+  const double r = (double)0.1f;  // SRC_F/Stat_ScaRL/statistics_RF.f90:277
+  int off = 0;
+  for (int d = 0; d < 3; ++d) {
+    const int nl = L[d];
+    const int nkeep = nl / 2;
+    std::vector<double> w(nl);
+    for (int i = 0; i < nl; ++i) {  // statistics_RF.f90:325-351
+      const double ratio = (double)i / (double)(nl - 1);
+      w[i] = 1.0;
+      if (tukey_literal) {
+        if (ratio < r) w[i] = 1.0 / 2.0 * (1 + std::cos(2.0 * kPiRef / r * (ratio - r / 2.0)));
+        else if (ratio > r) w[i] = 1.0 / 2.0 * (1 + std::cos(2.0 * kPiRef / r * (ratio - 1.0 + r / 2.0)));
+      } else {
+        if (ratio < r / 2.0) w[i] = 1.0 / 2.0 * (1 + std::cos(2.0 * M_PI / r * (ratio - r / 2.0)));
+        else if (ratio > 1.0 - r / 2.0) w[i] = 1.0 / 2.0 * (1 + std::cos(2.0 * M_PI / r * (ratio - 1.0 + r / 2.0)));
+      }
+    }
+    void* hp;
+    RC(pinned(ctx, (size_t)nl * 8, &hp));
+    std::memcpy(hp, w.data(), (size_t)nl * 8);
+    RC(ensure(ctx, ctx->tabs, (size_t)nl * 8));
+    RC(upload_pinned(ctx, ctx->tabs.p, (size_t)nl * 8));
+    const int np = lag_cov_parts(L, d);
+    RC(ensure(ctx, ctx->part, (size_t)np * std::max(nkeep, 1) * 8));
+    {
+      Prof p(ctx, "k_lag_cov");
+      CK(launch_lag_cov(dtype, dev, L, d, avg, stdDev, (const double*)ctx->tabs.p, nkeep,
+                        (double*)ctx->part.p, np, ctx->stream));
+    }
+    std::vector<double> h((size_t)np * nkeep);
+    CK(cudaMemcpyAsync(h.data(), ctx->part.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double nlines = (double)(n / (size_t)nl);
+    for (int m = 0; m < nkeep; ++m) {
+      double s = 0.0;
+      for (int b = 0; b < np; ++b) s += h[(size_t)b * nkeep + m];
+      SkTot[off + m] = s / ((double)nl * nlines);
+    }
+    off += nkeep;
+  }
+  return SCARL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,324 @@
+// gen_padded.cu -- the padded periodic-grid generator (the spectral method of
+// SRC_F/fftw_ScaRL.f90:157-255 with SRC_F/spectra_ScaRL.f90:10-142, made
+// Hermitian/C2R), as three HBM passes over a complex half spectrum
+// H[kx in 0..P0/2][ky][kz] of the tile's padded grid P:
+//
+//   pass 1  k_gen_z : synthesise H line by line along kz (amplitude x random
+//                     normals, no read from memory), inverse DFT along z,
+//                     keep z < Nz.  Output kx-fastest rows of pitch Hpad.
+//   pass 2  k_mid_y : inverse DFT along y for every (kx, z < Nz), keep
+//                     y < Ny, in place.
+//   pass 3  k_c2r_x : Hermitian C2R along x for every (y, z) line (one
+//                     half-length complex DFT plus the even/odd split), keep
+//                     x < Nx, then the fused epilogue: plain crop, or the
+//                     partition-of-unity blend into the global field with the
+//                     marginal transform applied by the tile that finishes a
+//                     point (SRC_F/main_ScaRL.f90:1216-1301, 984-1210,
+//                     1355-1395).
+#include "epilogue.cuh"
+#include "fft_engine.cuh"
+#include "scarl_internal.h"
+
+namespace scarl {
+
+constexpr double kPiRef = 3.1415926535898;  // SRC_F/constants_ScaRL.f90:5
+
+// ---------------------------------------------------------------------------
+// Literal build_Sk_mtx value at padded coordinate (kx, ky, kz), halved for
+// the C2R form (Re of the c2c = C2R with H = Sk/2 on kx >= 1).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int shino_index(int c, int P, int sz) {
+  if (c < sz) return c;
+  if (c >= P - sz) return c - (P - 2 * sz);
+  return -1;
+}
+
+template <typename T>
+__device__ __forceinline__ cplx_t<T> shino_mode(const GenArgs& a, int kx, int ky, int kz) {
+  const int n1 = a.sz[0], n2 = 2 * a.sz[1], n3 = 2 * a.sz[2];
+  const int i0 = kx;
+  const int j0 = shino_index(ky, a.P[1], a.sz[1]);
+  const int k0 = shino_index(kz, a.P[2], a.sz[2]);
+  if (i0 < 1 || i0 >= n1 || j0 <= 0 || k0 <= 0 || j0 >= n2 - 1 || k0 >= n3 - 1) return mk(T(0), T(0));
+  const uint64_t e = (uint64_t)i0 + (uint64_t)n1 * ((uint64_t)j0 + (uint64_t)n2 * (uint64_t)k0);
+  const uint32_t s = pm_jump(a.pm_s1, e, a.pm_pw);
+  const double u = (double)(int32_t)s * 4.656612875E-10;
+  const double ph = __dmul_rn(__dmul_rn(2.0, kPiRef), u);
+  const double c = (double)(float)cos(ph);
+  const double sn = (double)(float)sin(ph);
+  const double bi = (double)i0;
+  const double bj = (double)(j0 < a.sz[1] ? j0 : n2 - 1 - j0);
+  const double bk = (double)(k0 < a.sz[2] ? k0 : n3 - 1 - k0);
+  const double arg = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(bi, bi), a.de[0]),
+                                         __dmul_rn(__dmul_rn(bj, bj), a.de[1])),
+                               __dmul_rn(__dmul_rn(bk, bk), a.de[2]));
+  const double sv = sqrt(exp(-arg));
+  const double re = __dmul_rn(__dmul_rn(__dmul_rn(c, sv), a.shino_scale), a.shino_f);
+  const double im = __dmul_rn(__dmul_rn(__dmul_rn(sn, sv), a.shino_scale), a.shino_f);
+  return mk((T)(0.5 * re), (T)(0.5 * im));
+}
+
+template <typename T> __device__ __forceinline__ T powT(T s, T e);
+template <> __device__ __forceinline__ float powT<float>(float s, float e) { return __powf(s, e); }
+template <> __device__ __forceinline__ double powT<double>(double s, double e) { return pow(s, e); }
+
+// ---------------------------------------------------------------------------
+// Pass 1: synthesise + inverse DFT along z.
+// ---------------------------------------------------------------------------
+template <typename T, int N, int E, int B, int SPEC>
+__global__ void __launch_bounds__(B*(N / E)) k_gen_z(const GenArgs a) {
+  using C = cplx_t<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int b = threadIdx.x % B, t = threadIdx.x / B;
+  const int kx = blockIdx.x * B + b;
+  const int ky = blockIdx.y;
+  const bool valid = kx < a.Hx;
+  C* work = static_cast<C*>(a.work);
+  const T* ax = static_cast<const T*>(a.ax);
+  const T* ay = static_cast<const T*>(a.ay);
+  const T* az = static_cast<const T*>(a.az);
+  const T* qx = static_cast<const T*>(a.qx);
+  const T* qy = static_cast<const T*>(a.qy);
+  const T* qz = static_cast<const T*>(a.qz);
+  T fx = T(0), fy = T(0);
+  if constexpr (SPEC != SPEC_SHINO) {
+    if (valid) {
+      if (a.amp == AMP_SEPARABLE) { fx = ax[kx]; fy = ay[ky]; }
+      else { fx = ax[kx]; fy = T(1) + qx[kx] + qy[ky]; }
+    }
+  }
+  const uint64_t mrow = (uint64_t)kx + (uint64_t)a.Hx * (uint64_t)ky;
+  const uint64_t mz = (uint64_t)a.Hx * (uint64_t)a.P[1];
+  auto load = [&](int kz) -> C {
+    if (!valid) return mk(T(0), T(0));
+    if constexpr (SPEC == SPEC_SHINO) {
+      return shino_mode<T>(a, kx, ky, kz);
+    } else {
+      T A;
+      if (a.amp == AMP_SEPARABLE) A = fx * fy * az[kz];
+      else if (a.amp == AMP_RECIP) A = fx / (fy + qz[kz]);
+      else A = fx * powT<T>(fy + qz[kz], (T)a.expo);
+      const uint64_t m = mrow + mz * (uint64_t)kz;
+      C xi;
+      if constexpr (SPEC == SPEC_INJECT) xi = static_cast<const C*>(a.xi)[m];
+      else xi = Normals<T>::pair(m, a.stream, a.k0, a.k1);
+      return mk(A * xi.x, A * xi.y);
+    }
+  };
+  const int Nz = a.Nout[2];
+  auto store = [&](int z, C v) {
+    if (valid && z < Nz) work[((size_t)z * a.P[1] + ky) * a.Hpad + kx] = v;
+  };
+  line_ifft<C, N, E, SmemOrder::BatchFast, B, 0>(sm, b, t, static_cast<const C*>(a.tw_z), 1, load,
+                                                 store);
+}
+
+// ---------------------------------------------------------------------------
+// Pass 2: inverse DFT along y, in place, keep y < Ny.
+// ---------------------------------------------------------------------------
+template <typename T, int N, int E, int B>
+__global__ void __launch_bounds__(B*(N / E)) k_mid_y(const GenArgs a) {
+  using C = cplx_t<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int b = threadIdx.x % B, t = threadIdx.x / B;
+  const int kx = blockIdx.x * B + b;
+  const int z = blockIdx.y;
+  const bool valid = kx < a.Hx;
+  C* col = static_cast<C*>(a.work) + (size_t)z * a.P[1] * a.Hpad + kx;
+  const size_t pitch = (size_t)a.Hpad;
+  const int Ny = a.Nout[1];
+  auto load = [&](int ky) -> C { return valid ? col[(size_t)ky * pitch] : mk(T(0), T(0)); };
+  auto store = [&](int y, C v) {
+    if (valid && y < Ny) col[(size_t)y * pitch] = v;
+  };
+  line_ifft<C, N, E, SmemOrder::BatchFast, B, 0>(sm, b, t, static_cast<const C*>(a.tw_y), 1, load,
+                                                 store);
+}
+
+// ---------------------------------------------------------------------------
+// Pass 3: Hermitian C2R along x (complex length N = P0/2), crop, epilogue.
+// ---------------------------------------------------------------------------
+template <typename T, int N, int E, int B>
+__global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
+  using C = cplx_t<T>;
+  constexpr int TPL = N / E;
+  constexpr int LS = N + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int Nx = a.Nout[0], Ny = a.Nout[1], Nz = a.Nout[2];
+  const int64_t nlines = (int64_t)Ny * Nz;
+  const C* work = static_cast<const C*>(a.work);
+  for (int idx = threadIdx.x; idx < B * LS; idx += blockDim.x) {
+    const int bb = idx / LS, k = idx - bb * LS;
+    const int64_t l = (int64_t)blockIdx.x * B + bb;
+    C v = mk(T(0), T(0));
+    if (l < nlines) {
+      const int64_t y = l % Ny, z = l / Ny;
+      v = work[((size_t)z * a.P[1] + (size_t)y) * a.Hpad + k];
+    }
+    sm[bb * LS + k] = v;
+  }
+  __syncthreads();
+  const int b = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  const int64_t l = (int64_t)blockIdx.x * B + b;
+  const bool valid = l < nlines;
+  const int y = valid ? (int)(l % Ny) : 0, z = valid ? (int)(l / Ny) : 0;
+  const C* twx = static_cast<const C*>(a.tw_x);
+  const C* line = sm + b * LS;
+  auto load = [&](int k) -> C {
+    const C xk = line[k], xn = line[N - k];
+    if (k == 0) return mk(xk.x + xn.x, xk.x - xn.x);
+    const C xc = cconj(xn);
+    const C e = cadd(xk, xc);
+    const C o = cmul(csub(xk, xc), __ldg(twx + k));
+    return mk(e.x - o.y, e.y + o.x);
+  };
+  auto store = [&](int n, C v) {
+    if (!valid) return;
+    const int x0 = 2 * n;
+    if (x0 < Nx) epilogue_point<T>(a.epi, x0, y, z, Nx, Ny, v.x);
+    if (x0 + 1 < Nx) epilogue_point<T>(a.epi, x0 + 1, y, z, Nx, Ny, v.y);
+  };
+  line_ifft<C, N, E, SmemOrder::LineFast, B, LS>(sm, b, t, twx, 2, load, store);
+}
+
+// ---------------------------------------------------------------------------
+// Launch configuration: values per thread E and lines per block B.
+// ---------------------------------------------------------------------------
+template <typename T, int N> struct ColCfg {  // passes 1 and 2
+  static constexpr int E = (N >= 16) ? 16 : N;
+  static constexpr int B = sizeof(T) == 4 ? (N <= 256 ? 16 : (N <= 1024 ? 8 : 4))
+                                          : (N <= 256 ? 8 : 4);
+};
+template <typename T, int N> struct RowCfg {  // pass 3 (N = P0/2)
+  static constexpr int E = (N >= 16) ? 16 : N;
+  static constexpr int B = (N <= 512) ? 8 : 4;
+};
+
+template <typename K>
+static cudaError_t launch_k(K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                           const GenArgs& a) {
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  kernel<<<grid, block, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int N>
+static cudaError_t run_gen_z(const GenArgs& a, cudaStream_t s) {
+  using Cf = ColCfg<T, N>;
+  dim3 grid((a.Hx + Cf::B - 1) / Cf::B, a.P[1], 1);
+  dim3 block(Cf::B * (N / Cf::E));
+  size_t smem = (size_t)Cf::B * N * sizeof(cplx_t<T>);
+  switch (a.spec) {
+    case SPEC_PHILOX: return launch_k(k_gen_z<T, N, Cf::E, Cf::B, SPEC_PHILOX>, grid, block, smem, s, a);
+    case SPEC_INJECT: return launch_k(k_gen_z<T, N, Cf::E, Cf::B, SPEC_INJECT>, grid, block, smem, s, a);
+    case SPEC_SHINO: return launch_k(k_gen_z<T, N, Cf::E, Cf::B, SPEC_SHINO>, grid, block, smem, s, a);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T, int N>
+static cudaError_t run_mid_y(const GenArgs& a, cudaStream_t s) {
+  using Cf = ColCfg<T, N>;
+  dim3 grid((a.Hx + Cf::B - 1) / Cf::B, a.Nout[2], 1);
+  dim3 block(Cf::B * (N / Cf::E));
+  size_t smem = (size_t)Cf::B * N * sizeof(cplx_t<T>);
+  return launch_k(k_mid_y<T, N, Cf::E, Cf::B>, grid, block, smem, s, a);
+}
+
+template <typename T, int N>
+static cudaError_t run_c2r_x(const GenArgs& a, cudaStream_t s) {
+  using Cf = RowCfg<T, N>;
+  const int64_t nlines = (int64_t)a.Nout[1] * a.Nout[2];
+  dim3 grid((unsigned)((nlines + Cf::B - 1) / Cf::B), 1, 1);
+  dim3 block(Cf::B * (N / Cf::E));
+  size_t smem = (size_t)Cf::B * (N + 1) * sizeof(cplx_t<T>);
+  return launch_k(k_c2r_x<T, N, Cf::E, Cf::B>, grid, block, smem, s, a);
+}
+
+#define SCARL_DISPATCH_N(N_, FN, T_, ...)                   \
+  switch (N_) {                                             \
+    case 4: return FN<T_, 4>(__VA_ARGS__);                  \
+    case 8: return FN<T_, 8>(__VA_ARGS__);                  \
+    case 16: return FN<T_, 16>(__VA_ARGS__);                \
+    case 32: return FN<T_, 32>(__VA_ARGS__);                \
+    case 64: return FN<T_, 64>(__VA_ARGS__);                \
+    case 128: return FN<T_, 128>(__VA_ARGS__);              \
+    case 256: return FN<T_, 256>(__VA_ARGS__);              \
+    case 512: return FN<T_, 512>(__VA_ARGS__);              \
+    case 1024: return FN<T_, 1024>(__VA_ARGS__);            \
+    case 2048: return FN<T_, 2048>(__VA_ARGS__);            \
+    default: return cudaErrorInvalidValue;                  \
+  }
+
+template <typename T> static cudaError_t gen_z_t(const GenArgs& a, cudaStream_t s) {
+  SCARL_DISPATCH_N(a.P[2], run_gen_z, T, a, s)
+}
+template <typename T> static cudaError_t mid_y_t(const GenArgs& a, cudaStream_t s) {
+  SCARL_DISPATCH_N(a.P[1], run_mid_y, T, a, s)
+}
+template <typename T> static cudaError_t c2r_x_t(const GenArgs& a, cudaStream_t s) {
+  SCARL_DISPATCH_N(a.P[0] / 2, run_c2r_x, T, a, s)
+}
+
+cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a, cudaStream_t s) {
+  if (pass == 1) return dt == 8 ? gen_z_t<double>(a, s) : gen_z_t<float>(a, s);
+  if (pass == 2) return dt == 8 ? mid_y_t<double>(a, s) : mid_y_t<float>(a, s);
+  if (pass == 3) return dt == 8 ? c2r_x_t<double>(a, s) : c2r_x_t<float>(a, s);
+  return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 spectral variance-normalisation sum over the full periodic grid.
+// ---------------------------------------------------------------------------
+constexpr int kSumThreads = 256;
+int spectrum_sum_blocks() { return 148 * 8; }
+
+__global__ void __launch_bounds__(kSumThreads) k_spec_sum(const GenArgs a, const double* rx,
+                                                          const double* ry, const double* rz,
+                                                          double craw2, double* partial) {
+  const double* qx = static_cast<const double*>(a.qx);
+  const double* qy = static_cast<const double*>(a.qy);
+  const double* qz = static_cast<const double*>(a.qz);
+  const int64_t total = (int64_t)a.Hx * a.P[1] * a.P[2];
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(i % a.Hx);
+    const int64_t r = i / a.Hx;
+    const int ky = (int)(r % a.P[1]);
+    const int kz = (int)(r / a.P[1]);
+    const double c = (kx == 0 || 2 * kx == a.P[0]) ? 1.0 : 2.0;
+    double v;
+    if (a.amp == AMP_SEPARABLE) {
+      const double A = rx[kx] * ry[ky] * rz[kz];
+      v = A * A;
+    } else {
+      v = craw2 * pow(1.0 + qx[kx] + qy[ky] + qz[kz], 2.0 * a.expo);
+    }
+    acc += c * v;
+  }
+  __shared__ double red[kSumThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < kSumThreads / 32 ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+  }
+}
+
+cudaError_t launch_spectrum_sum(const GenArgs& a, const double* rx, const double* ry,
+                                const double* rz, double craw2, double* partial, int nblocks,
+                                cudaStream_t s) {
+  k_spec_sum<<<nblocks, kSumThreads, 0, s>>>(a, rx, ry, rz, craw2, partial);
+  return cudaGetLastError();
+}
+
+}  // namespace scarl

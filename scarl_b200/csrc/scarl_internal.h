@@ -1,0 +1,125 @@
+// scarl_internal.h -- kernel argument blocks and launcher declarations shared
+// between the CUDA translation units and the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace scarl {
+
+// Per-axis blend tables for one tile (device pointers, Np[d] entries each).
+//   lo/hi : partition-of-unity factors of the low / high side (1.0 where the
+//           side has no neighbour), multiplied low x,y,z then high x,y,z.
+//   flags : bit0 = the tile contributes the point along this axis,
+//           bit1 = first contributor, bit2 = last contributor.
+struct BlendAxis {
+  const double* lo;
+  const double* hi;
+  const uint8_t* flags;
+};
+
+struct Epilogue {
+  int mode;            // 0 = plain crop, 1 = blend into a global field
+  void* out;           // plain: Nx*Ny*Nz tile; blend: L0*L1*L2 global field
+  int64_t L[3];        // global extent (blend)
+  int64_t off[3];      // tile origin in the global field (blend)
+  BlendAxis ax[3];
+  int marginal;        // 0 none, 1 Gaussian (x*s+mu), 2 lognormal exp(x*s+mu)
+  double ms, mmu;
+  int apply_pou;
+};
+
+// Spectrum synthesis for the padded periodic grid.
+enum SpecMode : int {
+  SPEC_PHILOX = 0,  // canonical Philox normals times amplitude
+  SPEC_INJECT = 1,  // caller-supplied normal pairs times amplitude
+  SPEC_SHINO = 2,   // build_Sk_mtx phases (Park-Miller) and amplitude, literal
+};
+enum AmpKind : int {
+  AMP_SEPARABLE = 0,  // A = ax[kx] * ay[ky] * az[kz]
+  AMP_RECIP = 1,      // A = ax[kx] / (1 + qx + qy + qz)
+  AMP_POW = 2,        // A = ax[kx] * (1 + qx + qy + qz)^expo
+};
+
+struct GenArgs {
+  int P[3];
+  int Hx, Hpad;
+  int Nout[3];
+  void* work;            // complex intermediate, Hpad * P1 * Nout2 entries
+  const void* tw_z;      // e^{2 pi i m / P2}
+  const void* tw_y;      // e^{2 pi i m / P1}
+  const void* tw_x;      // e^{2 pi i m / P0}
+  // spectrum
+  int spec;              // SpecMode
+  int amp;               // AmpKind
+  const void* ax;        // separable: amplitude factors; Matern: g(kx)/sqrt(norm) prefactor
+  const void* ay;
+  const void* az;
+  const void* qx;        // Matern: 4 pi^2 a_d^2 f_d^2 per axis
+  const void* qy;
+  const void* qz;
+  double expo;           // Matern: -(nu + 3/2) / 2
+  uint32_t k0, k1, stream;
+  const void* xi;        // injected normal pairs (SPEC_INJECT)
+  // literal Shino spectrum (FP64 tables)
+  int sz[3];
+  uint32_t pm_s1;        // Park-Miller state after the first step
+  const uint32_t* pm_pw; // 16807^(2^b) mod (2^31-1)
+  double de[3];          // (PI^2/2) delta_k^2
+  double shino_scale;    // sqrt(8) and 2 sqrt(prod delta_k) applied in order
+  double shino_f;
+  Epilogue epi;
+};
+
+// Launchers (return cudaSuccess or the launch error).  dt: 4 = FP32, 8 = FP64.
+// pass: 1 = synthesis + z, 2 = y, 3 = C2R x + epilogue.
+cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a, cudaStream_t s);
+// FP64 sum over the full periodic grid of S(k) dk^3: separable tables r*
+// (A_raw = rx ry rz) or Matern q tables with A_raw^2 = craw2 (1+q)^(2 expo).
+cudaError_t launch_spectrum_sum(const GenArgs& a, const double* rx, const double* ry,
+                                const double* rz, double craw2, double* partial, int nblocks,
+                                cudaStream_t s);
+int spectrum_sum_blocks();
+
+// Literal DCT-III path (FP64).
+struct DctArgs {
+  int Np[3];
+  int K[3];
+  const double* cx;  // per-axis corrL * exp(-PI k^2) factors, order of the reference
+  const double* cy;
+  const double* cz;
+  double corrL[3];
+  const double* phi;    // injected phases (K0*K1*K2) or null (Philox uniforms)
+  const double* gamma;  // injected amplitudes or null (1)
+  uint32_t k0, k1, stream;
+  double* sk;           // K0*K1*K2 spectrum
+  double* t1;           // N0*K1*K2
+  double* t2;           // N0*N1*K2
+  double* out;          // N0*N1*N2
+  const double* ctab[3];  // 2*cos(pi m / (2 N)) (and 1 at i = 0), m < 4N
+};
+cudaError_t launch_dct_literal(const DctArgs& a, cudaStream_t s);
+
+// Post steps.
+cudaError_t launch_blend_tile(int dt, const void* tile, const int Np[3], const Epilogue& e,
+                              cudaStream_t s);
+cudaError_t launch_apply_pou(int dt, void* field, const int Np[3], const BlendAxis ax[3],
+                             cudaStream_t s);
+cudaError_t launch_add_overlap(const double* in, double* out, const int Np[3],
+                               const int Np_ovlp[3], const int topo[3], cudaStream_t s);
+cudaError_t launch_marginal(int dt, void* f, int64_t n, int kind, double sc, double mu,
+                            cudaStream_t s);
+cudaError_t launch_affine(int dt, void* f, int64_t n, double sub, double div, cudaStream_t s);
+// FP64 sums of x and x^2 over nmc blocks of xN values; partial has
+// nmc * nb * 2 doubles.
+cudaError_t launch_sums(int dt, const void* f, int64_t xN, int nmc, double* partial, int nb,
+                        cudaStream_t s);
+int sums_blocks(int64_t xN);
+
+// Directional circular autocovariance of the standardised, windowed field.
+cudaError_t launch_lag_cov(int dt, const void* f, const int L[3], int dir, double avg,
+                           double sd, const double* win, int nkeep, double* partial, int nparts,
+                           cudaStream_t s);
+int lag_cov_parts(const int L[3], int dir);
+
+}  // namespace scarl

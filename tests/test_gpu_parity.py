@@ -1,0 +1,298 @@
+"""CUDA path (through the C ABI) against the CPU oracle and the golden
+fixtures.  Tolerances: FP64 fields rel-L2 <= 1e-12; FP32 fields rel-L2 <=
+1e-5 against FP64; weights, overlap sums and index maps bit-exact."""
+import os
+
+import numpy as np
+import pytest
+
+import scarl_b200 as S
+
+pytestmark = pytest.mark.gpu
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden.npz"))
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+# ---------------------------------------------------------------------------
+# padded periodic generator
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("tag", ["g", "e", "v"])
+@pytest.mark.parametrize("dtype,tol", [(S.F64, TOL64), (S.F32, TOL32)])
+def test_gen_padded_injected_golden(ctx, tag, dtype, tol):
+    xi = GOLD[f"pad_{tag}_xi"]
+    if dtype == S.F32:
+        xi = xi.astype(np.float32)
+    out = S.gen_padded(ctx, GOLD[f"pad_{tag}_Np"], GOLD[f"pad_{tag}_dx"], GOLD[f"pad_{tag}_corrL"],
+                       int(GOLD[f"pad_{tag}_cm"]), float(GOLD[f"pad_{tag}_nu"]),
+                       pad=GOLD[f"pad_{tag}_P"], xi=xi, dtype=dtype)
+    assert rel(out, GOLD[f"pad_{tag}_out"]) < tol
+
+
+@pytest.mark.parametrize("Np,P,dx,cl,cm,nu", [
+    ((20, 20, 20), (64, 64, 64), (1, 1, 1), (5, 5, 5), 1, 0.5),
+    ((30, 17, 11), (64, 32, 32), (0.5, 1, 2), (3, 6, 9), 3, 0.5),
+    ((33, 40, 25), (128, 64, 64), (1, 1, 1), (8, 4, 6), 2, 1.5),
+    ((16, 16, 16), (32, 32, 32), (1, 1, 1), (4, 4, 4), 2, 0.3),
+    ((100, 7, 9), (256, 16, 32), (1, 1, 1), (10, 2, 3), 3, 0.5),
+    ((5, 60, 3), (32, 128, 32), (1, 1, 1), (2, 10, 2), 1, 0.5),
+])
+def test_gen_padded_philox_vs_oracle(ctx, oracle, Np, P, dx, cl, cm, nu):
+    ref = oracle.gen_padded(Np, P, dx, cl, cm, nu, 1, seed=77, stream=3)
+    out64 = S.gen_padded(ctx, Np, dx, cl, cm, nu, pad=P, seed=77, stream=3, dtype=S.F64)
+    assert rel(out64, ref) < TOL64
+    out32 = S.gen_padded(ctx, Np, dx, cl, cm, nu, pad=P, seed=77, stream=3, dtype=S.F32)
+    assert rel(out32, ref) < TOL32
+
+
+def test_gen_padded_unnormalised_vs_oracle(ctx, oracle):
+    Np, P = (24, 24, 24), (64, 64, 64)
+    ref = oracle.gen_padded(Np, P, (1, 1, 1), (6, 6, 6), 3, 0.5, 0, seed=5)
+    out = S.gen_padded(ctx, Np, (1, 1, 1), (6, 6, 6), 3, pad=P, normalise=False, seed=5,
+                       dtype=S.F64)
+    assert rel(out, ref) < TOL64
+
+
+def test_gen_padded_default_pad_and_determinism(ctx):
+    a = S.gen_padded(ctx, (40, 30, 20), (1, 1, 1), (5, 5, 5), 1, seed=9)
+    b = S.gen_padded(ctx, (40, 30, 20), (1, 1, 1), (5, 5, 5), 1, seed=9)
+    c = S.gen_padded(ctx, (40, 30, 20), (1, 1, 1), (5, 5, 5), 1, seed=10)
+    assert np.array_equal(a, b)
+    assert not np.allclose(a, c)
+
+
+def test_gen_padded_device_pointer(ctx):
+    torch = pytest.importorskip("torch")
+    host = S.gen_padded(ctx, (32, 16, 8), (1, 1, 1), (4, 4, 4), 1, seed=1, dtype=S.F32)
+    dev = torch.empty(8 * 16 * 32, dtype=torch.float32, device="cuda")
+    S.gen_padded(ctx, (32, 16, 8), (1, 1, 1), (4, 4, 4), 1, seed=1, dtype=S.F32, out=dev)
+    ctx.sync()
+    np.testing.assert_array_equal(dev.cpu().numpy(), host.reshape(-1, order="F"))
+
+
+# ---------------------------------------------------------------------------
+# reference generators
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_dct_generator_golden(ctx, tag):
+    out = S.gen_std_gauss_FFT(ctx, GOLD[f"dct_{tag}_Np"], GOLD[f"dct_{tag}_xRange"],
+                              GOLD[f"dct_{tag}_corrL"], 1, 0, 0, phiK=GOLD[f"dct_{tag}_phi"])
+    assert rel(out, GOLD[f"dct_{tag}_out"]) < TOL64
+
+
+@pytest.mark.parametrize("Np", [(64, 64, 64), (37, 50, 29), (128, 20, 3)])
+def test_dct_generator_vs_oracle(ctx, oracle, Np):
+    rng = np.random.default_rng(sum(Np))
+    phi = np.asfortranarray(rng.random([n // 2 for n in Np]))
+    gam = np.asfortranarray(rng.random([n // 2 for n in Np]))
+    xr = [(n - 1) * 0.5 for n in Np]
+    cl = (3.0, 4.0, 5.0)
+    ref = oracle.gen_std_gauss_fft(Np, xr, cl, phi, gam)
+    out = S.gen_std_gauss_FFT(ctx, Np, xr, cl, 1, 0, 0, phiK=phi, gammaK=gam)
+    assert rel(out, ref) < TOL64
+
+
+def test_dct_generator_default_phases(ctx, oracle):
+    Np = (20, 22, 18)
+    xr = [19.0, 21.0, 17.0]
+    seed, rank = 41, 3
+    phi = oracle.uniforms(seed + rank, 0, 0, 10 * 11 * 9).reshape((10, 11, 9), order="F")
+    ref = oracle.gen_std_gauss_fft(Np, xr, (2, 2, 2), phi)
+    out = S.gen_std_gauss_FFT(ctx, Np, xr, (2, 2, 2), 1, seed, rank)
+    assert rel(out, ref) < TOL64
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_shino_generator_golden(ctx, tag):
+    out = S.gen_std_gauss_Shino_FFT(ctx, GOLD[f"shino_{tag}_Np"], GOLD[f"shino_{tag}_xRange"],
+                                    GOLD[f"shino_{tag}_corrL"], seed=int(GOLD[f"shino_{tag}_seed"]))
+    assert rel(out, GOLD[f"shino_{tag}_out"]) < TOL64
+
+
+@pytest.mark.parametrize("Np,xr,cl,seed", [
+    ((40, 40, 40), (39.0, 39.0, 39.0), (4.0, 4.0, 4.0), 1),
+    ((25, 70, 33), (24.0, 34.5, 64.0), (3.0, 2.0, 5.0), -17),
+    ((100, 12, 9), (99.0, 11.0, 8.0), (9.0, 1.0, 1.0), 2147483000),
+])
+def test_shino_generator_vs_oracle(ctx, oracle, Np, xr, cl, seed):
+    ref = oracle.gen_std_gauss_shino_fft(Np, xr, cl, seed, 0)
+    out = S.gen_std_gauss_Shino_FFT(ctx, Np, xr, cl, seed=seed)
+    assert rel(out, ref) < TOL64
+
+
+# ---------------------------------------------------------------------------
+# full sample: tiles, PoU, overlap, marginal
+# ---------------------------------------------------------------------------
+SAMPLES = [
+    # xmin, xmax, corrL, overlap, ppcl, corrMod, nu, margi, avg, std, seed, nb, topo
+    ((0, 0, 0), (30, 24, 20), (4, 3, 5), (1, 1, 1), (5, 4, 6), 1, 0.5, 1, 0.0, 1.0, 0, 8, None),
+    ((0, 0, 0), (40, 20, 12), (5, 5, 3), (2, 1, 0.5), (6, 6, 5), 3, 0.5, 2, 1.0, 0.3, 3, 6, (3, 2, 1)),
+    ((-5, 2, 1), (20, 30, 14), (3, 6, 2), (0, 1, 1), (4, 5, 5), 2, 1.5, 2, 2.0, 0.5, 11, 4, (2, 1, 2)),
+    ((0, 0, 0), (16, 16, 16), (2, 2, 2), (0, 0, 0), (5, 5, 5), 1, 0.5, 1, 1.0, 2.0, 7, 8, (2, 2, 2)),
+    ((0, 0, 0), (24, 18, 10), (2, 3, 2), (0.25, 0.34, 0.1), (5, 4, 4), 3, 0.5, 1, 0.0, 1.0, 2, 8, None),
+]
+
+
+@pytest.mark.parametrize("case", range(len(SAMPLES)))
+@pytest.mark.parametrize("generator", [S.GEN_PADDED, S.GEN_DCT, S.GEN_SHINO])
+def test_generate_sample_vs_oracle(ctx, oracle, case, generator):
+    (xmin, xmax, cl, ov, ppcl, cm, nu, mf, avg, sd, seed, nb, topo) = SAMPLES[case]
+    if generator != S.GEN_PADDED:
+        cm = 1
+    s = S.make_sample(xmin, xmax, cl, ov, ppcl, cm, mf, avg, sd, seed, nu)
+    ref, lay = oracle.generate_sample(generator, xmin, xmax, cl, ov, ppcl, cm, nu, mf, avg, sd,
+                                      seed, nb, topo)
+    out, glay = S.generate_sample(ctx, s, generator=generator, dtype=S.F64, nb_procs=nb, topo=topo)
+    np.testing.assert_array_equal(glay["L"], lay["L"])
+    assert rel(out, ref) < TOL64
+    if generator == S.GEN_PADDED:
+        out32, _ = S.generate_sample(ctx, s, generator=generator, dtype=S.F32, nb_procs=nb, topo=topo)
+        assert rel(out32, ref) < TOL32
+
+
+def test_generate_sample_normalize_field(ctx, oracle):
+    args = ((0, 0, 0), (30, 24, 20), (4, 3, 5), (1, 1, 1), (5, 4, 6))
+    s = S.make_sample(*args, 1, 2, 1.0, 0.4, 5)
+    ref, _ = oracle.generate_sample(3, *args, 1, 0.5, 2, 1.0, 0.4, 5, 8, None, normalize_field=1)
+    out, _ = S.generate_sample(ctx, s, dtype=S.F64, nb_procs=8, normalize_field=True)
+    assert rel(out, ref) < TOL64
+
+
+def test_generate_sample_constant_field(ctx):
+    s = S.make_sample((0, 0, 0), (10, 10, 10), (1, 1, 1), (1, 1, 1), (3, 3, 3), 1, 1, 2.5, 0.0, 0)
+    out, _ = S.generate_sample(ctx, s, nb_procs=2)
+    assert np.all(out == np.float32(2.5))
+
+
+def test_generate_sample_dct_injected_phases(ctx, oracle):
+    args = ((0, 0, 0), (12, 10, 8), (2, 2, 2), (1, 1, 1), (4, 4, 4))
+    lay = oracle.sample_layout(*args, 1, 4)
+    K = int(np.prod(lay["Np"] // 2))
+    phi = np.random.default_rng(0).random(4 * K)
+    s = S.make_sample(*args, 1, 1, 0.0, 1.0, 0)
+    ref, _ = oracle.generate_sample(1, *args, 1, 0.5, 1, 0.0, 1.0, 0, 4, None, phiK_all=phi)
+    out, _ = S.generate_sample(ctx, s, generator=S.GEN_DCT, dtype=S.F64, nb_procs=4, phiK=phi)
+    assert rel(out, ref) < TOL64
+
+
+# ---------------------------------------------------------------------------
+# post steps
+# ---------------------------------------------------------------------------
+def test_apply_unity_partition_bit_exact(ctx, oracle):
+    rng = np.random.default_rng(1)
+    for Np, No, pos, shape in [((9, 8, 7), (4, 3, 2), (1, 0, 1), (3, 2, 2)),
+                               ((16, 12, 10), (5, 1, 3), (0, 1, 0), (2, 2, 2)),
+                               ((7, 7, 7), (3, 3, 3), (1, 1, 1), (3, 3, 3))]:
+        f = np.asfortranarray(rng.standard_normal(Np))
+        ref = oracle.apply_unity_partition(f, Np, No, pos, shape)
+        g = f.copy(order="F")
+        S.apply_UnityPartition_mtx(ctx, g, Np, No, 1, pos, shape)
+        np.testing.assert_array_equal(g, ref)
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_add_overlap_bit_exact(ctx, tag):
+    tiles = np.ascontiguousarray(GOLD[f"ovl_{tag}_in"])
+    shape = GOLD[f"ovl_{tag}_shape"]
+    Np = GOLD[f"ovl_{tag}_Np"]
+    # tiles are stored rank-major, each tile in Fortran order
+    flat = np.concatenate([t.reshape(-1, order="F") for t in tiles])
+    S.add_overlap(ctx, flat, Np, GOLD[f"ovl_{tag}_No"], shape)
+    ref = np.concatenate([t.reshape(-1, order="F") for t in GOLD[f"ovl_{tag}_out"]])
+    np.testing.assert_array_equal(flat, ref)
+
+
+@pytest.mark.parametrize("mf,avg,sd", [(1, 0.5, 2.0), (2, 1.0, 0.3), (2, 3.0, 1.5)])
+def test_multivariate_transformation(ctx, oracle, mf, avg, sd):
+    f = np.random.default_rng(2).standard_normal(1000)
+    ref = oracle.multivariate_transformation(avg, sd, mf, f)
+    g = f.copy()
+    S.multiVariateTransformation(ctx, avg, sd, mf, g)
+    np.testing.assert_allclose(g, ref, rtol=1e-15, atol=1e-15)
+    g32 = f.astype(np.float32)
+    S.multiVariateTransformation(ctx, avg, sd, mf, g32)
+    assert rel(g32, ref) < TOL32
+
+
+def test_normalize_field(ctx, oracle):
+    f = np.asfortranarray(np.random.default_rng(3).standard_normal((20, 15, 10)) * 3 + 1)
+    (ref,), a, s = oracle.normalize_field([f], [20, 15, 10], [0, 0, 0], [1, 1, 1])
+    g = f.copy(order="F")
+    a2, s2 = S.normalize_field(ctx, g)
+    assert a2 == pytest.approx(a, rel=1e-13) and s2 == pytest.approx(s, rel=1e-13)
+    assert rel(g, ref) < TOL64
+
+
+def test_marginal_rejects_nonpositive_lognormal_mean(ctx):
+    with pytest.raises(S.ScarlError) as e:
+        S.multiVariateTransformation(ctx, 0.0, 1.0, 2, np.zeros(4))
+    assert e.value.code == 1
+
+
+# ---------------------------------------------------------------------------
+# estimators
+# ---------------------------------------------------------------------------
+def test_moments_vs_oracle(ctx, oracle):
+    f = np.random.default_rng(4).standard_normal((7000, 5)) * 2 + 0.5
+    ref = oracle.moments(f)
+    got = S.calculate_average_and_stdVar(ctx, np.asfortranarray(f), Nmc=5)
+    np.testing.assert_allclose(got[0], ref[0], rtol=1e-12)
+    np.testing.assert_allclose(got[1], ref[1], rtol=1e-12)
+    assert got[2] == pytest.approx(ref[2], rel=1e-12) and got[3] == pytest.approx(ref[3], rel=1e-12)
+    got32 = S.calculate_average_and_stdVar(ctx, np.asfortranarray(f.astype(np.float32)), Nmc=5)
+    assert got32[3] == pytest.approx(ref[3], rel=1e-6)
+
+
+def test_rebuild_sk_golden(ctx):
+    f = GOLD["sk_field"]
+    sk = S.rebuild_Sk(ctx, f, f.shape, float(GOLD["sk_avg"]), float(GOLD["sk_sd"]))
+    off = 0
+    for d in range(3):
+        n = f.shape[d] // 2
+        np.testing.assert_allclose(sk[off:off + n], GOLD[f"sk_dir{d}"][:n], rtol=1e-12, atol=1e-14)
+        off += n
+
+
+@pytest.mark.parametrize("shape", [(33, 20, 17), (64, 8, 40), (5, 6, 7)])
+@pytest.mark.parametrize("literal", [True, False])
+def test_rebuild_sk_vs_oracle(ctx, oracle, shape, literal):
+    f = np.asfortranarray(np.random.default_rng(sum(shape)).standard_normal(shape))
+    avg, sd = float(f.mean()), float(f.std())
+    sk = S.rebuild_Sk(ctx, f, shape, avg, sd, tukey_literal=literal)
+    off = 0
+    for d in range(3):
+        n = shape[d] // 2
+        ref = oracle.rebuild_sk_fft(f, d, avg, sd, int(literal))
+        np.testing.assert_allclose(sk[off:off + n], ref[:n], rtol=1e-11, atol=1e-13)
+        off += n
+    cl = S.rebuild_corrL(sk, shape, (1.0, 0.5, 2.0))
+    np.testing.assert_array_equal(cl, oracle.rebuild_corrL(sk, [v // 2 for v in shape], (1.0, 0.5, 2.0)))
+
+
+# ---------------------------------------------------------------------------
+# error paths
+# ---------------------------------------------------------------------------
+def test_error_paths(ctx):
+    with pytest.raises(S.ScarlError) as e:
+        S.gen_padded(ctx, (10, 10, 10), (1, 1, 1), (2, 2, 2), 1, pad=(24, 32, 32))
+    assert e.value.code == 5
+    with pytest.raises(S.ScarlError) as e:
+        S.gen_padded(ctx, (40, 10, 10), (1, 1, 1), (2, 2, 2), 1, pad=(32, 32, 32))
+    assert e.value.code == 1
+    with pytest.raises(S.ScarlError) as e:
+        S.gen_std_gauss_FFT(ctx, (8, 8, 8), (7, 7, 7), (1, 1, 1), corrMod=2)
+    assert e.value.code == 1
+    small = S.Context(0, budget_bytes=1 << 20)
+    try:
+        with pytest.raises(S.ScarlError) as e:
+            S.gen_padded(small, (200, 200, 200), (1, 1, 1), (8, 8, 8), 1)
+        assert e.value.code == 2
+    finally:
+        small.close()

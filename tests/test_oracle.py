@@ -1,0 +1,222 @@
+"""The CPU oracle pinned against the reference's known-answer values, the
+published Philox vectors, FFTW's transform definitions (numpy/scipy) and the
+independent numpy restatement in tests/golden/golden.npz."""
+import os
+
+import numpy as np
+import pytest
+import scipy.fft as sfft
+from scipy.special import gamma, kv
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden.npz"))
+
+
+def test_park_miller_kat(oracle):
+    # SRC_F/normal_ScaRL.f90:762-769
+    s = 12345
+    seeds = []
+    for _ in range(3):
+        s = oracle.pm_step(s)
+        seeds.append(s)
+    assert seeds == [207482415, 1790989824, 2035175616]
+    r, last = oracle.r8vec_uniform_01(3, 12345)
+    # the table prints six decimals
+    np.testing.assert_allclose(r, [0.096616, 0.833995, 0.947702], rtol=0, atol=1.0e-6)
+    assert last == 2035175616
+    np.testing.assert_array_equal(r, GOLD["pm_12345"])
+
+
+def test_park_miller_jump(oracle):
+    s = oracle.pm_step(987654321)
+    seq, _ = oracle.r8vec_uniform_01(200, s)
+    for n in (1, 2, 17, 199):
+        assert oracle.pm_jump(s, n) * 4.656612875e-10 == seq[n - 1]
+
+
+def test_r8vec_normal_01_box_muller(oracle):
+    for n in (1, 6, 7):
+        x, _ = oracle.r8vec_normal_01(n, 4242)
+        u, _ = oracle.r8vec_uniform_01(2 * ((n + 1) // 2), 4242)
+        pi = 3.141592653589793
+        if n == 1:
+            ref = [np.sqrt(-2 * np.log(u[0])) * np.cos(2 * pi * u[1])]
+        else:
+            ref = []
+            for i in range(n // 2):
+                r = np.sqrt(-2 * np.log(u[2 * i]))
+                ref += [r * np.cos(2 * pi * u[2 * i + 1]), r * np.sin(2 * pi * u[2 * i + 1])]
+            if n % 2:
+                ref.append(np.sqrt(-2 * np.log(u[n - 1])) * np.cos(2 * pi * u[n]))
+        np.testing.assert_allclose(x, ref, rtol=1e-15, atol=1e-15)
+
+
+@pytest.mark.parametrize("ctr,key,expect", [
+    # Random123 known-answer vectors for philox4x32_R(10)
+    ((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+    ((0xffffffff,) * 4, (0xffffffff,) * 2, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+    ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+     (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1)),
+])
+def test_philox_kat(oracle, ctr, key, expect):
+    assert tuple(oracle.philox(ctr, key)) == expect
+
+
+def test_normals_distribution(oracle):
+    z = oracle.normals(5, 0, 0, 200000)
+    assert abs(z.mean()) < 0.01 and abs(z.std() - 1) < 0.01
+    np.testing.assert_array_equal(oracle.normals(5, 0, 100, 10), z[100:110])
+    assert not np.array_equal(oracle.normals(5, 1, 0, 10), z[:10])
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 37, 64, 297])
+def test_dct3_is_fftw_redft01(oracle, n):
+    x = np.random.default_rng(n).random(n)
+    np.testing.assert_allclose(oracle.dct3_1d(x), sfft.dct(x, type=3), rtol=1e-12, atol=1e-12)
+
+
+def test_dct3_3d(oracle):
+    x = np.asfortranarray(np.random.default_rng(1).random((8, 6, 11)))
+    np.testing.assert_allclose(oracle.dct3_3d(x), sfft.dctn(x, type=3), rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("n", [1, 2, 8, 12, 64, 97, 513])
+def test_fft_backward_forward(oracle, n):
+    z = np.random.default_rng(n).random(n) + 1j * np.random.default_rng(n + 1).random(n)
+    np.testing.assert_allclose(oracle.fft1d(z, -1), np.fft.fft(z), rtol=1e-12, atol=1e-11)
+    np.testing.assert_allclose(oracle.fft1d(z, +1), np.fft.ifft(z) * n, rtol=1e-12, atol=1e-11)
+
+
+def test_c2r_crop_is_irfftn(oracle):
+    P = [16, 8, 12]
+    rng = np.random.default_rng(3)
+    H = rng.random((9, 8, 12)) + 1j * rng.random((9, 8, 12))
+    ref = np.fft.irfftn(H.transpose(2, 1, 0), s=(12, 8, 16), axes=(0, 1, 2)).transpose(2, 1, 0)
+    ref = ref * np.prod(P)
+    np.testing.assert_allclose(oracle.c2r_3d_crop(H, P, [11, 5, 7]), ref[:11, :5, :7],
+                               rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_dct_generator_golden(oracle, tag):
+    out = oracle.gen_std_gauss_fft(GOLD[f"dct_{tag}_Np"], GOLD[f"dct_{tag}_xRange"],
+                                   GOLD[f"dct_{tag}_corrL"], GOLD[f"dct_{tag}_phi"])
+    ref = GOLD[f"dct_{tag}_out"]
+    assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-13
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+@pytest.mark.parametrize("via_c2c", [1, 0])
+def test_shino_generator_golden(oracle, tag, via_c2c):
+    out = oracle.gen_std_gauss_shino_fft(GOLD[f"shino_{tag}_Np"], GOLD[f"shino_{tag}_xRange"],
+                                         GOLD[f"shino_{tag}_corrL"], int(GOLD[f"shino_{tag}_seed"]),
+                                         via_c2c)
+    ref = GOLD[f"shino_{tag}_out"]
+    assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-13
+
+
+@pytest.mark.parametrize("tag", ["g", "e", "v"])
+def test_padded_generator_golden(oracle, tag):
+    P = GOLD[f"pad_{tag}_P"]
+    out = oracle.gen_padded(GOLD[f"pad_{tag}_Np"], P, GOLD[f"pad_{tag}_dx"],
+                            GOLD[f"pad_{tag}_corrL"], int(GOLD[f"pad_{tag}_cm"]),
+                            float(GOLD[f"pad_{tag}_nu"]), 1, xi=GOLD[f"pad_{tag}_xi"].reshape(-1))
+    ref = GOLD[f"pad_{tag}_out"]
+    assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-13
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_pou_and_overlap_golden_bit_exact(oracle, tag):
+    w = oracle.unity_partition_weights(GOLD[f"pou_{tag}_Np"], GOLD[f"pou_{tag}_No"],
+                                       GOLD[f"pou_{tag}_pos"], GOLD[f"pou_{tag}_shape"])
+    np.testing.assert_array_equal(w, GOLD[f"pou_{tag}_w"])
+    fs = oracle.add_overlap(list(GOLD[f"ovl_{tag}_in"]), GOLD[f"ovl_{tag}_Np"],
+                            GOLD[f"ovl_{tag}_No"], GOLD[f"ovl_{tag}_shape"])
+    np.testing.assert_array_equal(np.stack(fs), GOLD[f"ovl_{tag}_out"])
+
+
+def test_rebuild_sk_golden(oracle):
+    f = GOLD["sk_field"]
+    for d in range(3):
+        s = oracle.rebuild_sk_fft(f, d, float(GOLD["sk_avg"]), float(GOLD["sk_sd"]), 1)
+        np.testing.assert_allclose(s, GOLD[f"sk_dir{d}"], rtol=1e-12, atol=1e-14)
+
+
+def test_rebuild_sk_is_circular_autocorrelation(oracle):
+    f = np.asfortranarray(np.random.default_rng(9).standard_normal((9, 7, 8)))
+    for lit in (1, 0):
+        w = oracle.tukey(7, lit)
+        s = oracle.rebuild_sk_fft(f, 1, 0.1, 1.3, lit)
+        t = (f - 0.1) / 1.3 * w[None, :, None]
+        ref = np.array([np.mean(np.sum(t * np.roll(t, -m, axis=1), axis=1)) / 7 for m in range(7)])
+        np.testing.assert_allclose(s, ref, rtol=1e-12, atol=1e-14)
+
+
+def test_tukey_windows(oracle):
+    lit = oracle.tukey(101, 1)
+    std = oracle.tukey(101, 0)
+    assert std[50] == 1.0 and np.all(std[6:95] == 1.0)
+    assert lit[0] == pytest.approx(0.0, abs=1e-12)
+    # the literal window's high-side formula oscillates across the middle
+    assert lit[30:70].min() < 0.1
+
+
+def test_moments_formula(oracle):
+    f = np.random.default_rng(2).random((500, 3))
+    ea, es, ga, gs = oracle.moments(f)
+    np.testing.assert_allclose(ea, f.mean(axis=0), rtol=1e-13)
+    np.testing.assert_allclose(es, f.std(axis=0), rtol=1e-12)
+    assert ga == pytest.approx(f.mean(), rel=1e-13)
+    assert gs == pytest.approx(f.std(), rel=1e-12)
+
+
+@pytest.mark.parametrize("nu", [0.3, 0.5, 1.5])
+def test_von_karman_spectrum_is_matern(oracle, nu):
+    """The 3D spectral density integrates back to C(r): check C(0) = 1 and the
+    closed-form correlation at r = l along an axis against scipy's K_nu."""
+    corrL = [6.0, 6.0, 6.0]
+    P, dx = [128, 128, 128], [1.0, 1.0, 1.0]
+    # the grid-sampled spectrum recovers more of the unit variance as the
+    # grid is refined (rough, small-nu fields keep variance above Nyquist)
+    s1 = oracle.spectrum_sum(2, nu, P, dx, corrL)
+    s2 = oracle.spectrum_sum(2, nu, P, [0.5, 0.5, 0.5], [c * 0.5 for c in corrL])
+    s3 = oracle.spectrum_sum(2, nu, [256, 256, 256], [0.5, 0.5, 0.5], corrL)
+    assert 0.7 < s1 < s3 < 1.0 and s2 == pytest.approx(s1, rel=0.02)
+    a = corrL[0] * gamma(nu) / (2 * np.sqrt(np.pi) * gamma(nu + 0.5))
+    r = corrL[0]
+    c_ref = 2 ** (1 - nu) / gamma(nu) * (r / a) ** nu * kv(nu, r / a)
+    # integral of the correlation along an axis equals corrL
+    rr = np.linspace(1e-9, 40 * corrL[0], 400001)
+    cc = 2 ** (1 - nu) / gamma(nu) * (rr / a) ** nu * kv(nu, rr / a)
+    assert 2 * np.trapezoid(cc, rr) == pytest.approx(corrL[0], rel=1e-3)
+    assert 0 < c_ref < 1
+
+
+def test_spectra_integrate_to_unit_variance(oracle):
+    P, dx = [64, 64, 64], [1.0, 1.0, 1.0]
+    assert oracle.spectrum_sum(1, 0.5, P, dx, [4.0, 4.0, 4.0]) == pytest.approx(1.0, rel=1e-5)
+    # the exponential spectrum decays as |k|^-4: about 17% lies beyond Nyquist at 4 cells per l
+    assert 0.8 < oracle.spectrum_sum(3, 0.5, P, dx, [4.0, 4.0, 4.0]) < 1.0
+
+
+def test_padded_method_variance_and_mean(oracle):
+    out = oracle.gen_padded([48, 48, 48], [128, 128, 128], [1, 1, 1], [6, 6, 6], 1, 0.5, 1, seed=11)
+    assert abs(out.mean()) < 0.2
+    assert out.var() == pytest.approx(1.0, rel=0.3)
+
+
+def test_generate_sample_constant_field(oracle):
+    g, lay = oracle.generate_sample(3, (0, 0, 0), (10, 10, 10), (1, 1, 1), (1, 1, 1), (3, 3, 3),
+                                    std_dev=0.0, avg=2.5, nb_procs=2)
+    assert np.all(g == 2.5)
+
+
+def test_generate_sample_rejects_invalid(oracle):
+    with pytest.raises(ValueError):
+        oracle.generate_sample(3, (0, 0, 0), (10, 10, 10), (1, 1, 1), (1, 1, 1), (1, 3, 3))
+
+
+def test_streaming_generator_matches(oracle):
+    args = ([20, 17, 11], [64, 32, 32], [1, 0.5, 2], [3, 6, 9], 3, 0.5)
+    a = oracle.gen_padded(*args, 1, seed=4, stream=2)
+    b = oracle.gen_padded_stream(*args, seed=4, stream=2)
+    np.testing.assert_array_equal(a, b)
