@@ -32,6 +32,7 @@ DECK = dict(xMinGlob=(0, 0, 0), xMaxGlob=(512, 512, 512), corrL=(40, 20, 10),
             overlap=(2, 2, 2), pointsPerCorrL=(41, 21, 11), corrMod=3, margiFirst=2,
             avg=1.0, std_dev=0.3, seedBase=0, nu=0.5)
 TOPO = (2, 2, 2)
+PAD_TOL = 1e-3  # periodic-image tolerance of the AUTO padded grid
 
 
 def load_peaks():
@@ -114,14 +115,18 @@ def layout_of(S):
     return s, S.sample_layout(s, 1, 8, TOPO)
 
 
-def pass_bytes(lay, dtype_bytes=4):
+def pads(S, lay, policy):
+    return [int(v) for v in S.pad_size(policy, DECK["corrMod"], DECK["corrL"], lay["xStep"],
+                                       lay["Np"], DECK["nu"], PAD_TOL)]
+
+
+def pass_bytes(lay, P, dtype_bytes=4):
     """Algorithmic HBM bytes per launch of each pass, averaged over tiles.
     Pass 1 writes the z-transformed half spectrum (its input is synthesised in
     registers); pass 2 reads it and writes the y-pruned rows; pass 3 reads
     those and writes the tile's points into the field (plus the re-read of
     points an earlier tile already wrote)."""
     Np, No, T = [int(v) for v in lay["Np"]], [int(v) for v in lay["Np_ovlp"]], lay["topo"]
-    P = [1 << (2 * n - 1).bit_length() for n in Np]
     Hx = P[0] // 2 + 1
     c = 2 * dtype_bytes
     b1 = Hx * P[1] * Np[2] * c
@@ -136,15 +141,14 @@ def pass_bytes(lay, dtype_bytes=4):
             own *= Np[d] - (No[d] if pos[d] > 0 and No[d] >= 2 else 0)
         reread += Np[0] * Np[1] * Np[2] - own
     b3 = Hx * Np[1] * Np[2] * c + Np[0] * Np[1] * Np[2] * dtype_bytes + reread * dtype_bytes // nb
-    return {"k_gen_z": b1, "k_mid_y": b2, "k_c2r_x": b3}, P
+    return {"k_gen_z": b1, "k_mid_y": b2, "k_c2r_x": b3}
 
 
-def cpu_sample(lay, steps, warmup, stride=8):
+def cpu_sample(lay, P, steps, warmup, stride=8):
     """The oracle (CPU restatement, OpenMP) on every stride-th line of each
-    pass of tile 0: per step, 1/stride of one tile's work."""
+    pass of tile 0 on padded grid P: per step, 1/stride of one tile's work."""
     from oracle import oracle as O
     Np = [int(v) for v in lay["Np"]]
-    P = [1 << (2 * n - 1).bit_length() for n in Np]
     dx = [float(v) for v in lay["xStep"]]
     norm = O.spectrum_sum(DECK["corrMod"], DECK["nu"], P, dx, DECK["corrL"])
     out = __import__("numpy").zeros(Np, order="F")
@@ -172,25 +176,25 @@ def run_reference(args, rank):
         return
     import scarl_b200 as S
     _, lay = layout_of(S)
-    base, dt = cpu_sample(lay, args.steps, args.warmup)
+    base, dt = cpu_sample(lay, pads(S, lay, S.PAD_AUTO), args.steps, args.warmup)
     line = {"metric": METRIC, "value": base["value"], "unit": "Mpoints/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": config_of(lay),
+            "config": config_of(lay, pads(S, lay, S.PAD_AUTO)),
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "Mpoints/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def config_of(lay):
+def config_of(lay, P):
     return {"workload": "512^3 deck -> 513^3 field, exponential, l=(40,20,10), lognormal mean 1 "
                         "CV 0.3, 2x2x2 tiles, overlap 2l, padded periodic C2R FP32",
             "global_points": [int(v) for v in lay["L"]], "tile_points": [int(v) for v in lay["Np"]],
             "overlap_points": [int(v) for v in lay["Np_ovlp"]], "tiles": [int(v) for v in lay["topo"]],
-            "padded_grid": [1 << (2 * int(n) - 1).bit_length() for n in lay["Np"]],
-            "l2": "working set larger than L2 (1.3 GB intermediate, 0.54 GB field)"}
+            "padded_grid": P, "pad_policy": f"auto (periodic image error <= {PAD_TOL:g})",
+            "l2": "working set larger than L2 (field 0.54 GB, intermediate >= 0.15 GB per tile)"}
 
 
 def main():
@@ -224,7 +228,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     ctx = S.Context(local)
-    stream = torch.cuda.current_stream()
+    # a real stream shared by the library and the timing events (the legacy
+    # default stream's handle is 0, which the library reads as "own stream")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     sample, lay = layout_of(S)
     sample.seedBase = 1000 * rank  # independent replica per rank
@@ -232,9 +239,11 @@ def main():
     npts = L[0] * L[1] * L[2]
     field = torch.empty(npts, dtype=torch.float32, device="cuda")
 
-    def step(out=field, dtype=S.F32):
+    P_auto, P_full = pads(S, lay, S.PAD_AUTO), pads(S, lay, S.PAD_FULL)
+
+    def step(out=field, dtype=S.F32, policy=S.PAD_AUTO):
         S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=dtype, nb_procs=8,
-                          topo=TOPO, out=out)
+                          topo=TOPO, pad_policy=policy, pad_tol=PAD_TOL, out=out)
 
     def barrier():
         if dist is not None:
@@ -242,16 +251,16 @@ def main():
 
     for _ in range(args.warmup):
         step()
+        step(policy=S.PAD_FULL)
     torch.cuda.synchronize()
 
     # ---- timed region: device-resident output, CUDA events on the launch stream
     launches0 = ctx.counters()["launches"]
     props = torch.cuda.get_device_properties(local)
-    bus = getattr(props, "pci_bus_id", None)
-    if bus is None:
-        bus = "%08x:%02x:%02x.0" % (getattr(props, "pci_domain_id", 0), getattr(props, "pci_bus_id", 0),
-                                     getattr(props, "pci_device_id", 0))
-    clk = Clocks(str(bus))
+    bus = "%08x:%02x:%02x.0" % (int(getattr(props, "pci_domain_id", 0)),
+                                int(getattr(props, "pci_bus_id", 0)),
+                                int(getattr(props, "pci_device_id", 0)))
+    clk = Clocks(bus)
     clk.start()
     barrier()
     torch.cuda.synchronize()
@@ -272,6 +281,23 @@ def main():
         ms = float(t.item())
     value = world * npts / (ms * 1e-3) / 1e6
 
+    # ---- the plain path: the reference's full padding, same timing method
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(policy=S.PAD_FULL)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_full = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms_full], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_full = float(t.item())
+    plain = {"value": round(world * npts / (ms_full * 1e-3) / 1e6, 2), "ms_per_step": round(ms_full, 4),
+             "padded_grid": P_full, "pad_policy": "full, 2^ceil(log2(2 Np)) (SRC_F/fftw_ScaRL.f90:194)"}
+
     # ---- per-kernel device times (separate, profiled steps)
     ctx.profile(True)
     ctx.profile_reset()
@@ -281,7 +307,7 @@ def main():
     torch.cuda.synchronize()
     stats = ctx.profile_stats()
     ctx.profile(False)
-    pb, P = pass_bytes(lay)
+    pb = pass_bytes(lay, P_auto)
     peak, peak_kind = load_peaks()
     kern = {}
     for k, (tot, n) in stats.items():
@@ -319,12 +345,14 @@ def main():
     host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
     hnp = host.numpy()
     ctx.set_stream(0)  # library-owned stream; host calls synchronise inside
-    S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, out=hnp)
+    S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
+                      pad_tol=PAD_TOL, out=hnp)
     c0 = ctx.counters()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, out=hnp)
+        S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
+                          pad_tol=PAD_TOL, out=hnp)
     e2e_s = (time.perf_counter() - t0) / args.steps
     c1 = ctx.counters()
     if dist is not None:
@@ -338,7 +366,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu, _ = cpu_sample(lay, 1, 0)
+        cpu, _ = cpu_sample(lay, P_auto, 1, 0)
 
     if dist is not None:
         dist.barrier()
@@ -346,8 +374,9 @@ def main():
         line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpoints/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (Philox normals, seeded per rank)", "config": config_of(lay),
-                "rel_l2_vs_fp64": rel, "roofline": roof, "kernels": kern,
+                "data": "synthetic (Philox normals, seeded per rank)",
+                "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "roofline": roof,
+                "kernels": kern, "plain_path": plain,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -57,6 +57,10 @@ extern "C" {
 #define SCARL_GEN_SHINO 2    /* gen_std_gauss_Shino_FFT, SRC_F/fftw_ScaRL.f90:157 */
 #define SCARL_GEN_PADDED 3   /* padded periodic C2R, normalised spectra */
 
+/* ---- padded grid policies ---- */
+#define SCARL_PAD_FULL 0     /* 2^ceil(log2(2 Np)), SRC_F/fftw_ScaRL.f90:194 */
+#define SCARL_PAD_AUTO 1     /* smallest power of two with image error <= tol */
+
 typedef struct scarl_ctx scarl_ctx;
 
 /* One deck entry: the 11 per-sample lines of input_ScaRL.txt
@@ -102,7 +106,9 @@ typedef struct {
   int dtype;              /* SCARL_F32 / SCARL_F64, 0 = SCARL_F32 */
   int nb_procs;           /* tiles requested (mpirun -np), 0 = 1 */
   int topo_shape[3];      /* explicit topology (extra_config_ScaRL.txt); 0 = decide */
-  int pad[3];             /* padded grid per axis, 0 = 2^ceil(log2(2 Np)) */
+  int pad[3];             /* explicit padded grid per axis; 0 = chosen by pad_policy */
+  int pad_policy;         /* SCARL_PAD_FULL (default) or SCARL_PAD_AUTO */
+  double pad_tol;         /* SCARL_PAD_AUTO image tolerance, 0 = 1e-3 */
   int no_spectral_normalisation; /* 1 = raw Riemann-sum amplitudes */
   int normalize_field;    /* 1 = normalize_field (disabled in the reference) */
   uint32_t stream;        /* realisation stream (ensembles), 0 by default */
@@ -154,6 +160,15 @@ int scarl_unity_partition_weights(const int Np[3], const int Np_ovlp[3], int par
  * spectrum box and delta_k of the Shino generator (k_cut clamped to k_max). */
 int scarl_shino_sizes(const int Np[3], const double xRange[3], const double corrL[3],
                       int sz_c[3], int sz_Sk[3], double delta_k[3]);
+
+/* Padded periodic grid of a tile (no counterpart in the reference beyond
+ * the FULL rule of SRC_F/fftw_ScaRL.f90:194).  AUTO: smallest power of two
+ * P >= 8 per axis with C((P - Np + 1) xStep) <= tol, C the target model's
+ * unit-variance correlation along that axis. */
+int scarl_pad_size(int policy, int corrMod, double nu, const double corrL[3],
+                   const double xStep[3], const int Np[3], double tol, int P[3]);
+/* Target model correlation at lag r along an axis of integral scale l. */
+double scarl_axis_correlation(int corrMod, double nu, double l, double r);
 
 /* ------------------------------------------------------------------ */
 /* [host] Input decks (SRC_F/read_input.f90)                           */

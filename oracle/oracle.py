@@ -37,7 +37,7 @@ def _declare(L):
     L.so_pm_jump.restype = C.c_int32
     L.so_pm_jump.argtypes = [C.c_int32, C.c_uint64]
     L.so_philox4x32_10.argtypes = [_u32, _u32, _u32]
-    L.so_normals.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _d]
+    L.so_normals.argtypes = [C.c_uint64, C.c_uint32, _i, _d]
     L.so_uniforms.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _d]
     L.so_verify_inputs.restype = C.c_int
     L.so_verify_inputs.argtypes = [_d, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int, _i, C.c_int]
@@ -133,10 +133,13 @@ def philox(ctr, key):
     return [int(v) for v in o]
 
 
-def normals(seed, stream, first, n):
-    out = np.empty(2 * n)
-    lib().so_normals(seed, stream, first, n, _dp(out))
-    return out.reshape(n, 2)
+def normals(seed, stream, P):
+    """Canonical normals of padded grid P as (P2, P1, P0/2+1, 2) in C order."""
+    p, pp = _ia(P)
+    Hx = int(P[0]) // 2 + 1
+    out = np.empty((int(P[2]), int(P[1]), Hx, 2))
+    lib().so_normals(seed, stream, pp, _dp(out))
+    return out
 
 
 def uniforms(seed, stream, first, n):

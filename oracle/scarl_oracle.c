@@ -116,23 +116,46 @@ static inline double so_u01(uint32_t hi, uint32_t lo) {
   return (double)(a >> 12) * 0x1p-52 + 0x1p-53;
 }
 
-/* Canonical standard-normal pairs of the padded-spectrum generator: mode
- * index m -> Philox(ctr = {m_lo, m_hi, stream, 0}, key = {seed_lo, seed_hi}),
- * Box-Muller on (u1, u2). */
-void so_normals(uint64_t seed, uint32_t stream, uint64_t first, uint64_t n, double* re_im) {
+/* Box-Muller pair from two 32-bit words: u = (w + 1/2) 2^-32. */
+static inline void so_bm(uint32_t a, uint32_t b, double* re, double* im) {
+  double u1 = (double)a * 0x1p-32 + 0x1p-33;
+  double u2 = (double)b * 0x1p-32 + 0x1p-33;
+  double r = sqrt(-2.0 * log(u1));
+  *re = r * cos(2.0 * M_PI * u2);
+  *im = r * sin(2.0 * M_PI * u2);
+}
+
+/* Canonical standard normals of the padded spectrum: modes (kx, ky, kz0) and
+ * (kx, ky, kz0 + P2/2), kz0 < P2/2, share the draw
+ * Philox(ctr = {c_lo, c_hi, stream, 0}, key = {seed_lo, seed_hi}) with
+ * c = kx + Hx (ky + P1 kz0); words (0,1) feed the first mode, (2,3) the
+ * second.  out = {re0, im0, re1, im1}. */
+static inline void so_mode_pair(const uint32_t key[2], uint32_t stream, int kx, int ky, int kz0,
+                                int Hx, int P1, double out[4]) {
+  const uint64_t c = (uint64_t)kx + (uint64_t)Hx * ((uint64_t)ky + (uint64_t)P1 * kz0);
+  uint32_t ctr[4] = {(uint32_t)c, (uint32_t)(c >> 32), stream, 0u};
+  uint32_t o[4];
+  so_philox4x32_10(ctr, key, o);
+  so_bm(o[0], o[1], out, out + 1);
+  so_bm(o[2], o[3], out + 2, out + 3);
+}
+
+/* All canonical normals of a padded grid P, pairs in mode order
+ * m = kx + Hx (ky + P1 kz). */
+void so_normals(uint64_t seed, uint32_t stream, const int P[3], double* re_im) {
   const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-#pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < (int64_t)n; ++i) {
-    uint64_t m = first + (uint64_t)i;
-    uint32_t ctr[4] = {(uint32_t)m, (uint32_t)(m >> 32), stream, 0u};
-    uint32_t o[4];
-    so_philox4x32_10(ctr, key, o);
-    double u1 = so_u01(o[0], o[1]);
-    double u2 = so_u01(o[2], o[3]);
-    double r = sqrt(-2.0 * log(u1));
-    re_im[2 * i] = r * cos(2.0 * M_PI * u2);
-    re_im[2 * i + 1] = r * sin(2.0 * M_PI * u2);
-  }
+  const int Hx = P[0] / 2 + 1, h = P[2] / 2;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int kz0 = 0; kz0 < h; ++kz0)
+    for (int ky = 0; ky < P[1]; ++ky)
+      for (int kx = 0; kx < Hx; ++kx) {
+        double o[4];
+        so_mode_pair(key, stream, kx, ky, kz0, Hx, P[1], o);
+        int64_t m0 = kx + (int64_t)Hx * (ky + (int64_t)P[1] * kz0);
+        int64_t m1 = kx + (int64_t)Hx * (ky + (int64_t)P[1] * (kz0 + h));
+        re_im[2 * m0] = o[0]; re_im[2 * m0 + 1] = o[1];
+        re_im[2 * m1] = o[2]; re_im[2 * m1 + 1] = o[3];
+      }
 }
 
 /* Canonical uniform phases (counter word 3 = 1) used when the DCT-path
@@ -953,7 +976,7 @@ void so_padded_spectrum(int corrMod, double nu, const int P[3], const double dx[
   double* own = NULL;
   if (!xi) {
     own = (double*)malloc(sizeof(double) * 2 * M);
-    so_normals(seed, stream, 0, (uint64_t)M, own);
+    so_normals(seed, stream, P, own);
     xi = own;
   }
 #pragma omp parallel for schedule(static)
@@ -1001,18 +1024,17 @@ void so_gen_padded_stream(double* out, const int Np[3], const int P[3], const do
 #pragma omp for schedule(static)
     for (int64_t l = 0; l < (int64_t)Hx * P[1]; l += st) {
       const int kx = (int)(l % Hx), ky = (int)(l / Hx);
-      for (int kz = 0; kz < P[2]; ++kz) {
-        const uint64_t m = (uint64_t)kx + (uint64_t)Hx * ((uint64_t)ky + (uint64_t)P[1] * kz);
-        double f[3] = {so_freq(kx, P[0], dx[0]), so_freq(ky, P[1], dx[1]), so_freq(kz, P[2], dx[2])};
-        double g = (kx == 0 || 2 * kx == P[0]) ? 1.0 : M_SQRT1_2;
-        double A = sqrt(so_spectrum(corrMod, nu, corrL, f) * dk3 / norm) * g;
-        uint32_t ctr[4] = {(uint32_t)m, (uint32_t)(m >> 32), stream, 0u};
-        uint32_t o[4];
-        so_philox4x32_10(ctr, key, o);
-        double u1 = so_u01(o[0], o[1]);
-        double u2 = so_u01(o[2], o[3]);
-        double r = sqrt(-2.0 * log(u1));
-        line[kz] = A * (r * cos(2.0 * M_PI * u2)) + I * (A * (r * sin(2.0 * M_PI * u2)));
+      const int h = P[2] / 2;
+      for (int kz0 = 0; kz0 < h; ++kz0) {
+        double nv[4];
+        so_mode_pair(key, stream, kx, ky, kz0, Hx, P[1], nv);
+        for (int half = 0; half < 2; ++half) {
+          const int kz = kz0 + half * h;
+          double f[3] = {so_freq(kx, P[0], dx[0]), so_freq(ky, P[1], dx[1]), so_freq(kz, P[2], dx[2])};
+          double g = (kx == 0 || 2 * kx == P[0]) ? 1.0 : M_SQRT1_2;
+          double A = sqrt(so_spectrum(corrMod, nu, corrL, f) * dk3 / norm) * g;
+          line[kz] = A * nv[2 * half] + I * (A * nv[2 * half + 1]);
+        }
       }
       so_fft_sign(line, P[2], +1);
       for (int z = 0; z < Nz; ++z) T[kx + (int64_t)Hx * (ky + (int64_t)P[1] * z)] = line[z];

@@ -40,7 +40,7 @@ void so_r8vec_uniform_01(int n, int32_t* seed, double* r);
 void so_r8vec_normal_01(int n, int32_t* seed, double* x);
 int32_t so_pm_jump(int32_t state, uint64_t n);
 void so_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
-void so_normals(uint64_t seed, uint32_t stream, uint64_t first, uint64_t n, double* re_im);
+void so_normals(uint64_t seed, uint32_t stream, const int P[3], double* re_im);
 void so_uniforms(uint64_t seed, uint32_t stream, uint64_t first, uint64_t n, double* u);
 
 /* ---------------- index maps ---------------- */

@@ -18,6 +18,7 @@ CM_GAUSSIAN, CM_VON_KARMAN, CM_EXPONENTIAL = 1, 2, 3
 FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
 F32, F64 = 4, 8
 GEN_DCT, GEN_SHINO, GEN_PADDED = 1, 2, 3
+PAD_FULL, PAD_AUTO = 0, 1
 
 
 class Sample(C.Structure):
@@ -42,6 +43,7 @@ class Tile(C.Structure):
 class GenOpts(C.Structure):
     _fields_ = [("generator", C.c_int), ("dtype", C.c_int), ("nb_procs", C.c_int),
                 ("topo_shape", C.c_int * 3), ("pad", C.c_int * 3),
+                ("pad_policy", C.c_int), ("pad_tol", C.c_double),
                 ("no_spectral_normalisation", C.c_int), ("normalize_field", C.c_int),
                 ("stream", C.c_uint32), ("phiK", C.POINTER(C.c_double))]
 
@@ -72,6 +74,8 @@ SIGNATURES = {
     "scarl_tile_geometry": (C.c_int, [C.POINTER(Layout), _dp, C.c_int, C.POINTER(Tile)]),
     "scarl_unity_partition_weights": (C.c_int, [_ip, _ip, C.c_int, _ip, _ip, _dp]),
     "scarl_shino_sizes": (C.c_int, [_ip, _dp, _dp, _ip, _ip, _dp]),
+    "scarl_pad_size": (C.c_int, [C.c_int, C.c_int, C.c_double, _dp, _dp, _ip, C.c_double, _ip]),
+    "scarl_axis_correlation": (C.c_double, [C.c_int, C.c_double, C.c_double, C.c_double]),
     "scarl_read_config": (C.c_int, [C.c_char_p, _ip, _ip, _ip, _ip, _ip, C.c_char_p,
                                     C.c_size_t]),
     "scarl_read_extra_config": (C.c_int, [C.c_char_p, _ip, _ip]),

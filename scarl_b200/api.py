@@ -10,8 +10,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (F32, F64, GEN_DCT, GEN_PADDED, GEN_SHINO, GenOpts, Layout, Sample,
-                   ScarlError, Tile, lib)
+from ._lib import (F32, F64, GEN_DCT, GEN_PADDED, GEN_SHINO, PAD_AUTO, PAD_FULL, GenOpts, Layout,
+                   Sample, ScarlError, Tile, lib)
 
 
 def _check(rc, ctx=None):
@@ -269,9 +269,19 @@ def gen_padded(ctx, Np, xStep, corrL, corrMod=1, nu=0.5, pad=None, normalise=Tru
     return out
 
 
+def pad_size(policy, corrMod, corrL, xStep, Np, nu=0.5, tol=1e-3):
+    P = (C.c_int * 3)()
+    _check(lib().scarl_pad_size(policy, corrMod, nu, _d3(corrL), _d3(xStep), _i3(Np), tol, P))
+    return np.array(P[:], dtype=np.int32)
+
+
+def axis_correlation(corrMod, l, r, nu=0.5):
+    return float(lib().scarl_axis_correlation(corrMod, nu, l, r))
+
+
 def generate_sample(ctx, sample, generator=GEN_PADDED, dtype=F32, nb_procs=1, topo=None,
-                    pad=None, normalise_spectrum=True, normalize_field=False, stream=0,
-                    phiK=None, out=None):
+                    pad=None, pad_policy=PAD_FULL, pad_tol=1e-3, normalise_spectrum=True,
+                    normalize_field=False, stream=0, phiK=None, out=None):
     """One deck sample end to end (layout, tiles, PoU blend, marginal)."""
     lay = sample_layout(sample, 1, nb_procs, topo)
     out = _alloc_out(out, tuple(int(v) for v in lay["L"]), dtype)
@@ -281,6 +291,7 @@ def generate_sample(ctx, sample, generator=GEN_PADDED, dtype=F32, nb_procs=1, to
         o.topo_shape = _i3(topo)
     if pad is not None:
         o.pad = _i3(pad)
+    o.pad_policy, o.pad_tol = int(pad_policy), float(pad_tol)
     o.no_spectral_normalisation = 0 if normalise_spectrum else 1
     o.normalize_field = int(bool(normalize_field))
     o.stream = int(stream)

@@ -521,20 +521,21 @@ struct BlendTabs {
 
 int upload_blend_tables(scarl_ctx* ctx, const scarl_layout& lay, int partitionType,
                         std::vector<BlendAxis>* axes) {
+  // per tile and axis: lo, hi, sqrt(lo*hi) as doubles; sqrt(lo*hi) as
+  // floats; flags as bytes -- three sections of one upload
   const int nb = lay.nb_tiles;
-  size_t nd = 0, nf = 0;
-  for (int d = 0; d < 3; ++d) {
-    nd += 2 * (size_t)lay.Np[d];
-    nf += (size_t)lay.Np[d];
-  }
-  const size_t dbytes = nd * 8 * nb;
-  const size_t fbytes = round_up((int)(nf * nb), 16);
-  const size_t total = dbytes + fbytes;
+  size_t nsum = 0;
+  for (int d = 0; d < 3; ++d) nsum += (size_t)lay.Np[d];
+  const size_t dbytes = 3 * nsum * 8 * nb;
+  const size_t fbytes = (nsum * 4 * nb + 15) / 16 * 16;
+  const size_t bbytes = (nsum * nb + 15) / 16 * 16;
+  const size_t total = dbytes + fbytes + bbytes;
   void* hp;
   RC(pinned(ctx, total, &hp));
   RC(ensure(ctx, ctx->tabs, total));
   double* hd = (double*)hp;
-  uint8_t* hf = (uint8_t*)hp + dbytes;
+  float* hf = (float*)((char*)hp + dbytes);
+  uint8_t* hb = (uint8_t*)hp + dbytes + fbytes;
   const char* dbase = (const char*)ctx->tabs.p;
   axes->resize((size_t)nb * 3);
   size_t od = 0, of = 0;
@@ -543,13 +544,22 @@ int upload_blend_tables(scarl_ctx* ctx, const scarl_layout& lay, int partitionTy
     get_topo_pos(r, lay.topo_shape, pos);
     for (int d = 0; d < 3; ++d) {
       const int Np = lay.Np[d];
-      pou_axis_tables(Np, lay.Np_ovlp[d], pos[d], lay.topo_shape[d], partitionType, hd + od, hd + od + Np);
-      blend_axis_flags(Np, lay.Np_ovlp[d], pos[d], lay.topo_shape[d], hf + of);
+      double* lo = hd + od;
+      double* hi = lo + Np;
+      double* sw = hi + Np;
+      pou_axis_tables(Np, lay.Np_ovlp[d], pos[d], lay.topo_shape[d], partitionType, lo, hi);
+      for (int x = 0; x < Np; ++x) {
+        sw[x] = std::sqrt(lo[x] * hi[x]);
+        hf[of + x] = (float)sw[x];
+      }
+      blend_axis_flags(Np, lay.Np_ovlp[d], pos[d], lay.topo_shape[d], hb + of);
       BlendAxis& ax = (*axes)[(size_t)r * 3 + d];
       ax.lo = (const double*)(dbase + od * 8);
       ax.hi = (const double*)(dbase + (od + Np) * 8);
-      ax.flags = (const uint8_t*)(dbase + dbytes + of);
-      od += 2 * (size_t)Np;
+      ax.sw64 = (const double*)(dbase + (od + 2 * (size_t)Np) * 8);
+      ax.sw32 = (const float*)(dbase + dbytes + of * 4);
+      ax.flags = (const uint8_t*)(dbase + dbytes + fbytes + of);
+      od += 3 * (size_t)Np;
       of += (size_t)Np;
     }
   }
@@ -812,6 +822,16 @@ int scarl_shino_sizes(const int Np[3], const double xRange[3], const double corr
   return SCARL_OK;
 }
 
+int scarl_pad_size(int policy, int corrMod, double nu, const double corrL[3],
+                   const double xStep[3], const int Np[3], double tol, int P[3]) {
+  if (!corrL || !xStep || !Np || !P) return SCARL_EINVAL;
+  return pad_size(policy, corrMod, nu, corrL, xStep, Np, tol, P);
+}
+
+double scarl_axis_correlation(int corrMod, double nu, double l, double r) {
+  return axis_correlation(corrMod, nu, l, r);
+}
+
 int scarl_read_config(const char* path, int* gen_meth, int* c_info_file, int* d_sample,
                       int* one_file, int* one_hdf_ds, char* input_file, size_t len) {
   if (!path || !gen_meth || !c_info_file || !d_sample || !one_file || !one_hdf_ds) return SCARL_EINVAL;
@@ -988,7 +1008,11 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   PaddedPlan* pl = nullptr;
   int P[3];
   if (gen == SCARL_GEN_PADDED) {
-    for (int d = 0; d < 3; ++d) P[d] = o.pad[d] > 0 ? o.pad[d] : default_pad(lay.Np[d]);
+    int Pp[3];
+    const double tol = o.pad_tol > 0.0 ? o.pad_tol : 1e-3;
+    if (pad_size(o.pad_policy, s->corrMod, s->nu, s->corrL, lay.xStep, lay.Np, tol, Pp) != SCARL_OK)
+      return fail(ctx, SCARL_EINVAL, "invalid padding policy or tolerance");
+    for (int d = 0; d < 3; ++d) P[d] = o.pad[d] > 0 ? o.pad[d] : Pp[d];
     RC(check_grid(ctx, P, lay.Np));
     for (int d = 0; d < 3; ++d)
       if (!(s->corrL[d] > 0.0)) return fail(ctx, SCARL_EINVAL, "corrL must be > 0");
@@ -1070,6 +1094,8 @@ int scarl_apply_unity_partition(scarl_ctx* ctx, double* field, const int Np[3],
     ax[d].lo = (const double*)ctx->tabs.p + od;
     ax[d].hi = (const double*)ctx->tabs.p + od + Np[d];
     ax[d].flags = nullptr;
+    ax[d].sw64 = nullptr;
+    ax[d].sw32 = nullptr;
     od += 2 * (size_t)Np[d];
   }
   RC(upload_pinned(ctx, ctx->tabs.p, nd * 8));

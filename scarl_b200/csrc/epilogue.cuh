@@ -20,30 +20,69 @@ __device__ __forceinline__ T marginal_apply(const Epilogue& e, T v) {
   return v;
 }
 
+template <typename T> __device__ __forceinline__ const T* sw_of(const BlendAxis& a);
+template <> __device__ __forceinline__ const float* sw_of<float>(const BlendAxis& a) { return a.sw32; }
+template <> __device__ __forceinline__ const double* sw_of<double>(const BlendAxis& a) { return a.sw64; }
+
+// Output stage of one tile line (fixed y, z; x varies).  In blend mode the
+// partition-of-unity factor is the product of the per-axis sqrt factors,
+// sqrt(w) = s_x s_y s_z, with s_d = sqrt(lo_d hi_d) computed in FP64 on the
+// host (equal to sqrt of the reference's product up to rounding).
+template <typename T>
+struct LineEpilogue {
+  T* out;
+  size_t base;        // output index of x = 0
+  uint8_t fyz;        // flags of y and z, AND-ed
+  T syz;              // s_y s_z
+  const uint8_t* fx;  // flags along x (blend)
+  const T* sx;        // s_x (blend)
+  int mode, marginal, pou;
+  T ms, mu;
+
+  __device__ __forceinline__ LineEpilogue(const Epilogue& e, int y, int z, int Nx, int Ny) {
+    out = static_cast<T*>(e.out);
+    mode = e.mode;
+    marginal = e.marginal;
+    ms = (T)e.ms;
+    mu = (T)e.mmu;
+    pou = e.apply_pou;
+    if (mode == 0) {
+      base = (size_t)Nx * ((size_t)y + (size_t)Ny * z);
+      fyz = 7;
+      syz = T(1);
+      fx = nullptr;
+      sx = nullptr;
+    } else {
+      base = (size_t)e.off[0] + (size_t)e.L[0] * ((size_t)(e.off[1] + y) + (size_t)e.L[1] * (size_t)(e.off[2] + z));
+      fyz = e.ax[1].flags[y] & e.ax[2].flags[z];
+      syz = pou ? sw_of<T>(e.ax[1])[y] * sw_of<T>(e.ax[2])[z] : T(1);
+      fx = e.ax[0].flags;
+      sx = sw_of<T>(e.ax[0]);
+    }
+  }
+  __device__ __forceinline__ T marg(T v) const {
+    if (marginal == 1) return v * ms + mu;
+    if (marginal == 2) return exp(v * ms + mu);
+    return v;
+  }
+  __device__ __forceinline__ void put(int x, T v) const {
+    if (mode == 0) {
+      out[base + x] = marg(v);
+      return;
+    }
+    const uint8_t f = fyz & fx[x];
+    if (!(f & 1)) return;
+    if (pou) v = v * (syz * sx[x]);
+    if (!(f & 2)) v = out[base + x] + v;
+    if (f & 4) v = marg(v);
+    out[base + x] = v;
+  }
+};
+
 template <typename T>
 __device__ __forceinline__ void epilogue_point(const Epilogue& e, int x, int y, int z, int Nx,
                                                int Ny, T v) {
-  if (e.mode == 0) {
-    static_cast<T*>(e.out)[(size_t)x + (size_t)Nx * ((size_t)y + (size_t)Ny * z)] = marginal_apply(e, v);
-    return;
-  }
-  const uint8_t f = e.ax[0].flags[x] & e.ax[1].flags[y] & e.ax[2].flags[z];
-  if (!(f & 1)) return;
-  if (e.apply_pou) {
-    double w = e.ax[0].lo[x];
-    w = __dmul_rn(w, e.ax[1].lo[y]);
-    w = __dmul_rn(w, e.ax[2].lo[z]);
-    w = __dmul_rn(w, e.ax[0].hi[x]);
-    w = __dmul_rn(w, e.ax[1].hi[y]);
-    w = __dmul_rn(w, e.ax[2].hi[z]);
-    if (w != 1.0) v = (T)((double)v * sqrt(w));
-  }
-  const size_t g = (size_t)(e.off[0] + x) +
-                   (size_t)e.L[0] * ((size_t)(e.off[1] + y) + (size_t)e.L[1] * (size_t)(e.off[2] + z));
-  T* o = static_cast<T*>(e.out);
-  if (!(f & 2)) v = o[g] + v;
-  if (f & 4) v = marginal_apply(e, v);
-  o[g] = v;
+  LineEpilogue<T>(e, y, z, Nx, Ny).put(x, v);
 }
 
 }  // namespace scarl

@@ -118,8 +118,10 @@ __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, i
   __syncthreads();
 }
 
-// Full line transform.  load(n) -> C for the first stage, store(n, C) for the
-// last.  sm holds B lines laid out by O.  All threads of the block must call.
+// Full line transform.  load(j, v) fills the first stage's R1 inputs
+// v[r] = x[j + r N/R1] (r < R1, R1 = StagePlan<N,E>::radix(0)); store(n, C)
+// takes each output of the last stage.  sm holds B lines laid out by O.  All
+// threads of the block must call.
 template <typename C, int N, int E, SmemOrder O, int B, int LS, class Load, class Store>
 __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, const C* __restrict__ tw,
                                           int twmul, Load&& load, Store&& store) {
@@ -129,11 +131,7 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
   constexpr int NB1 = E / R1;
   C v[E];
 #pragma unroll
-  for (int q = 0; q < NB1; ++q) {
-    const int j = t + TPL * q;
-#pragma unroll
-    for (int r = 0; r < R1; ++r) v[q * R1 + r] = load(j + r * (N / R1));
-  }
+  for (int q = 0; q < NB1; ++q) load(t + TPL * q, v + q * R1);
   if constexpr (P::S == 1) {
 #pragma unroll
     for (int q = 0; q < NB1; ++q) {
@@ -185,6 +183,21 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
       for (int r = 0; r < RL; ++r) store(j + r * NsL, v[q * RL + brev<RL>(r)]);
     }
   }
+}
+
+// Adapts a per-element loader f(n) -> C to the group interface of line_ifft.
+template <typename C, int N, int E, class F>
+struct EachLoad {
+  F f;
+  __device__ __forceinline__ void operator()(int j, C* v) const {
+    constexpr int R1 = StagePlan<N, E>::radix(0);
+#pragma unroll
+    for (int r = 0; r < R1; ++r) v[r] = f(j + r * (N / R1));
+  }
+};
+template <typename C, int N, int E, class F>
+__device__ __forceinline__ EachLoad<C, N, E, F> each_load(F f) {
+  return EachLoad<C, N, E, F>{f};
 }
 
 }  // namespace scarl

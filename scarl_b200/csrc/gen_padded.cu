@@ -58,8 +58,12 @@ __device__ __forceinline__ cplx_t<T> shino_mode(const GenArgs& a, int kx, int ky
   return mk((T)(0.5 * re), (T)(0.5 * im));
 }
 
+template <typename T> __device__ __forceinline__ T fast_div(T a, T b);
+template <> __device__ __forceinline__ float fast_div<float>(float a, float b) { return __fdividef(a, b); }
+template <> __device__ __forceinline__ double fast_div<double>(double a, double b) { return a / b; }
+
 template <typename T> __device__ __forceinline__ T powT(T s, T e);
-template <> __device__ __forceinline__ float powT<float>(float s, float e) { return __powf(s, e); }
+template <> __device__ __forceinline__ float powT<float>(float s, float e) { return powf(s, e); }
 template <> __device__ __forceinline__ double powT<double>(double s, double e) { return pow(s, e); }
 
 // ---------------------------------------------------------------------------
@@ -90,20 +94,42 @@ __global__ void __launch_bounds__(B*(N / E)) k_gen_z(const GenArgs a) {
   }
   const uint64_t mrow = (uint64_t)kx + (uint64_t)a.Hx * (uint64_t)ky;
   const uint64_t mz = (uint64_t)a.Hx * (uint64_t)a.P[1];
-  auto load = [&](int kz) -> C {
-    if (!valid) return mk(T(0), T(0));
-    if constexpr (SPEC == SPEC_SHINO) {
-      return shino_mode<T>(a, kx, ky, kz);
-    } else {
-      T A;
-      if (a.amp == AMP_SEPARABLE) A = fx * fy * az[kz];
-      else if (a.amp == AMP_RECIP) A = fx / (fy + qz[kz]);
-      else A = fx * powT<T>(fy + qz[kz], (T)a.expo);
-      const uint64_t m = mrow + mz * (uint64_t)kz;
-      C xi;
-      if constexpr (SPEC == SPEC_INJECT) xi = static_cast<const C*>(a.xi)[m];
-      else xi = Normals<T>::pair(m, a.stream, a.k0, a.k1);
-      return mk(A * xi.x, A * xi.y);
+  auto amp = [&](int kz) -> T {
+    if (a.amp == AMP_SEPARABLE) return fx * fy * az[kz];
+    if (a.amp == AMP_RECIP) return fast_div(fx, fy + qz[kz]);
+    return fx * powT<T>(fy + qz[kz], (T)a.expo);
+  };
+  // First-stage inputs kz = j + r N/R1; r and r + R1/2 are kz and kz + N/2,
+  // the two modes of one Philox draw.
+  auto load = [&](int j, C* v) {
+    constexpr int R1 = StagePlan<N, E>::radix(0);
+    constexpr int H = R1 / 2;
+#pragma unroll
+    for (int r = 0; r < H; ++r) {
+      const int kz0 = j + r * (N / R1), kz1 = kz0 + N / 2;
+      if (!valid) {
+        v[r] = mk(T(0), T(0));
+        v[r + H] = mk(T(0), T(0));
+        continue;
+      }
+      if constexpr (SPEC == SPEC_SHINO) {
+        v[r] = shino_mode<T>(a, kx, ky, kz0);
+        v[r + H] = shino_mode<T>(a, kx, ky, kz1);
+      } else {
+        C x0, x1;
+        if constexpr (SPEC == SPEC_INJECT) {
+          x0 = static_cast<const C*>(a.xi)[mrow + mz * (uint64_t)kz0];
+          x1 = static_cast<const C*>(a.xi)[mrow + mz * (uint64_t)kz1];
+        } else {
+          const uint64_t c = mrow + mz * (uint64_t)kz0;
+          const u32x4 o = philox4x32_10({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.k0, a.k1);
+          x0 = Normals<T>::from(o.x, o.y);
+          x1 = Normals<T>::from(o.z, o.w);
+        }
+        const T A0 = amp(kz0), A1 = amp(kz1);
+        v[r] = mk(A0 * x0.x, A0 * x0.y);
+        v[r + H] = mk(A1 * x1.x, A1 * x1.y);
+      }
     }
   };
   const int Nz = a.Nout[2];
@@ -118,7 +144,7 @@ __global__ void __launch_bounds__(B*(N / E)) k_gen_z(const GenArgs a) {
 // Pass 2: inverse DFT along y, in place, keep y < Ny.
 // ---------------------------------------------------------------------------
 template <typename T, int N, int E, int B>
-__global__ void __launch_bounds__(B*(N / E)) k_mid_y(const GenArgs a) {
+__global__ void __launch_bounds__(B*(N / E), (B * (N / E) >= 512 ? 2 : 1)) k_mid_y(const GenArgs a) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
@@ -129,7 +155,7 @@ __global__ void __launch_bounds__(B*(N / E)) k_mid_y(const GenArgs a) {
   C* col = static_cast<C*>(a.work) + (size_t)z * a.P[1] * a.Hpad + kx;
   const size_t pitch = (size_t)a.Hpad;
   const int Ny = a.Nout[1];
-  auto load = [&](int ky) -> C { return valid ? col[(size_t)ky * pitch] : mk(T(0), T(0)); };
+  auto load = each_load<C, N, E>([&](int ky) -> C { return valid ? col[(size_t)ky * pitch] : mk(T(0), T(0)); });
   auto store = [&](int y, C v) {
     if (valid && y < Ny) col[(size_t)y * pitch] = v;
   };
@@ -150,36 +176,31 @@ __global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
   const int Nx = a.Nout[0], Ny = a.Nout[1], Nz = a.Nout[2];
   const int64_t nlines = (int64_t)Ny * Nz;
   const C* work = static_cast<const C*>(a.work);
-  for (int idx = threadIdx.x; idx < B * LS; idx += blockDim.x) {
-    const int bb = idx / LS, k = idx - bb * LS;
-    const int64_t l = (int64_t)blockIdx.x * B + bb;
-    C v = mk(T(0), T(0));
-    if (l < nlines) {
-      const int64_t y = l % Ny, z = l / Ny;
-      v = work[((size_t)z * a.P[1] + (size_t)y) * a.Hpad + k];
-    }
-    sm[bb * LS + k] = v;
-  }
-  __syncthreads();
   const int b = threadIdx.x / TPL, t = threadIdx.x % TPL;
   const int64_t l = (int64_t)blockIdx.x * B + b;
   const bool valid = l < nlines;
   const int y = valid ? (int)(l % Ny) : 0, z = valid ? (int)(l / Ny) : 0;
+  {  // stage the raw half-spectrum line (N + 1 values), coalesced per line
+    const C* src = work + ((size_t)z * a.P[1] + (size_t)y) * a.Hpad;
+    for (int k = t; k < LS; k += TPL) sm[b * LS + k] = valid ? src[k] : mk(T(0), T(0));
+  }
+  __syncthreads();
   const C* twx = static_cast<const C*>(a.tw_x);
   const C* line = sm + b * LS;
-  auto load = [&](int k) -> C {
+  auto load = each_load<C, N, E>([&](int k) -> C {
     const C xk = line[k], xn = line[N - k];
     if (k == 0) return mk(xk.x + xn.x, xk.x - xn.x);
     const C xc = cconj(xn);
     const C e = cadd(xk, xc);
     const C o = cmul(csub(xk, xc), __ldg(twx + k));
     return mk(e.x - o.y, e.y + o.x);
-  };
+  });
+  const LineEpilogue<T> ep(a.epi, y, z, Nx, Ny);
   auto store = [&](int n, C v) {
     if (!valid) return;
     const int x0 = 2 * n;
-    if (x0 < Nx) epilogue_point<T>(a.epi, x0, y, z, Nx, Ny, v.x);
-    if (x0 + 1 < Nx) epilogue_point<T>(a.epi, x0 + 1, y, z, Nx, Ny, v.y);
+    if (x0 < Nx) ep.put(x0, v.x);
+    if (x0 + 1 < Nx) ep.put(x0 + 1, v.y);
   };
   line_ifft<C, N, E, SmemOrder::LineFast, B, LS>(sm, b, t, twx, 2, load, store);
 }

@@ -273,6 +273,59 @@ int shino_sizes(const int Np[3], const double xRange[3], const double corrL[3], 
 }
 
 // ---------------------------------------------------------------------------
+// Padded grid sizes
+// ---------------------------------------------------------------------------
+// K_nu(x) from K_nu(x) = int_0^inf exp(-x cosh t) cosh(nu t) dt (trapezoid;
+// the integrand is smooth and decays doubly exponentially).
+static double bessel_k(double nu, double x) {
+  const double h = 1.0 / 64.0;
+  double s = 0.5 * std::exp(-x);
+  for (int i = 1; i < 64 * 40; ++i) {
+    const double t = i * h;
+    const double e = x * std::cosh(t);
+    if (e > 745.0) break;
+    s += std::exp(-e) * std::cosh(nu * t);
+  }
+  return s * h;
+}
+
+// Unit-variance correlation at lag r along an axis with integral scale l.
+double axis_correlation(int corrMod, double nu, double l, double r) {
+  if (r <= 0.0) return 1.0;
+  if (corrMod == SCARL_CM_GAUSSIAN) return std::exp(-M_PI * r * r / (l * l));
+  if (corrMod == SCARL_CM_EXPONENTIAL) return std::exp(-2.0 * r / l);
+  const double a = l * std::tgamma(nu) / (2.0 * std::sqrt(M_PI) * std::tgamma(nu + 0.5));
+  const double x = r / a;
+  if (x > 700.0) return 0.0;
+  return std::pow(2.0, 1.0 - nu) / std::tgamma(nu) * std::pow(x, nu) * bessel_k(nu, x);
+}
+
+// policy 0: the reference's 2^ceil(log2(2 Np)) (SRC_F/fftw_ScaRL.f90:194).
+// policy 1: smallest power of two P >= 8 with C((P - Np + 1) dx) <= tol along
+// each axis: the nearest periodic image of the farthest pair of tile points
+// then contributes at most tol to the covariance.
+int pad_size(int policy, int corrMod, double nu, const double corrL[3], const double xStep[3],
+             const int Np[3], double tol, int P[3]) {
+  for (int d = 0; d < 3; ++d) {
+    if (Np[d] < 1) return SCARL_EINVAL;
+    int p = 8;
+    if (policy == 0) {
+      while (p < 2 * Np[d]) p <<= 1;
+    } else if (policy == 1) {
+      if (!(tol > 0.0 && tol < 1.0) || !(corrL[d] > 0.0) || !(xStep[d] > 0.0)) return SCARL_EINVAL;
+      while (p < Np[d] || axis_correlation(corrMod, nu, corrL[d], (p - Np[d] + 1) * xStep[d]) > tol) {
+        p <<= 1;
+        if (p > (1 << 24)) return SCARL_EINVAL;
+      }
+    } else {
+      return SCARL_EINVAL;
+    }
+    P[d] = p;
+  }
+  return SCARL_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Plain-text decks: getLine (SRC_F/read_input.f90:565-585) plus Fortran
 // list-directed reads of the returned record.
 // ---------------------------------------------------------------------------

@@ -68,17 +68,17 @@ __device__ __forceinline__ double u01_d(uint32_t hi, uint32_t lo) {
   const uint64_t a = ((uint64_t)hi << 32) | lo;
   return (double)(a >> 12) * 0x1p-52 + 0x1p-53;
 }
-// Single-precision view of the same draw: the top 23 bits plus a half offset.
-__device__ __forceinline__ float u01_f(uint32_t hi) {
-  return (float)(hi >> 9) * 0x1p-23f + 0x1p-24f;
-}
-
-// Standard-normal pair (re, im) of mode m: Box-Muller on Philox(m).
+// Canonical standard normals of the padded spectrum.  Modes (kx, ky, kz) and
+// (kx, ky, kz + P2/2), kz < P2/2, share one Philox draw
+//   Philox(ctr = {c_lo, c_hi, stream, 0}, key),  c = kx + Hx (ky + P1 kz),
+// words (x, y) feeding the first and (z, w) the second mode; each word pair
+// (a, b) gives u1 = (a + 1/2) 2^-32, u2 = (b + 1/2) 2^-32 and the Box-Muller
+// pair r (cos 2 pi u2, sin 2 pi u2), r = sqrt(-2 ln u1).
 template <typename T> struct Normals;
 template <> struct Normals<double> {
-  static __device__ __forceinline__ double2 pair(uint64_t m, uint32_t stream, uint32_t k0, uint32_t k1) {
-    const u32x4 o = philox4x32_10({(uint32_t)m, (uint32_t)(m >> 32), stream, 0u}, k0, k1);
-    const double u1 = u01_d(o.x, o.y), u2 = u01_d(o.z, o.w);
+  static __device__ __forceinline__ double2 from(uint32_t a, uint32_t b) {
+    const double u1 = (double)a * 0x1p-32 + 0x1p-33;
+    const double u2 = (double)b * 0x1p-32 + 0x1p-33;
     const double r = sqrt(-2.0 * log(u1));
     double s, c;
     sincospi(2.0 * u2, &s, &c);
@@ -86,13 +86,17 @@ template <> struct Normals<double> {
   }
 };
 template <> struct Normals<float> {
-  static __device__ __forceinline__ float2 pair(uint64_t m, uint32_t stream, uint32_t k0, uint32_t k1) {
-    const u32x4 o = philox4x32_10({(uint32_t)m, (uint32_t)(m >> 32), stream, 0u}, k0, k1);
-    const float u1 = u01_f(o.x), u2 = u01_f(o.z);
+  // Single precision, hardware transcendentals: u1 is formed with one
+  // rounding (relative error 2^-24, so small u1 keep their digits); the
+  // phase is reduced to (-pi, pi) where __sincosf is accurate, and the
+  // half-turn folded back by the sign.
+  static __device__ __forceinline__ float2 from(uint32_t a, uint32_t b) {
+    const float u1 = __fmaf_rn((float)a, 0x1p-32f, 0x1p-33f);
+    const float u2 = __fmaf_rn((float)b, 0x1p-32f, 0x1p-33f);
     const float r = sqrtf(-2.0f * __logf(u1));
     float s, c;
-    sincospif(2.0f * u2, &s, &c);
-    return make_float2(r * c, r * s);
+    __sincosf(6.28318530717958647692f * (u2 - 0.5f), &s, &c);
+    return make_float2(-r * c, -r * s);
   }
 };
 

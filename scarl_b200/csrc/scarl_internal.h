@@ -16,6 +16,8 @@ struct BlendAxis {
   const double* lo;
   const double* hi;
   const uint8_t* flags;
+  const double* sw64;  // sqrt(lo * hi): the axis' factor of sqrt(weight)
+  const float* sw32;
 };
 
 struct Epilogue {

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared():
     txt = open(os.path.join(ROOT, "include", "scarl.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(scarl_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|double|const char\*)\s+(scarl_\w+)\s*\(", txt, re.M)))
 
 
 def test_every_declared_symbol_is_exported():

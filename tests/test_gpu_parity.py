@@ -16,9 +16,11 @@ TOL32 = 1e-5
 
 
 def rel(a, b):
+    """rel-L2 error, scaled first so that huge fields cannot overflow the norm."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
-    return np.linalg.norm(a - b) / np.linalg.norm(b)
+    s = np.max(np.abs(b))
+    return np.linalg.norm((a - b) / s) / np.linalg.norm(b / s)
 
 
 # ---------------------------------------------------------------------------
@@ -43,6 +45,11 @@ def test_gen_padded_injected_golden(ctx, tag, dtype, tol):
     ((16, 16, 16), (32, 32, 32), (1, 1, 1), (4, 4, 4), 2, 0.3),
     ((100, 7, 9), (256, 16, 32), (1, 1, 1), (10, 2, 3), 3, 0.5),
     ((5, 60, 3), (32, 128, 32), (1, 1, 1), (2, 10, 2), 1, 0.5),
+    ((300, 6, 5), (512, 16, 16), (1, 1, 1), (40, 3, 3), 3, 0.5),
+    ((600, 5, 4), (2048, 8, 8), (1, 1, 1), (60, 2, 2), 3, 0.5),
+    ((6, 400, 5), (16, 1024, 16), (1, 1, 1), (3, 30, 3), 2, 0.8),
+    ((5, 6, 700), (16, 16, 2048), (1, 1, 1), (3, 3, 50), 1, 0.5),
+    ((7, 5, 297), (16, 8, 1024), (1, 1, 1), (3, 3, 10), 3, 0.5),
 ])
 def test_gen_padded_philox_vs_oracle(ctx, oracle, Np, P, dx, cl, cm, nu):
     ref = oracle.gen_padded(Np, P, dx, cl, cm, nu, 1, seed=77, stream=3)
@@ -296,3 +303,15 @@ def test_error_paths(ctx):
         assert e.value.code == 2
     finally:
         small.close()
+
+
+@pytest.mark.parametrize("cm,nu", [(3, 0.5), (1, 0.5), (2, 1.2)])
+def test_generate_sample_auto_padding_vs_oracle(ctx, oracle, cm, nu):
+    args = ((0, 0, 0), (40, 30, 20), (6, 4, 3), (1, 1, 1), (7, 5, 4))
+    s = S.make_sample(*args, cm, 2, 1.0, 0.3, 9, nu)
+    lay = S.sample_layout(s, 1, 8)
+    P = S.pad_size(S.PAD_AUTO, cm, args[2], lay["xStep"], lay["Np"], nu, 1e-3)
+    assert np.prod(P) < np.prod(S.pad_size(S.PAD_FULL, cm, args[2], lay["xStep"], lay["Np"]))
+    ref, _ = oracle.generate_sample(3, *args, cm, nu, 2, 1.0, 0.3, 9, 8, None, pad=P)
+    out, _ = S.generate_sample(ctx, s, dtype=S.F64, nb_procs=8, pad_policy=S.PAD_AUTO)
+    assert rel(out, ref) < TOL64

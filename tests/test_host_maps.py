@@ -176,3 +176,28 @@ def test_rebuild_corrL_matches_oracle(oracle):
     xs = [0.5, 1.0, 2.0]
     np.testing.assert_array_equal(S.rebuild_corrL(sk, L, xs),
                                   oracle.rebuild_corrL(sk, [v // 2 for v in L], xs))
+
+
+@pytest.mark.parametrize("cm,nu", [(1, 0.5), (3, 0.5), (2, 0.3), (2, 1.5)])
+def test_pad_size_auto_is_minimal(cm, nu):
+    """AUTO picks the smallest power of two whose nearest periodic image of the
+    farthest tile pair has correlation <= tol (checked against scipy)."""
+    from scipy.special import gamma, kv
+
+    def corr(l, r):
+        if cm == 1:
+            return np.exp(-np.pi * r * r / (l * l))
+        v = 0.5 if cm == 3 else nu
+        a = l * gamma(v) / (2 * np.sqrt(np.pi) * gamma(v + 0.5))
+        x = r / a
+        return 2 ** (1 - v) / gamma(v) * x ** v * kv(v, x)
+    for Np, cl, dx in [((297, 277, 267), (40, 20, 10), (1, 1, 1)), ((50, 9, 120), (3, 7, 12), (0.5, 1, 2))]:
+        for tol in (1e-2, 1e-3, 1e-6):
+            P = S.pad_size(S.PAD_AUTO, cm, cl, dx, Np, nu, tol)
+            for d in range(3):
+                assert P[d] >= 8 and P[d] & (P[d] - 1) == 0 and P[d] >= Np[d]
+                assert corr(cl[d], (P[d] - Np[d] + 1) * dx[d]) <= tol * (1 + 1e-9)
+                if P[d] > 8 and P[d] // 2 >= Np[d]:
+                    assert corr(cl[d], (P[d] // 2 - Np[d] + 1) * dx[d]) > tol
+    full = S.pad_size(S.PAD_FULL, cm, (40, 20, 10), (1, 1, 1), (297, 277, 267))
+    assert list(full) == [1024, 1024, 1024]

@@ -62,10 +62,16 @@ def test_philox_kat(oracle, ctr, key, expect):
 
 
 def test_normals_distribution(oracle):
-    z = oracle.normals(5, 0, 0, 200000)
+    P = [128, 64, 64]
+    z = oracle.normals(5, 0, P)
     assert abs(z.mean()) < 0.01 and abs(z.std() - 1) < 0.01
-    np.testing.assert_array_equal(oracle.normals(5, 0, 100, 10), z[100:110])
-    assert not np.array_equal(oracle.normals(5, 1, 0, 10), z[:10])
+    # modes kz and kz + P2/2 come from one draw, all pairs distinct
+    assert not np.array_equal(z[0], z[32])
+    assert not np.array_equal(oracle.normals(5, 1, P)[:2], z[:2])
+    # padded spectrum with these normals equals the injected-normals path
+    H1 = oracle.padded_spectrum(3, 0.5, P, [1, 1, 1], [4, 4, 4], 1, 5, 0)
+    H2 = oracle.padded_spectrum(3, 0.5, P, [1, 1, 1], [4, 4, 4], 1, 0, 0, xi=z.reshape(-1))
+    np.testing.assert_array_equal(H1, H2)
 
 
 @pytest.mark.parametrize("n", [1, 2, 7, 37, 64, 297])
