@@ -46,7 +46,7 @@ def load_peaks():
 
 
 class Clocks:
-    """nvidia-smi samples (200 ms) while the timed region runs."""
+    """nvidia-smi samples (50 ms) while the timed region runs."""
 
     FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -63,7 +63,7 @@ class Clocks:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200", "-f", self.path],
+                 "-lms", "50", "-f", self.path],
                 stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -200,8 +200,8 @@ def config_of(lay, P):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="scarl", choices=["scarl", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

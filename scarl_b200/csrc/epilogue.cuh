@@ -65,6 +65,32 @@ struct LineEpilogue {
     if (marginal == 2) return exp(v * ms + mu);
     return v;
   }
+  // K outputs at once: every read of an earlier tile's partial sum is issued
+  // before any write.
+  template <int K>
+  __device__ __forceinline__ void put_group(const int* xs, const T* v, int Nx) const {
+    if (mode == 0) {
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if (xs[i] < Nx) out[base + xs[i]] = marg(v[i]);
+      return;
+    }
+    uint8_t f[K];
+    T old[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      f[i] = xs[i] < Nx ? (uint8_t)(fyz & fx[xs[i]]) : (uint8_t)0;
+      old[i] = ((f[i] & 3) == 1) ? out[base + xs[i]] : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      if (!(f[i] & 1)) continue;
+      T w = pou ? v[i] * (syz * sx[xs[i]]) : v[i];
+      if (!(f[i] & 2)) w = old[i] + w;
+      if (f[i] & 4) w = marg(w);
+      out[base + xs[i]] = w;
+    }
+  }
   __device__ __forceinline__ void put(int x, T v) const {
     if (mode == 0) {
       out[base + x] = marg(v);

@@ -77,18 +77,24 @@ template <int N, int E> struct StagePlan {
   static constexpr int S = count();
 };
 
-// Shared-memory addressing of line element n of line b.
-//   BatchFast: element (n, b) at n*B + b  (lanes of a warp span lines)
-//   LineFast : element (n, b) at b*LS + n (lanes of a warp span a line)
+// Shared-memory addressing of line element n of line b, skewed by one slot
+// per SK elements (SK = first radix) so the first stage's stride-SK writes
+// fall in distinct banks:
+//   BatchFast: element (n, b) at p(n)*B + b  (lanes of a warp span lines)
+//   LineFast : element (n, b) at b*LS + p(n) (lanes of a warp span a line)
+// with p(n) = n + n / SK.  A line occupies N + N/SK slots.
 enum class SmemOrder { BatchFast, LineFast };
 
-template <SmemOrder O, int B, int LS> __device__ __forceinline__ int sidx(int n, int b) {
-  return O == SmemOrder::BatchFast ? n * B + b : b * LS + n;
+template <int N, int SK> __host__ __device__ constexpr int skewed_len() { return N + N / SK; }
+
+template <SmemOrder O, int B, int LS, int SK> __device__ __forceinline__ int sidx(int n, int b) {
+  const int p = n + n / SK;
+  return O == SmemOrder::BatchFast ? p * B + b : b * LS + p;
 }
 
 // One Stockham stage reading/writing shared memory (middle stages).
 // tw: e^{+2 pi i m / (N * twmul)} table, so w_{Ns R}^{q} = tw[q * (N / (Ns R)) * twmul].
-template <typename C, int N, int E, int R, int Ns, SmemOrder O, int B, int LS>
+template <typename C, int N, int E, int R, int Ns, SmemOrder O, int B, int LS, int SK>
 __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, int t,
                                                     const C* __restrict__ tw, int twmul) {
   constexpr int TPL = N / E;
@@ -98,7 +104,7 @@ __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, i
   for (int q = 0; q < NB; ++q) {
     const int j = t + TPL * q;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[q * R + r] = sm[sidx<O, B, LS>(j + r * (N / R), b)];
+    for (int r = 0; r < R; ++r) v[q * R + r] = sm[sidx<O, B, LS, SK>(j + r * (N / R), b)];
   }
   __syncthreads();
 #pragma unroll
@@ -113,14 +119,16 @@ __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, i
     dft_reg<R>(v + q * R);
     const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) sm[sidx<O, B, LS>(base + r * Ns, b)] = v[q * R + brev<R>(r)];
+    for (int r = 0; r < R; ++r) sm[sidx<O, B, LS, SK>(base + r * Ns, b)] = v[q * R + brev<R>(r)];
   }
   __syncthreads();
 }
 
 // Full line transform.  load(j, v) fills the first stage's R1 inputs
-// v[r] = x[j + r N/R1] (r < R1, R1 = StagePlan<N,E>::radix(0)); store(n, C)
-// takes each output of the last stage.  sm holds B lines laid out by O.  All
+// v[r] = x[j + r N/R1] (r < R1, R1 = StagePlan<N,E>::radix(0)); store(j, v)
+// takes the last stage's RL outputs v[r] = y[j + r N/RL] together, so a
+// caller can issue all its memory reads for them before its writes.  sm holds
+// B lines laid out by O with skew SK = R1 (line stride LS for LineFast).  All
 // threads of the block must call.
 template <typename C, int N, int E, SmemOrder O, int B, int LS, class Load, class Store>
 __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, const C* __restrict__ tw,
@@ -128,6 +136,7 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
   using P = StagePlan<N, E>;
   constexpr int TPL = N / E;
   constexpr int R1 = P::radix(0);
+  constexpr int SK = R1;
   constexpr int NB1 = E / R1;
   C v[E];
 #pragma unroll
@@ -137,8 +146,10 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
     for (int q = 0; q < NB1; ++q) {
       const int j = t + TPL * q;
       dft_reg<R1>(v + q * R1);
+      C o[R1];
 #pragma unroll
-      for (int r = 0; r < R1; ++r) store(j + r * (N / R1), v[q * R1 + brev<R1>(r)]);
+      for (int r = 0; r < R1; ++r) o[r] = v[q * R1 + brev<R1>(r)];
+      store(j, o);
     }
     __syncthreads();  // keep the barrier count uniform with the multi-stage path
   } else {
@@ -150,13 +161,13 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
     for (int q = 0; q < NB1; ++q) {
       const int j = t + TPL * q;
 #pragma unroll
-      for (int r = 0; r < R1; ++r) sm[sidx<O, B, LS>(j * R1 + r, b)] = v[q * R1 + brev<R1>(r)];
+      for (int r = 0; r < R1; ++r) sm[sidx<O, B, LS, SK>(j * R1 + r, b)] = v[q * R1 + brev<R1>(r)];
     }
     __syncthreads();
     if constexpr (P::S >= 3)
-      stockham_smem_stage<C, N, E, P::radix(1), R1, O, B, LS>(sm, b, t, tw, twmul);
+      stockham_smem_stage<C, N, E, P::radix(1), R1, O, B, LS, SK>(sm, b, t, tw, twmul);
     if constexpr (P::S >= 4)
-      stockham_smem_stage<C, N, E, P::radix(2), R1 * P::radix(1), O, B, LS>(sm, b, t, tw, twmul);
+      stockham_smem_stage<C, N, E, P::radix(2), R1 * P::radix(1), O, B, LS, SK>(sm, b, t, tw, twmul);
     static_assert(P::S <= 4, "line length too long for the register budget");
     // last stage
     constexpr int RL = P::radix(P::S - 1);
@@ -166,7 +177,7 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
     for (int q = 0; q < NBL; ++q) {
       const int j = t + TPL * q;
 #pragma unroll
-      for (int r = 0; r < RL; ++r) v[q * RL + r] = sm[sidx<O, B, LS>(j + r * (N / RL), b)];
+      for (int r = 0; r < RL; ++r) v[q * RL + r] = sm[sidx<O, B, LS, SK>(j + r * (N / RL), b)];
     }
 #pragma unroll
     for (int q = 0; q < NBL; ++q) {
@@ -179,10 +190,31 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
       }
       dft_reg<RL>(v + q * RL);
       // last stage: (j / NsL) == 0, output index j + r * NsL
+      C o[RL];
 #pragma unroll
-      for (int r = 0; r < RL; ++r) store(j + r * NsL, v[q * RL + brev<RL>(r)]);
+      for (int r = 0; r < RL; ++r) o[r] = v[q * RL + brev<RL>(r)];
+      store(j, o);
     }
   }
+}
+
+// Shared-memory slots of one line for a block using line_ifft<.., N, E, ..>.
+template <int N, int E> __host__ __device__ constexpr int line_slots() {
+  return skewed_len<N, StagePlan<N, E>::radix(0)>();
+}
+
+// Radix of the last stage (outputs per store group).
+template <int N, int E> __host__ __device__ constexpr int last_radix() {
+  return StagePlan<N, E>::radix(StagePlan<N, E>::S - 1);
+}
+
+// Asynchronous 16-byte global -> shared copy (cp.async, L2 only).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 // Adapts a per-element loader f(n) -> C to the group interface of line_ifft.

@@ -133,8 +133,13 @@ __global__ void __launch_bounds__(B*(N / E)) k_gen_z(const GenArgs a) {
     }
   };
   const int Nz = a.Nout[2];
-  auto store = [&](int z, C v) {
-    if (valid && z < Nz) work[((size_t)z * a.P[1] + ky) * a.Hpad + kx] = v;
+  constexpr int RL = last_radix<N, E>();
+  auto store = [&](int j, const C* o) {
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const int z = j + r * (N / RL);
+      if (valid && z < Nz) work[((size_t)z * a.P[1] + ky) * a.Hpad + kx] = o[r];
+    }
   };
   line_ifft<C, N, E, SmemOrder::BatchFast, B, 0>(sm, b, t, static_cast<const C*>(a.tw_z), 1, load,
                                                  store);
@@ -144,20 +149,37 @@ __global__ void __launch_bounds__(B*(N / E)) k_gen_z(const GenArgs a) {
 // Pass 2: inverse DFT along y, in place, keep y < Ny.
 // ---------------------------------------------------------------------------
 template <typename T, int N, int E, int B>
-__global__ void __launch_bounds__(B*(N / E), (B * (N / E) >= 512 ? 2 : 1)) k_mid_y(const GenArgs a) {
+__global__ void __launch_bounds__(B*(N / E)) k_mid_y(const GenArgs a) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int b = threadIdx.x % B, t = threadIdx.x / B;
-  const int kx = blockIdx.x * B + b;
+  const int kx0 = blockIdx.x * B;
+  const int kx = kx0 + b;
   const int z = blockIdx.y;
   const bool valid = kx < a.Hx;
-  C* col = static_cast<C*>(a.work) + (size_t)z * a.P[1] * a.Hpad + kx;
+  C* colblk = static_cast<C*>(a.work) + (size_t)z * a.P[1] * a.Hpad + kx0;
   const size_t pitch = (size_t)a.Hpad;
+  {  // stage the N x B column block: raw[n * B + b], 16-byte async copies
+    constexpr int CPR = B * (int)sizeof(C) / 16;  // chunks per row
+    for (int c = threadIdx.x; c < N * CPR; c += blockDim.x) {
+      const int n = c / CPR, q = c - n * CPR;
+      cp_async16(reinterpret_cast<char*>(sm + n * B) + q * 16,
+                 reinterpret_cast<const char*>(colblk + (size_t)n * pitch) + q * 16);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
   const int Ny = a.Nout[1];
-  auto load = each_load<C, N, E>([&](int ky) -> C { return valid ? col[(size_t)ky * pitch] : mk(T(0), T(0)); });
-  auto store = [&](int y, C v) {
-    if (valid && y < Ny) col[(size_t)y * pitch] = v;
+  auto load = each_load<C, N, E>([&](int ky) -> C { return sm[ky * B + b]; });
+  constexpr int RL = last_radix<N, E>();
+  C* col = colblk + b;
+  auto store = [&](int j, const C* o) {
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const int y = j + r * (N / RL);
+      if (valid && y < Ny) col[(size_t)y * pitch] = o[r];
+    }
   };
   line_ifft<C, N, E, SmemOrder::BatchFast, B, 0>(sm, b, t, static_cast<const C*>(a.tw_y), 1, load,
                                                  store);
@@ -166,11 +188,15 @@ __global__ void __launch_bounds__(B*(N / E), (B * (N / E) >= 512 ? 2 : 1)) k_mid
 // ---------------------------------------------------------------------------
 // Pass 3: Hermitian C2R along x (complex length N = P0/2), crop, epilogue.
 // ---------------------------------------------------------------------------
+template <int N, int E> __host__ __device__ constexpr int c2r_line_stride() {
+  return line_slots<N, E>() > N + 2 ? line_slots<N, E>() : N + 2;
+}
+
 template <typename T, int N, int E, int B>
 __global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
   using C = cplx_t<T>;
   constexpr int TPL = N / E;
-  constexpr int LS = N + 1;
+  constexpr int LS = c2r_line_stride<N, E>();
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int Nx = a.Nout[0], Ny = a.Nout[1], Nz = a.Nout[2];
@@ -180,11 +206,15 @@ __global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
   const int64_t l = (int64_t)blockIdx.x * B + b;
   const bool valid = l < nlines;
   const int y = valid ? (int)(l % Ny) : 0, z = valid ? (int)(l / Ny) : 0;
-  {  // stage the raw half-spectrum line (N + 1 values), coalesced per line
+  {  // stage the raw half-spectrum line (N + 1 values, padded to 16 bytes)
+    constexpr int CH = (N + 2) * (int)sizeof(C) / 16;
     const C* src = work + ((size_t)z * a.P[1] + (size_t)y) * a.Hpad;
-    for (int k = t; k < LS; k += TPL) sm[b * LS + k] = valid ? src[k] : mk(T(0), T(0));
+    if (valid)
+      for (int c = t; c < CH; c += TPL)
+        cp_async16(reinterpret_cast<char*>(sm + b * LS) + c * 16, reinterpret_cast<const char*>(src) + c * 16);
+    cp_async_wait_all();
+    __syncthreads();
   }
-  __syncthreads();
   const C* twx = static_cast<const C*>(a.tw_x);
   const C* line = sm + b * LS;
   auto load = each_load<C, N, E>([&](int k) -> C {
@@ -196,11 +226,20 @@ __global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
     return mk(e.x - o.y, e.y + o.x);
   });
   const LineEpilogue<T> ep(a.epi, y, z, Nx, Ny);
-  auto store = [&](int n, C v) {
+  constexpr int RL = last_radix<N, E>();
+  auto store = [&](int j, const C* o) {
     if (!valid) return;
-    const int x0 = 2 * n;
-    if (x0 < Nx) ep.put(x0, v.x);
-    if (x0 + 1 < Nx) ep.put(x0 + 1, v.y);
+    T v[2 * RL];
+    int xs[2 * RL];
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const int n = j + r * (N / RL);
+      v[2 * r] = o[r].x;
+      v[2 * r + 1] = o[r].y;
+      xs[2 * r] = 2 * n;
+      xs[2 * r + 1] = 2 * n + 1;
+    }
+    ep.template put_group<2 * RL>(xs, v, Nx);
   };
   line_ifft<C, N, E, SmemOrder::LineFast, B, LS>(sm, b, t, twx, 2, load, store);
 }
@@ -234,7 +273,7 @@ static cudaError_t run_gen_z(const GenArgs& a, cudaStream_t s) {
   using Cf = ColCfg<T, N>;
   dim3 grid((a.Hx + Cf::B - 1) / Cf::B, a.P[1], 1);
   dim3 block(Cf::B * (N / Cf::E));
-  size_t smem = (size_t)Cf::B * N * sizeof(cplx_t<T>);
+  size_t smem = (size_t)Cf::B * line_slots<N, Cf::E>() * sizeof(cplx_t<T>);
   switch (a.spec) {
     case SPEC_PHILOX: return launch_k(k_gen_z<T, N, Cf::E, Cf::B, SPEC_PHILOX>, grid, block, smem, s, a);
     case SPEC_INJECT: return launch_k(k_gen_z<T, N, Cf::E, Cf::B, SPEC_INJECT>, grid, block, smem, s, a);
@@ -248,7 +287,7 @@ static cudaError_t run_mid_y(const GenArgs& a, cudaStream_t s) {
   using Cf = ColCfg<T, N>;
   dim3 grid((a.Hx + Cf::B - 1) / Cf::B, a.Nout[2], 1);
   dim3 block(Cf::B * (N / Cf::E));
-  size_t smem = (size_t)Cf::B * N * sizeof(cplx_t<T>);
+  size_t smem = (size_t)Cf::B * line_slots<N, Cf::E>() * sizeof(cplx_t<T>);
   return launch_k(k_mid_y<T, N, Cf::E, Cf::B>, grid, block, smem, s, a);
 }
 
@@ -258,7 +297,7 @@ static cudaError_t run_c2r_x(const GenArgs& a, cudaStream_t s) {
   const int64_t nlines = (int64_t)a.Nout[1] * a.Nout[2];
   dim3 grid((unsigned)((nlines + Cf::B - 1) / Cf::B), 1, 1);
   dim3 block(Cf::B * (N / Cf::E));
-  size_t smem = (size_t)Cf::B * (N + 1) * sizeof(cplx_t<T>);
+  size_t smem = (size_t)Cf::B * c2r_line_stride<N, Cf::E>() * sizeof(cplx_t<T>);
   return launch_k(k_c2r_x<T, N, Cf::E, Cf::B>, grid, block, smem, s, a);
 }
 
