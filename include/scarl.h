@@ -217,6 +217,25 @@ int scarl_gen_padded(scarl_ctx* ctx, void* out, int dtype, const int Np[3], cons
                      const double xStep[3], const double corrL[3], int corrMod, double nu,
                      int normalise, uint64_t seed, uint32_t stream, const void* xi);
 
+/* No counterpart in the reference.  scarl_gen_padded for callers that
+ * cannot allocate GPU memory (a host code whose device memory belongs to its
+ * own pool allocator, or a running time-critical loop that must not call
+ * cudaMalloc): no context, no allocation.  Its scratch is a fixed 64 MiB
+ * device array reserved on every GPU that loads this library until the
+ * process exits; requests whose intermediate and tables do not fit (the
+ * intermediate is round_up(P0/2+1, 16) * P1 * Np[2] complex values: about
+ * 8.3 M in FP32, 4.1 M in FP64, e.g. a 256^3 padded grid with Np[2] <= 225 in
+ * FP32) return SCARL_EINVAL with the needed size in msg.
+ * out must be device memory of the current GPU; work is enqueued on
+ * cuda_stream (NULL = the legacy default stream).  The first call on a
+ * device looks up the array's address: make it before any stream capture.
+ * Calls share the array: calls whose GPU work may overlap race and must be
+ * serialised.  Output equals scarl_gen_padded with xi = NULL. */
+int scarl_gen_padded_noalloc(void* out, int dtype, const int Np[3], const int pad[3],
+                             const double xStep[3], const double corrL[3], int corrMod, double nu,
+                             int normalise, uint64_t seed, uint32_t stream, void* cuda_stream,
+                             char* msg, size_t msg_len);
+
 /* One deck sample end to end on the GPU (SRC_F/main_ScaRL.f90:95-214 +
  * create_fields :345-583 without file output): layout, every tile generated,
  * PoU-weighted, overlap-summed and assembled into the global field

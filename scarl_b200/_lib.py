@@ -89,6 +89,9 @@ SIGNATURES = {
                                                 C.c_int, C.c_int]),
     "scarl_gen_padded": (C.c_int, [_vp, _vp, C.c_int, _ip, _ip, _dp, _dp, C.c_int, C.c_double,
                                    C.c_int, C.c_uint64, C.c_uint32, _vp]),
+    "scarl_gen_padded_noalloc": (C.c_int, [_vp, C.c_int, _ip, _ip, _dp, _dp, C.c_int, C.c_double,
+                                           C.c_int, C.c_uint64, C.c_uint32, _vp, C.c_char_p,
+                                           C.c_size_t]),
     "scarl_generate_sample": (C.c_int, [_vp, C.POINTER(Sample), C.POINTER(GenOpts), _vp]),
     "scarl_apply_unity_partition": (C.c_int, [_vp, _vp, _ip, _ip, C.c_int, _ip, _ip]),
     "scarl_add_overlap": (C.c_int, [_vp, _vp, _ip, _ip, _ip]),
