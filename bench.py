@@ -243,7 +243,7 @@ def main():
 
     def step(out=field, dtype=S.F32, policy=S.PAD_AUTO):
         S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=dtype, nb_procs=8,
-                          topo=TOPO, pad_policy=policy, pad_tol=PAD_TOL, out=out)
+                          topo=TOPO, pad_policy=policy, pad_tol=PAD_TOL, autotune=True, out=out)
 
     def barrier():
         if dist is not None:
@@ -346,13 +346,13 @@ def main():
     hnp = host.numpy()
     ctx.set_stream(0)  # library-owned stream; host calls synchronise inside
     S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
-                      pad_tol=PAD_TOL, out=hnp)
+                      pad_tol=PAD_TOL, autotune=True, out=hnp)
     c0 = ctx.counters()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
-                          pad_tol=PAD_TOL, out=hnp)
+                          pad_tol=PAD_TOL, autotune=True, out=hnp)
     e2e_s = (time.perf_counter() - t0) / args.steps
     c1 = ctx.counters()
     if dist is not None:

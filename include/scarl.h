@@ -112,6 +112,7 @@ typedef struct {
   int no_spectral_normalisation; /* 1 = raw Riemann-sum amplitudes */
   int normalize_field;    /* 1 = normalize_field (disabled in the reference) */
   uint32_t stream;        /* realisation stream (ensembles), 0 by default */
+  int autotune;           /* 1 = autotune each new grid shape on first use */
   const double* phiK;     /* DCT generator: injected phases, nb x (Np/2)^3 */
 } scarl_gen_opts;
 
@@ -123,6 +124,17 @@ int scarl_ctx_destroy(scarl_ctx* ctx);
 const char* scarl_last_error(const scarl_ctx* ctx);
 int scarl_ctx_set_stream(scarl_ctx* ctx, void* cuda_stream);
 int scarl_sync(scarl_ctx* ctx);
+/* Autotuner (no counterpart in the reference): times every launch variant
+ * (values per thread, lines per block) of the three generator passes on
+ * padded grid P and tile Np, keeps the fastest per (dtype, pass, line
+ * length) in the context, and merges the choices into cache_path (text
+ * lines "dtype pass N variant"; NULL = no file).  Contexts also load the
+ * file named by the environment variable SCARL_TUNE_CACHE when created. */
+int scarl_autotune(scarl_ctx* ctx, int dtype, int corrMod, double nu, const int P[3],
+                   const int Np[3], const double xStep[3], const double corrL[3],
+                   const char* cache_path);
+int scarl_tune_get(scarl_ctx* ctx, int dtype, int pass, int N, int* variant);
+int scarl_tune_set(scarl_ctx* ctx, int dtype, int pass, int N, int variant);
 /* Kernels launched and bytes copied host->device / device->host by this
  * context since its creation. */
 int scarl_counters(scarl_ctx* ctx, long long* launches, unsigned long long* h2d_bytes,

@@ -45,7 +45,7 @@ class GenOpts(C.Structure):
                 ("topo_shape", C.c_int * 3), ("pad", C.c_int * 3),
                 ("pad_policy", C.c_int), ("pad_tol", C.c_double),
                 ("no_spectral_normalisation", C.c_int), ("normalize_field", C.c_int),
-                ("stream", C.c_uint32), ("phiK", C.POINTER(C.c_double))]
+                ("stream", C.c_uint32), ("autotune", C.c_int), ("phiK", C.POINTER(C.c_double))]
 
 
 _vp = C.c_void_p
@@ -61,6 +61,10 @@ SIGNATURES = {
     "scarl_sync": (C.c_int, [_vp]),
     "scarl_counters": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong),
                                  C.POINTER(C.c_ulonglong)]),
+    "scarl_autotune": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, _ip, _ip, _dp, _dp,
+                                 C.c_char_p]),
+    "scarl_tune_get": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _ip]),
+    "scarl_tune_set": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "scarl_profile": (C.c_int, [_vp, C.c_int]),
     "scarl_profile_read": (C.c_int, [_vp, C.c_int, C.c_char_p, C.c_size_t, _dp,
                                      C.POINTER(C.c_longlong)]),

@@ -78,6 +78,18 @@ class Context:
     def profile_reset(self):
         _check(lib().scarl_profile(self.handle, 2), self)
 
+    def autotune(self, dtype, corrMod, P, Np, xStep, corrL, nu=0.5, cache_path=None):
+        _check(lib().scarl_autotune(self.handle, dtype, corrMod, nu, _i3(P), _i3(Np), _d3(xStep),
+                                    _d3(corrL), cache_path.encode() if cache_path else None), self)
+
+    def tune_get(self, dtype, pass_, N):
+        v = C.c_int()
+        _check(lib().scarl_tune_get(self.handle, dtype, pass_, N, C.byref(v)), self)
+        return v.value
+
+    def tune_set(self, dtype, pass_, N, variant):
+        _check(lib().scarl_tune_set(self.handle, dtype, pass_, N, variant), self)
+
     def counters(self):
         n = C.c_longlong(); h = C.c_ulonglong(); d = C.c_ulonglong()
         _check(lib().scarl_counters(self.handle, C.byref(n), C.byref(h), C.byref(d)), self)
@@ -281,7 +293,7 @@ def axis_correlation(corrMod, l, r, nu=0.5):
 
 def generate_sample(ctx, sample, generator=GEN_PADDED, dtype=F32, nb_procs=1, topo=None,
                     pad=None, pad_policy=PAD_FULL, pad_tol=1e-3, normalise_spectrum=True,
-                    normalize_field=False, stream=0, phiK=None, out=None):
+                    normalize_field=False, stream=0, phiK=None, autotune=False, out=None):
     """One deck sample end to end (layout, tiles, PoU blend, marginal)."""
     lay = sample_layout(sample, 1, nb_procs, topo)
     out = _alloc_out(out, tuple(int(v) for v in lay["L"]), dtype)
@@ -295,6 +307,7 @@ def generate_sample(ctx, sample, generator=GEN_PADDED, dtype=F32, nb_procs=1, to
     o.no_spectral_normalisation = 0 if normalise_spectrum else 1
     o.normalize_field = int(bool(normalize_field))
     o.stream = int(stream)
+    o.autotune = int(bool(autotune))
     keep = None
     if phiK is not None:
         keep = np.ascontiguousarray(phiK, dtype=np.float64)

@@ -15,7 +15,8 @@ LIB = os.path.join(HERE, "libscarl_b200.so")
 OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-CUDA_SOURCES = ["gen_padded.cu", "dct_literal.cu", "post.cu", "stats.cu", "noalloc.cu"]
+CUDA_SOURCES = ["gen_padded.cu", "gen_f32.cu", "gen_f64.cu", "dct_literal.cu", "post.cu", "stats.cu",
+                "noalloc.cu"]
 HOST_SOURCES = ["api.cpp", "host_maps.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",

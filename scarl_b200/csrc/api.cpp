@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -65,6 +66,8 @@ struct scarl_ctx {
   std::vector<cudaEvent_t> pool;
   std::vector<std::string> porder;
   std::map<std::string, std::pair<double, long long>> pstats;
+  std::map<long long, int> tune;          // (dtype, pass, N) -> launch variant
+  std::map<std::string, bool> tuned_shapes;
 };
 
 namespace {
@@ -461,6 +464,32 @@ int check_grid(scarl_ctx* ctx, const int P[3], const int Np[3]) {
   return SCARL_OK;
 }
 
+long long tune_key(int dt, int pass, int N) { return ((long long)dt * 8 + pass) * 100000 + N; }
+
+// Tuning cache file: lines "dtype pass N variant".
+void tune_load(scarl_ctx* ctx, const char* path) {
+  if (!path || !*path) return;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return;
+  int dt, pass, N, v;
+  while (std::fscanf(f, "%d %d %d %d", &dt, &pass, &N, &v) == 4)
+    if ((dt == 4 || dt == 8) && pass >= 1 && pass <= 3 && v >= 0 && v < gen_variant_count(dt, pass))
+      ctx->tune[tune_key(dt, pass, N)] = v;
+  std::fclose(f);
+}
+
+void tune_save(scarl_ctx* ctx, const char* path) {
+  if (!path || !*path) return;
+  FILE* f = std::fopen(path, "w");
+  if (!f) return;
+  for (const auto& kv : ctx->tune) {
+    const long long k = kv.first;
+    const int N = (int)(k % 100000), dp = (int)(k / 100000);
+    std::fprintf(f, "%d %d %d %d\n", dp / 8, dp % 8, N, kv.second);
+  }
+  std::fclose(f);
+}
+
 // Common GenArgs of the padded passes for one tile.
 int gen_args(scarl_ctx* ctx, int dt, const int P[3], const int Np[3], GenArgs* a) {
   std::memset(a, 0, sizeof *a);
@@ -476,6 +505,11 @@ int gen_args(scarl_ctx* ctx, int dt, const int P[3], const int Np[3], GenArgs* a
   RC(twiddles(ctx, P[2], dt, &a->tw_z));
   RC(twiddles(ctx, P[1], dt, &a->tw_y));
   RC(twiddles(ctx, P[0], dt, &a->tw_x));
+  const int Nl[3] = {P[2], P[1], P[0] / 2};
+  for (int p = 0; p < 3; ++p) {
+    auto it = ctx->tune.find(tune_key(dt, p + 1, Nl[p]));
+    a->var[p] = it == ctx->tune.end() ? 0 : it->second;
+  }
   return SCARL_OK;
 }
 
@@ -489,6 +523,59 @@ void set_plan(GenArgs* a, const PaddedPlan* pl) {
   a->qx = pl->t[3];
   a->qy = pl->t[4];
   a->qz = pl->t[5];
+}
+
+// Times every valid launch variant of the three passes on grid P / tile Np
+// (CUDA events, best of 3 after one warm-up) and keeps the fastest per
+// (dtype, pass, line length) in the context.
+int autotune_shape(scarl_ctx* ctx, int dt, const int P[3], const int Np[3], int corrMod, double nu,
+                   const double xStep[3], const double corrL[3]) {
+  PaddedPlan* pl;
+  RC(padded_plan(ctx, dt, P, xStep, corrL, corrMod, nu, 1, &pl));
+  GenArgs a;
+  RC(gen_args(ctx, dt, P, Np, &a));
+  set_plan(&a, pl);
+  const size_t n = (size_t)Np[0] * Np[1] * Np[2];
+  RC(ensure(ctx, ctx->tile, n * dt));
+  a.epi.mode = 0;
+  a.epi.out = ctx->tile.p;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int Nl[3] = {P[2], P[1], P[0] / 2};
+  for (int pass = 1; pass <= 3; ++pass) {
+    int best = 0;
+    float best_ms = 1e30f;
+    for (int v = 0; v < gen_variant_count(dt, pass); ++v) {
+      GenArgs b = a;
+      b.var[pass - 1] = v;
+      cudaError_t e = launch_gen_pass(dt, pass, b, ctx->stream);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      float tmin = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        cudaEventRecord(e0, ctx->stream);
+        launch_gen_pass(dt, pass, b, ctx->stream);
+        cudaEventRecord(e1, ctx->stream);
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        tmin = std::min(tmin, ms);
+      }
+      if (tmin < best_ms) {
+        best_ms = tmin;
+        best = v;
+      }
+    }
+    ctx->tune[tune_key(dt, pass, Nl[pass - 1])] = best;
+    a.var[pass - 1] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaGetLastError());
+  return SCARL_OK;
 }
 
 // Marginal parameters exactly as SRC_F/main_ScaRL.f90:1371-1389.
@@ -693,6 +780,7 @@ int scarl_ctx_create(int device, size_t budget_bytes, scarl_ctx** out) {
     return SCARL_EDEVICE;
   }
   c->own_stream = true;
+  tune_load(c, std::getenv("SCARL_TUNE_CACHE"));
   *out = c;
   return SCARL_OK;
 }
@@ -745,6 +833,33 @@ int scarl_counters(scarl_ctx* ctx, long long* launches, unsigned long long* h2d_
   if (launches) *launches = ctx->launches;
   if (h2d_bytes) *h2d_bytes = ctx->h2d;
   if (d2h_bytes) *d2h_bytes = ctx->d2h;
+  return SCARL_OK;
+}
+
+int scarl_autotune(scarl_ctx* ctx, int dtype, int corrMod, double nu, const int P[3],
+                   const int Np[3], const double xStep[3], const double corrL[3],
+                   const char* cache_path) {
+  RC(begin(ctx));
+  if (!P || !Np || !xStep || !corrL) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  RC(check_grid(ctx, P, Np));
+  tune_load(ctx, cache_path);
+  RC(autotune_shape(ctx, dtype, P, Np, corrMod, nu, xStep, corrL));
+  tune_save(ctx, cache_path);
+  return SCARL_OK;
+}
+
+int scarl_tune_get(scarl_ctx* ctx, int dtype, int pass, int N, int* variant) {
+  if (!ctx || !variant || pass < 1 || pass > 3) return SCARL_EINVAL;
+  auto it = ctx->tune.find(tune_key(dtype, pass, N));
+  *variant = it == ctx->tune.end() ? 0 : it->second;
+  return SCARL_OK;
+}
+
+int scarl_tune_set(scarl_ctx* ctx, int dtype, int pass, int N, int variant) {
+  if (!ctx || pass < 1 || pass > 3 || (dtype != SCARL_F32 && dtype != SCARL_F64)) return SCARL_EINVAL;
+  if (variant < 0 || variant >= gen_variant_count(dtype, pass)) return SCARL_EINVAL;
+  ctx->tune[tune_key(dtype, pass, N)] = variant;
   return SCARL_OK;
 }
 
@@ -1017,6 +1132,15 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
     for (int d = 0; d < 3; ++d)
       if (!(s->corrL[d] > 0.0)) return fail(ctx, SCARL_EINVAL, "corrL must be > 0");
     RC(padded_plan(ctx, dt, P, lay.xStep, s->corrL, s->corrMod, s->nu, !o.no_spectral_normalisation, &pl));
+    if (o.autotune) {
+      char key[128];
+      std::snprintf(key, sizeof key, "%d|%d,%d,%d|%d,%d,%d", dt, P[0], P[1], P[2], lay.Np[0], lay.Np[1], lay.Np[2]);
+      if (!ctx->tuned_shapes[key]) {
+        RC(autotune_shape(ctx, dt, P, lay.Np, s->corrMod, s->nu, lay.xStep, s->corrL));
+        ctx->tuned_shapes[key] = true;
+        tune_save(ctx, std::getenv("SCARL_TUNE_CACHE"));
+      }
+    }
   }
   if (gen == SCARL_GEN_DCT) {
     for (int d = 0; d < 3; ++d)

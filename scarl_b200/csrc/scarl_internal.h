@@ -71,11 +71,14 @@ struct GenArgs {
   double shino_scale;    // sqrt(8) and 2 sqrt(prod delta_k) applied in order
   double shino_f;
   Epilogue epi;
+  int var[3];            // launch variant of each pass (autotuned, 0 = default)
 };
 
 // Launchers (return cudaSuccess or the launch error).  dt: 4 = FP32, 8 = FP64.
 // pass: 1 = synthesis + z, 2 = y, 3 = C2R x + epilogue.
 cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a, cudaStream_t s);
+// Number of launch variants of a pass (valid ones depend on the line length).
+int gen_variant_count(int dt, int pass);
 // FP64 sum over the full periodic grid of S(k) dk^3: separable tables r*
 // (A_raw = rx ry rz) or Matern q tables with A_raw^2 = craw2 (1+q)^(2 expo).
 cudaError_t launch_spectrum_sum(const GenArgs& a, const double* rx, const double* ry,
