@@ -204,6 +204,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="scarl", choices=["scarl", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-tile", action="store_true",
+                    help="generate one field once (no timing) for profiler captures; launch "
+                         "variants come from SCARL_TUNE_CACHE when set")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -227,6 +230,17 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+    if args.profile_tile:
+        ctx = S.Context(local)
+        sample, lay = layout_of(S)
+        L = [int(v) for v in lay["L"]]
+        field = torch.empty(L[0] * L[1] * L[2], dtype=torch.float32, device="cuda")
+        S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=S.F32, nb_procs=8, topo=TOPO,
+                          pad_policy=S.PAD_AUTO, pad_tol=PAD_TOL, out=field)
+        ctx.sync()
+        print(json.dumps({"profile_tile": "ok", "launches": ctx.counters()["launches"]}))
+        ctx.close()
+        return
     ctx = S.Context(local)
     # a real stream shared by the library and the timing events (the legacy
     # default stream's handle is 0, which the library reads as "own stream")
@@ -364,6 +378,11 @@ def main():
            "d2h_bytes_per_step": (c1["d2h_bytes"] - c0["d2h_bytes"]) // args.steps,
            "ms_per_step": round(e2e_s * 1e3, 3)}
 
+    tuned = {}
+    for name, P in (("auto", P_auto), ("full", P_full)):
+        Nl = (P[2], P[1], P[0] // 2)
+        tuned[name] = [ctx.tune_get(S.F32, p + 1, Nl[p]) for p in range(3)]
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = cpu_sample(lay, P_auto, 1, 0)
@@ -376,7 +395,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (Philox normals, seeded per rank)",
                 "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "roofline": roof,
-                "kernels": kern, "plain_path": plain,
+                "kernels": kern, "launch_variants": tuned, "plain_path": plain,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(line), flush=True)
     ctx.close()
