@@ -188,6 +188,83 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def bench_ensemble(S, ctx, stream, steps, warmup):
+    """The 256-realisation ensemble of uneven grids: axes from {64, ..., 256},
+    isotropic l in [4, 32], exponential, seeds 0-255, FP32, AUTO padding.
+    Batched launches replayed from a CUDA graph against the same realisations
+    generated one scarl_gen_padded call at a time (same padded grids)."""
+    import numpy as np
+    import torch
+    ctx.set_stream(stream.cuda_stream)
+    Np, cl = S.ensemble_draw(0, 0, 256)
+    off = S.ensemble_offsets(Np)
+    total = int(off[-1])
+    out = torch.empty(total, dtype=torch.float32, device="cuda")
+    seeds = np.arange(256, dtype=np.uint64)
+    P = [[int(v) for v in S.pad_size(S.PAD_AUTO, 3, c, (1, 1, 1), n, 0.5, PAD_TOL)]
+         for n, c in zip(Np, cl)]
+
+    def batched():
+        S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_tol=PAD_TOL, seeds=seeds, autotune=True, out=out)
+
+    def single():
+        for i in range(256):
+            S.gen_padded(ctx, Np[i], (1, 1, 1), cl[i], 3, 0.5, pad=P[i], seed=i,
+                         out=out[int(off[i]):int(off[i + 1])])
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    for _ in range(warmup):
+        batched()
+    l0 = ctx.counters()["launches"]
+    ms_b = timed(batched, steps)
+    launches = (ctx.counters()["launches"] - l0) // steps
+    ref = out.clone()
+    single()
+    torch.cuda.synchronize()
+    ms_s = timed(single, max(2, steps // 5))
+    # e2e: pinned host output through the same call
+    host = torch.empty(total, dtype=torch.float32, pin_memory=True)
+    hnp = host.numpy()
+    ctx.set_stream(0)
+    S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_tol=PAD_TOL, seeds=seeds, autotune=True, out=hnp)
+    c0 = ctx.counters()
+    t0 = time.perf_counter()
+    k = max(2, steps // 5)
+    for _ in range(k):
+        S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_tol=PAD_TOL, seeds=seeds, autotune=True, out=hnp)
+    e2e_s = (time.perf_counter() - t0) / k
+    c1 = ctx.counters()
+    ctx.set_stream(stream.cuda_stream)
+    same = bool(torch.equal(torch.from_numpy(hnp).cuda(), ref))
+    pvol = sum(p[0] * p[1] * p[2] for p in P)
+    return {"workload": "256 realisations, axes uniform in {64,96,128,160,192,256}, isotropic "
+                        "l uniform in [4,32], exponential, seeds 0-255, FP32, AUTO padding "
+                        f"(image error <= {PAD_TOL:g})",
+            "points": total, "padded_points": pvol,
+            "value": round(total / (ms_b * 1e-3) / 1e6, 2), "unit": "Mpoints/s",
+            "ms_per_ensemble": round(ms_b, 3), "gpu_launches_per_ensemble": int(launches),
+            "per_realisation_path": {"value": round(total / (ms_s * 1e-3) / 1e6, 2),
+                                     "ms_per_ensemble": round(ms_s, 3),
+                                     "launches_per_ensemble": 3 * 256},
+            "batched_speedup": round(ms_s / ms_b, 3),
+            "e2e": {"value": round(total / e2e_s / 1e6, 2), "unit": "Mpoints/s",
+                    "h2d_bytes_per_step": (c1["h2d_bytes"] - c0["h2d_bytes"]) // k,
+                    "d2h_bytes_per_step": (c1["d2h_bytes"] - c0["d2h_bytes"]) // k,
+                    "ms_per_step": round(e2e_s * 1e3, 3)},
+            "host_output_equals_device_output": same}
+
+
 def config_of(lay, P):
     return {"workload": "512^3 deck -> 513^3 field, exponential, l=(40,20,10), lognormal mean 1 "
                         "CV 0.3, 2x2x2 tiles, overlap 2l, padded periodic C2R FP32",
@@ -204,6 +281,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="scarl", choices=["scarl", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--profile-tile", action="store_true",
                     help="generate one field once (no timing) for profiler captures; launch "
                          "variants come from SCARL_TUNE_CACHE when set")
@@ -383,6 +461,10 @@ def main():
         Nl = (P[2], P[1], P[0] // 2)
         tuned[name] = [ctx.tune_get(S.F32, p + 1, Nl[p]) for p in range(3)]
 
+    ens = None
+    if not args.no_ensemble:
+        ens = bench_ensemble(S, ctx, stream, max(3, min(args.steps, 20)), args.warmup)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = cpu_sample(lay, P_auto, 1, 0)
@@ -396,7 +478,8 @@ def main():
                 "data": "synthetic (Philox normals, seeded per rank)",
                 "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "roofline": roof,
                 "kernels": kern, "launch_variants": tuned, "plain_path": plain,
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+                "ensemble": ens}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

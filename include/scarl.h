@@ -257,6 +257,38 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
                           void* global);
 
 /* ------------------------------------------------------------------ */
+/* Ensembles (no counterpart in the reference, which generates one     */
+/* sample per run, SRC_F/main_ScaRL.f90:82-214)                        */
+/* ------------------------------------------------------------------ */
+#define SCARL_ENS_AUTOTUNE 1  /* time the launch variants of every batched launch once */
+#define SCARL_ENS_NO_GRAPH 2  /* launch eagerly instead of replaying the CUDA graph */
+
+/* [host] Shapes and isotropic correlation lengths of realisations
+ * first..first+n-1: realisation r reads the four words w of Philox4x32-10 at
+ * counter {r, r >> 32, 0, 2}, key {seed, seed >> 32}; axis d gets
+ * choices[floor(w_d * nchoices / 2^32)] points, the correlation length is
+ * lmin + (lmax - lmin) (w_3 + 1/2) 2^-32.  Np and corrL receive 3 n values. */
+int scarl_ensemble_draw(uint64_t seed, long long first, int n, const int* choices, int nchoices,
+                        double lmin, double lmax, int* Np, double* corrL);
+
+/* n independent padded-method realisations of uneven grids, one tile each:
+ * realisation i has Np[3i..3i+2] points of spacing xStep[3i..], correlation
+ * lengths corrL[3i..], Philox key seeds[i] (NULL: i) and stream streams[i]
+ * (NULL: 0).  Its field, column-major, starts at element
+ * sum_{j<i} Np_j0 Np_j1 Np_j2 of out (device or host pointer).  Padded grids
+ * follow pad_policy / pad_tol per realisation; margiFirst 0 leaves the
+ * standard field, 1 / 2 apply the Gaussian / lognormal marginal of avg,
+ * std_dev.  Realisations are grouped by line length in each of the three
+ * passes and every group runs as one batched launch; the first call for a
+ * list of shapes builds the plan (FP64 spectral sums, tables, workspace) and
+ * captures the launches in a CUDA graph that later calls replay. */
+int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* Np,
+                       const double* xStep, const double* corrL, int corrMod, double nu,
+                       int pad_policy, double pad_tol, const uint64_t* seeds,
+                       const uint32_t* streams, int margiFirst, double avg, double std_dev,
+                       int flags);
+
+/* ------------------------------------------------------------------ */
 /* Post steps (device kernels; FP64 fields in place)                   */
 /* ------------------------------------------------------------------ */
 /* apply_UnityPartition_mtx (SRC_F/main_ScaRL.f90:1216-1301), bit-exact. */
@@ -293,6 +325,18 @@ int scarl_moments(scarl_ctx* ctx, const void* field, int dtype, long long xNTota
  * r_tukey, taper formula over every ratio > r); 0 the standard Tukey window. */
 int scarl_rebuild_sk(scarl_ctx* ctx, const void* field, int dtype, const int L[3], double avg,
                      double stdDev, int tukey_literal, double* SkTot);
+/* Mean, variance and the covariance along each axis up to lag maxlag of
+ * one field L[0] x L[1] x L[2] (column-major, device or host pointer), FP64
+ * accumulation on the GPU:
+ *   cov[d (maxlag + 1) + h] = sum over point pairs (x, x + h e_d) of
+ *       (f(x) - mean)(f(x + h e_d) - mean) / number of such pairs,
+ * mean over all points, var = cov[0].  One moment pass plus one pass per
+ * axis over the field.  No direct counterpart: rebuild_Sk_FFT
+ * (statistics_RF.f90:258-462) windows and wraps each line; this is the
+ * plain linear estimator a covariance model is checked against.  Needs
+ * maxlag < L[d] and L[d] + maxlag <= 4096. */
+int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
+                   double* mean, double* var, double* cov);
 /* [host] rebuild_corrL (statistics_RF.f90:468-486). */
 int scarl_rebuild_corrL(const double* SkTot, const int L[3], const double xStep[3],
                         double corrL_out[3]);

@@ -39,6 +39,8 @@ def _declare(L):
     L.so_philox4x32_10.argtypes = [_u32, _u32, _u32]
     L.so_normals.argtypes = [C.c_uint64, C.c_uint32, _i, _d]
     L.so_uniforms.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _d]
+    L.so_ensemble_draw.argtypes = [C.c_uint64, C.c_int64, C.c_int, _i, C.c_int, C.c_double,
+                                   C.c_double, _i, _d]
     L.so_verify_inputs.restype = C.c_int
     L.so_verify_inputs.argtypes = [_d, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int, _i, C.c_int]
     L.so_find_factors.argtypes = [C.c_int, _i]
@@ -84,6 +86,7 @@ def _declare(L):
                                      C.c_int, _d, _d]
     L.so_moments.argtypes = [_d, C.c_int64, C.c_int, _d, _d, _d, _d]
     L.so_tukey.argtypes = [C.c_int, C.c_int, _d]
+    L.so_axis_cov.argtypes = [_d, _i, C.c_int, _d, _d]
     L.so_rebuild_sk_fft.argtypes = [_d, _i, C.c_int, C.c_double, C.c_double, C.c_int, _d]
     L.so_rebuild_corrL.argtypes = [_d, _i, _d, _d]
 
@@ -146,6 +149,15 @@ def uniforms(seed, stream, first, n):
     out = np.empty(max(n, 1))
     lib().so_uniforms(seed, stream, first, n, _dp(out))
     return out[:n]
+
+
+def ensemble_draw(seed, first, n, choices, lmin, lmax):
+    ch = np.ascontiguousarray(choices, dtype=np.int32)
+    Np = np.zeros((max(n, 1), 3), dtype=np.int32)
+    cl = np.zeros((max(n, 1), 3))
+    lib().so_ensemble_draw(seed, first, n, ch.ctypes.data_as(_i), len(ch), lmin, lmax,
+                           Np.ctypes.data_as(_i), _dp(cl))
+    return Np[:n], cl[:n]
 
 
 # ---------------- index maps ----------------
@@ -419,3 +431,13 @@ def rebuild_corrL(SkTot, nkeep, xStep):
     out = np.zeros(3)
     lib().so_rebuild_corrL(_dp(s), pn, px, _dp(out))
     return out
+
+
+def axis_cov(f, maxlag):
+    """Mean and (3, maxlag + 1) linear axis covariance of a Fortran-order field."""
+    f = np.asfortranarray(f, dtype=np.float64)
+    L, pL = _ia(f.shape)
+    cov = np.zeros(3 * (maxlag + 1))
+    m = C.c_double()
+    lib().so_axis_cov(f.ctypes.data_as(_d), pL, int(maxlag), C.byref(m), _dp(cov))
+    return m.value, cov.reshape(3, maxlag + 1)

@@ -172,6 +172,28 @@ void so_uniforms(uint64_t seed, uint32_t stream, uint64_t first, uint64_t n, dou
   }
 }
 
+/* Shapes and correlation lengths of an ensemble of realisations (no
+ * counterpart in the reference, which generates one sample per run,
+ * SRC_F/main_ScaRL.f90:82-214).  Realisation r = first + i draws the four
+ * words of Philox4x32-10 at counter {r, r >> 32, 0, 2}, key {seed, seed >> 32}:
+ * axis d takes choices[floor(w_d * nchoices / 2^32)] points and the
+ * isotropic correlation length is lmin + (lmax - lmin) (w_3 + 1/2) 2^-32. */
+void so_ensemble_draw(uint64_t seed, int64_t first, int n, const int* choices, int nchoices,
+                      double lmin, double lmax, int* Np, double* corrL) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int i = 0; i < n; ++i) {
+    const uint64_t r = (uint64_t)(first + i);
+    uint32_t ctr[4] = {(uint32_t)r, (uint32_t)(r >> 32), 0u, 2u};
+    uint32_t w[4];
+    so_philox4x32_10(ctr, key, w);
+    for (int d = 0; d < 3; ++d)
+      Np[3 * i + d] = choices[(int)(((uint64_t)w[d] * (uint64_t)nchoices) >> 32)];
+    const double u = (double)w[3] * 0x1p-32 + 0x1p-33;
+    const double l = lmin + (lmax - lmin) * u;
+    corrL[3 * i] = corrL[3 * i + 1] = corrL[3 * i + 2] = l;
+  }
+}
+
 /* ======================================================================== */
 /* Index maps                                                               */
 /* ======================================================================== */
@@ -1250,5 +1272,34 @@ void so_rebuild_corrL(const double* SkTot, const int nkeep[3], const double xSte
     for (int t = 0; t < nkeep[d]; ++t) s += SkTot[off + t];
     corrL_out[d] = 2.0 * (s - ((SkTot[off] + SkTot[off + nkeep[d] - 1]) / 2.0)) * xStep[d];
     off += nkeep[d];
+  }
+}
+
+/* Direct restatement of the linear axis covariance: for each axis d and lag
+ * h, the mean over all point pairs (x, x + h e_d) of (f - mu)(f' - mu), mu
+ * the mean over all points.  Test infrastructure for scarl_axis_cov. */
+void so_axis_cov(const double* f, const int L[3], int maxlag, double* mean, double* cov) {
+  const int64_t n = (int64_t)L[0] * L[1] * L[2];
+  double s = 0.0;
+  for (int64_t i = 0; i < n; ++i) s += f[i];
+  const double mu = s / (double)n;
+  *mean = mu;
+  const int64_t st[3] = {1, L[0], (int64_t)L[0] * L[1]};
+  for (int d = 0; d < 3; ++d) {
+#pragma omp parallel for schedule(dynamic)
+    for (int h = 0; h <= maxlag; ++h) {
+      double acc = 0.0;
+      int64_t pairs = 0;
+      for (int z = 0; z < L[2]; ++z)
+        for (int y = 0; y < L[1]; ++y)
+          for (int x = 0; x < L[0]; ++x) {
+            const int c[3] = {x, y, z};
+            if (c[d] + h >= L[d]) continue;
+            const int64_t i = x + (int64_t)L[0] * (y + (int64_t)L[1] * z);
+            acc += (f[i] - mu) * (f[i + (int64_t)h * st[d]] - mu);
+            ++pairs;
+          }
+      cov[d * (maxlag + 1) + h] = acc / (double)pairs;
+    }
   }
 }

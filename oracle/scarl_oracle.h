@@ -42,6 +42,8 @@ int32_t so_pm_jump(int32_t state, uint64_t n);
 void so_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void so_normals(uint64_t seed, uint32_t stream, const int P[3], double* re_im);
 void so_uniforms(uint64_t seed, uint32_t stream, uint64_t first, uint64_t n, double* u);
+void so_ensemble_draw(uint64_t seed, int64_t first, int n, const int* choices, int nchoices,
+                      double lmin, double lmax, int* Np, double* corrL);
 
 /* ---------------- index maps ---------------- */
 int so_verify_inputs(const double xMin[3], const double xMax[3], const double corrL[3],
@@ -113,6 +115,9 @@ int so_generate_sample(int generator, const double xMin[3], const double xMax[3]
 void so_moments(const double* f, int64_t xN, int nmc, double* evntAvg, double* evntStd,
                 double* gAvg, double* gStd);
 void so_tukey(int n, int literal, double* w);
+/* Plain linear covariance along each axis, lags 0..maxlag, of the field
+ * centred by its global mean (direct FP64 sums; cov has 3 (maxlag + 1)). */
+void so_axis_cov(const double* f, const int L[3], int maxlag, double* mean, double* cov);
 void so_rebuild_sk_fft(const double* f, const int L[3], int dir, double avg, double stdDev,
                        int tukey_literal, double* Sk);
 void so_rebuild_corrL(const double* SkTot, const int nkeep[3], const double xStep[3],

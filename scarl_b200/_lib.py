@@ -97,6 +97,13 @@ SIGNATURES = {
                                            C.c_int, C.c_uint64, C.c_uint32, _vp, C.c_char_p,
                                            C.c_size_t]),
     "scarl_generate_sample": (C.c_int, [_vp, C.POINTER(Sample), C.POINTER(GenOpts), _vp]),
+    "scarl_axis_cov": (C.c_int, [_vp, _vp, C.c_int, _ip, C.c_int, _dp, _dp, _dp]),
+    "scarl_ensemble_draw": (C.c_int, [C.c_uint64, C.c_longlong, C.c_int, _ip, C.c_int, C.c_double,
+                                      C.c_double, _ip, _dp]),
+    "scarl_gen_ensemble": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _ip, _dp, _dp, C.c_int,
+                                     C.c_double, C.c_int, C.c_double,
+                                     C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_int,
+                                     C.c_double, C.c_double, C.c_int]),
     "scarl_apply_unity_partition": (C.c_int, [_vp, _vp, _ip, _ip, C.c_int, _ip, _ip]),
     "scarl_add_overlap": (C.c_int, [_vp, _vp, _ip, _ip, _ip]),
     "scarl_multivariate_transformation": (C.c_int, [_vp, _vp, C.c_int, C.c_longlong, C.c_double,

@@ -10,7 +10,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (F32, F64, GEN_DCT, GEN_PADDED, GEN_SHINO, PAD_AUTO, PAD_FULL, GenOpts, Layout,
+from ._lib import (CM_EXPONENTIAL, F32, F64, GEN_DCT, GEN_PADDED, GEN_SHINO, PAD_AUTO, PAD_FULL,
+                   GenOpts, Layout,
                    Sample, ScarlError, Tile, lib)
 
 
@@ -281,6 +282,66 @@ def gen_padded(ctx, Np, xStep, corrL, corrMod=1, nu=0.5, pad=None, normalise=Tru
     return out
 
 
+ENS_AUTOTUNE = 1
+ENS_NO_GRAPH = 2
+ENSEMBLE_AXES = (64, 96, 128, 160, 192, 256)
+
+
+def ensemble_draw(seed, first, n, choices=ENSEMBLE_AXES, lmin=4.0, lmax=32.0):
+    """Shapes (n, 3) and isotropic correlation lengths (n, 3) of realisations
+    first..first+n-1 (Philox4x32-10 at counter {r, r >> 32, 0, 2})."""
+    ch = np.ascontiguousarray(choices, dtype=np.int32)
+    Np = np.zeros((max(n, 1), 3), dtype=np.int32)
+    cl = np.zeros((max(n, 1), 3))
+    _check(lib().scarl_ensemble_draw(int(seed), int(first), int(n),
+                                     ch.ctypes.data_as(C.POINTER(C.c_int)), len(ch), float(lmin),
+                                     float(lmax), Np.ctypes.data_as(C.POINTER(C.c_int)),
+                                     cl.ctypes.data_as(C.POINTER(C.c_double))))
+    return Np[:n], cl[:n]
+
+
+def ensemble_offsets(Np):
+    """First element of each realisation's field in the packed output."""
+    sizes = np.prod(np.asarray(Np, dtype=np.int64).reshape(-1, 3), axis=1)
+    return np.concatenate([[0], np.cumsum(sizes)])
+
+
+def ensemble_fields(out, Np):
+    """Views of the packed ensemble output, one Fortran-order array each."""
+    off = ensemble_offsets(Np)
+    Np = np.asarray(Np).reshape(-1, 3)
+    return [out[off[i]:off[i + 1]].reshape(tuple(int(v) for v in Np[i]), order="F")
+            for i in range(len(Np))]
+
+
+def gen_ensemble(ctx, Np, corrL, xStep=None, corrMod=CM_EXPONENTIAL, nu=0.5, pad_policy=PAD_AUTO,
+                 pad_tol=1e-3, seeds=None, streams=None, dtype=F32, margiFirst=0, avg=0.0,
+                 std_dev=1.0, autotune=False, graph=True, out=None):
+    """n independent realisations of uneven grids in batched launches (one
+    CUDA graph).  Returns the packed output (realisation i at
+    ensemble_offsets(Np)[i], column-major)."""
+    Np = np.ascontiguousarray(np.asarray(Np, dtype=np.int32).reshape(-1, 3))
+    n = Np.shape[0]
+    cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(n, 3))
+    dx = np.ones((n, 3)) if xStep is None else np.broadcast_to(
+        np.asarray(xStep, dtype=np.float64), (n, 3))
+    dx = np.ascontiguousarray(dx, dtype=np.float64)
+    total = int(ensemble_offsets(Np)[-1])
+    if out is None:
+        out = np.empty(total, dtype=_np_dtype(dtype))
+    sd = None if seeds is None else np.ascontiguousarray(seeds, dtype=np.uint64)
+    st = None if streams is None else np.ascontiguousarray(streams, dtype=np.uint32)
+    flags = (ENS_AUTOTUNE if autotune else 0) | (0 if graph else ENS_NO_GRAPH)
+    _check(lib().scarl_gen_ensemble(
+        ctx.handle, _ptr(out), dtype, n, Np.ctypes.data_as(C.POINTER(C.c_int)),
+        dx.ctypes.data_as(C.POINTER(C.c_double)), cl.ctypes.data_as(C.POINTER(C.c_double)),
+        corrMod, float(nu), int(pad_policy), float(pad_tol),
+        None if sd is None else sd.ctypes.data_as(C.POINTER(C.c_uint64)),
+        None if st is None else st.ctypes.data_as(C.POINTER(C.c_uint32)),
+        int(margiFirst), float(avg), float(std_dev), flags), ctx)
+    return out
+
+
 def pad_size(policy, corrMod, corrL, xStep, Np, nu=0.5, tol=1e-3):
     P = (C.c_int * 3)()
     _check(lib().scarl_pad_size(policy, corrMod, nu, _d3(corrL), _d3(xStep), _i3(Np), tol, P))
@@ -379,6 +440,18 @@ def rebuild_Sk(ctx, field, L, avg, stdDev, tukey_literal=True):
                                   int(bool(tukey_literal)),
                                   out.ctypes.data_as(C.POINTER(C.c_double))), ctx)
     return out
+
+
+def axis_cov(ctx, field, L, maxlag):
+    """Mean, variance and covariance (3, maxlag + 1) along each axis of one
+    field (numpy array or device tensor, column-major L), FP64 sums."""
+    L = [int(v) for v in L]
+    cov = np.zeros(3 * (maxlag + 1))
+    m, v = C.c_double(), C.c_double()
+    _check(lib().scarl_axis_cov(ctx.handle, _ptr(field), _dtype_of(field), _i3(L), int(maxlag),
+                                C.byref(m), C.byref(v), cov.ctypes.data_as(C.POINTER(C.c_double))),
+           ctx)
+    return m.value, v.value, cov.reshape(3, maxlag + 1)
 
 
 def rebuild_corrL(SkTot, L, xStep):

@@ -15,8 +15,10 @@ LIB = os.path.join(HERE, "libscarl_b200.so")
 OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-CUDA_SOURCES = ["gen_padded.cu", "gen_f32.cu", "gen_f64.cu", "dct_literal.cu", "post.cu", "stats.cu",
-                "noalloc.cu"]
+CUDA_SOURCES = ["gen_padded.cu", "dct_literal.cu", "post.cu", "stats.cu", "cov.cu", "noalloc.cu"]
+# gen_inst.cu once per (precision, line-length group): the generator pass
+# instantiations compile in parallel
+INSTANCES = [(dt, n) for dt in (4, 8) for n in (0, 256, 512, 1024, 2048)]
 HOST_SOURCES = ["api.cpp", "host_maps.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
@@ -52,8 +54,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 return LIB
     os.makedirs(OBJ, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
-    procs = []
+    jobs = []  # (label, command, object)
+    for dt, n in INSTANCES:
+        obj = os.path.join(OBJ, f"gen_inst_{dt}_{n}.o")
+        jobs.append((f"gen_inst.cu[{dt},{n}]", [nvcc] + ARCH + ["-lineinfo"] + COMMON + [
+            f"-DSCARL_INST_DT={dt}", f"-DSCARL_INST_N={n}", "-c", os.path.join(CSRC, "gen_inst.cu"),
+            "-o", obj], obj))
     for src in CUDA_SOURCES + HOST_SOURCES:
         obj = os.path.join(OBJ, src + ".o")
         cmd = [nvcc] + COMMON + ["-c", os.path.join(CSRC, src), "-o", obj]
@@ -61,14 +67,23 @@ def build(force: bool = False, verbose: bool = False) -> str:
             cmd[1:1] = ARCH + ["-lineinfo"]
         else:
             cmd[1:1] = ["-x", "cu"] + ARCH
-        if verbose:
-            print(" ".join(cmd))
-        procs.append(subprocess.Popen(cmd))
-        objs.append(obj)
-    rcs = [p.wait() for p in procs]
-    if any(rcs):
-        raise RuntimeError("nvcc failed for " + ", ".join(
-            s for s, r in zip(CUDA_SOURCES + HOST_SOURCES, rcs) if r))
+        jobs.append((src, cmd, obj))
+    # longest jobs first, at most one per core
+    pending = list(jobs)
+    running, failed = [], []
+    width = max(1, os.cpu_count() or 1)
+    while pending or running:
+        while pending and len(running) < width:
+            label, cmd, _ = pending.pop(0)
+            if verbose:
+                print(" ".join(cmd))
+            running.append((label, subprocess.Popen(cmd)))
+        label, p = running.pop(0)
+        if p.wait() != 0:
+            failed.append(label)
+    if failed:
+        raise RuntimeError("nvcc failed for " + ", ".join(failed))
+    objs = [j[2] for j in jobs]
     link = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs
     subprocess.check_call(link)
     with open(stamp, "w") as fh:

@@ -44,6 +44,28 @@ struct Mark {
   cudaEvent_t a, b;
 };
 
+// One batched launch of an ensemble: the realisations that share the line
+// length N of a pass, launched with variant var.
+struct EnsGroup {
+  int pass = 1, N = 0, var = 0;
+  std::vector<int> items;  // realisations, largest first
+  std::vector<int> start;  // block offsets (items.size() + 1)
+  BatchMap m{};
+};
+
+// Plan of the most recent ensemble (list of shapes) of a context.
+struct EnsPlan {
+  std::string key;
+  int dt = 4, n = 0;
+  std::vector<GenArgs> args;  // host copies of the device argument blocks
+  std::vector<size_t> off;    // first element of each field in the output
+  size_t total = 0;           // elements of all fields
+  Buf work, dargs, dmap, tmp;
+  std::vector<EnsGroup> groups;  // pass-major
+  bool uploaded = false, tuned = false, graph_failed = false;
+  cudaGraphExec_t exec = nullptr;
+};
+
 }  // namespace
 
 struct scarl_ctx {
@@ -68,6 +90,7 @@ struct scarl_ctx {
   std::map<std::string, std::pair<double, long long>> pstats;
   std::map<long long, int> tune;          // (dtype, pass, N) -> launch variant
   std::map<std::string, bool> tuned_shapes;
+  EnsPlan* ens = nullptr;
 };
 
 namespace {
@@ -599,6 +622,223 @@ int marginal_params(scarl_ctx* ctx, int margiFirst, double avg, double std_dev, 
   return SCARL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Ensembles of uneven grids: per pass, one batched launch per line length.
+// ---------------------------------------------------------------------------
+void ens_free(scarl_ctx* ctx) {
+  EnsPlan* e = ctx->ens;
+  if (!e) return;
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  for (Buf* b : {&e->work, &e->dargs, &e->dmap, &e->tmp}) release(ctx, *b);
+  delete e;
+  ctx->ens = nullptr;
+}
+
+// Block offsets of a group for launch variant v (host).
+int ens_starts(scarl_ctx* ctx, const EnsPlan* e, const EnsGroup& g, int v, std::vector<int>* st) {
+  st->assign(1, 0);
+  for (int i : g.items) {
+    const int nb = gen_pass_blocks(e->dt, g.pass, v, e->args[i]);
+    if (nb < 0) return SCARL_EUNSUPPORTED;
+    if ((long long)st->back() + nb > 2147483647LL)
+      return fail(ctx, SCARL_EINVAL, "ensemble too large for one launch");
+    st->push_back(st->back() + nb);
+  }
+  return SCARL_OK;
+}
+
+// Uploads every group's item list and block offsets (after the stream has
+// drained, since launches in flight read them).
+int ens_maps(scarl_ctx* ctx, EnsPlan* e) {
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<int> h;
+  std::vector<size_t> pos;
+  for (EnsGroup& g : e->groups) {
+    RC(ens_starts(ctx, e, g, g.var, &g.start));
+    pos.push_back(h.size());
+    h.insert(h.end(), g.items.begin(), g.items.end());
+    h.insert(h.end(), g.start.begin(), g.start.end());
+  }
+  RC(ensure(ctx, e->dmap, h.size() * sizeof(int)));
+  CK(cudaMemcpy(e->dmap.p, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+  ctx->h2d += h.size() * sizeof(int);
+  const int* base = static_cast<const int*>(e->dmap.p);
+  for (size_t k = 0; k < e->groups.size(); ++k) {
+    EnsGroup& g = e->groups[k];
+    g.m.args = static_cast<const GenArgs*>(e->dargs.p);
+    g.m.items = base + pos[k];
+    g.m.start = base + pos[k] + g.items.size();
+    g.m.n = (int)g.items.size();
+    g.m.total = g.start.back();
+  }
+  return SCARL_OK;
+}
+
+int ens_build(scarl_ctx* ctx, int dt, int n, const int* Np, const double* dx, const double* cl,
+              int corrMod, double nu, int policy, double tol, const std::string& key) {
+  CK(cudaStreamSynchronize(ctx->stream));
+  ens_free(ctx);
+  EnsPlan* e = new EnsPlan();
+  ctx->ens = e;
+  e->dt = dt;
+  e->n = n;
+  e->args.resize(n);
+  e->off.resize(n);
+  std::vector<size_t> woff(n);
+  size_t wtot = 0, tot = 0;
+  for (int i = 0; i < n; ++i) {
+    const int* np = Np + 3 * i;
+    int P[3];
+    if (pad_size(policy, corrMod, nu, cl + 3 * i, dx + 3 * i, np, tol, P) != SCARL_OK)
+      return fail(ctx, SCARL_EINVAL, "no padded grid for realisation " + std::to_string(i));
+    RC(check_grid(ctx, P, np));
+    PaddedPlan* pl;
+    RC(padded_plan(ctx, dt, P, dx + 3 * i, cl + 3 * i, corrMod, nu, 1, &pl));
+    GenArgs& a = e->args[i];
+    std::memset(&a, 0, sizeof a);
+    for (int d = 0; d < 3; ++d) {
+      a.P[d] = P[d];
+      a.Nout[d] = np[d];
+    }
+    a.Hx = P[0] / 2 + 1;
+    a.Hpad = round_up(a.Hx, 16);
+    RC(twiddles(ctx, P[2], dt, &a.tw_z));
+    RC(twiddles(ctx, P[1], dt, &a.tw_y));
+    RC(twiddles(ctx, P[0], dt, &a.tw_x));
+    set_plan(&a, pl);
+    a.epi.mode = 0;
+    woff[i] = wtot;
+    wtot += ((size_t)a.Hpad * P[1] * np[2] * 2 * dt + 255) / 256 * 256;
+    e->off[i] = tot;
+    tot += (size_t)np[0] * np[1] * np[2];
+  }
+  RC(ensure(ctx, e->work, wtot));
+  for (int i = 0; i < n; ++i) e->args[i].work = static_cast<char*>(e->work.p) + woff[i];
+  e->total = tot;
+  RC(ensure(ctx, e->dargs, (size_t)n * sizeof(GenArgs)));
+  // groups: per pass, realisations by line length; largest realisations first
+  // inside a group, groups with more blocks first
+  for (int pass = 1; pass <= 3; ++pass) {
+    std::map<int, std::vector<int>> by;
+    for (int i = 0; i < n; ++i) {
+      const GenArgs& a = e->args[i];
+      by[pass == 1 ? a.P[2] : (pass == 2 ? a.P[1] : a.P[0] / 2)].push_back(i);
+    }
+    std::vector<EnsGroup> gs;
+    for (auto& kv : by) {
+      EnsGroup g;
+      g.pass = pass;
+      g.N = kv.first;
+      g.items = kv.second;
+      std::stable_sort(g.items.begin(), g.items.end(), [&](int x, int y) {
+        const int* p = e->args[x].Nout;
+        const int* q = e->args[y].Nout;
+        return (long long)p[0] * p[1] * p[2] > (long long)q[0] * q[1] * q[2];
+      });
+      auto it = ctx->tune.find(tune_key(dt, pass, g.N));
+      g.var = it == ctx->tune.end() ? 0 : it->second;
+      std::vector<int> st;
+      if (ens_starts(ctx, e, g, g.var, &st) != SCARL_OK) g.var = 0;
+      RC(ens_starts(ctx, e, g, g.var, &st));
+      g.start = st;
+      gs.push_back(g);
+    }
+    std::stable_sort(gs.begin(), gs.end(), [](const EnsGroup& x, const EnsGroup& y) {
+      return x.start.back() > y.start.back();
+    });
+    e->groups.insert(e->groups.end(), gs.begin(), gs.end());
+  }
+  RC(ens_maps(ctx, e));
+  e->key = key;
+  return SCARL_OK;
+}
+
+const char* kBatchName[3] = {"k_gen_z_batch", "k_mid_y_batch", "k_c2r_x_batch"};
+
+int ens_launch(scarl_ctx* ctx, EnsPlan* e) {
+  for (EnsGroup& g : e->groups) {
+    Prof p(ctx, kBatchName[g.pass - 1]);
+    CK(launch_gen_pass_batch(e->dt, g.pass, g.var, e->args[g.items[0]], g.m, ctx->stream));
+  }
+  return SCARL_OK;
+}
+
+// Records the plan's launches into a CUDA graph; on any failure the plan
+// keeps launching eagerly.
+void ens_capture(scarl_ctx* ctx, EnsPlan* e) {
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    e->graph_failed = true;
+    return;
+  }
+  bool ok = true;
+  for (EnsGroup& gr : e->groups)
+    if (launch_gen_pass_batch(e->dt, gr.pass, gr.var, e->args[gr.items[0]], gr.m, ctx->stream) !=
+        cudaSuccess)
+      ok = false;
+  if (cudaStreamEndCapture(ctx->stream, &g) != cudaSuccess) ok = false;
+  if (ok && cudaGraphInstantiate(&e->exec, g, 0) != cudaSuccess) {
+    e->exec = nullptr;
+    ok = false;
+  }
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    cudaGetLastError();
+    e->graph_failed = true;
+  }
+}
+
+// Times every valid variant of every group (CUDA events, best of 3 after a
+// warm-up launch) and keeps the fastest.  The field is regenerated by the
+// caller afterwards.
+int ens_tune(scarl_ctx* ctx, EnsPlan* e) {
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (EnsGroup& g : e->groups) {
+    int best = g.var;
+    float best_ms = 1e30f;
+    for (int v = 0; v < gen_variant_count(e->dt, g.pass); ++v) {
+      std::vector<int> st;
+      if (ens_starts(ctx, e, g, v, &st) != SCARL_OK) continue;
+      CK(cudaStreamSynchronize(ctx->stream));
+      RC(ensure(ctx, e->tmp, st.size() * sizeof(int)));
+      CK(cudaMemcpy(e->tmp.p, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BatchMap m = g.m;
+      m.start = static_cast<const int*>(e->tmp.p);
+      m.total = st.back();
+      const GenArgs& rep = e->args[g.items[0]];
+      if (launch_gen_pass_batch(e->dt, g.pass, v, rep, m, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      float tmin = 1e30f;
+      for (int rep_i = 0; rep_i < 3; ++rep_i) {
+        CK(cudaEventRecord(e0, ctx->stream));
+        CK(launch_gen_pass_batch(e->dt, g.pass, v, rep, m, ctx->stream));
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        tmin = std::min(tmin, ms);
+      }
+      if (tmin < best_ms) {
+        best_ms = tmin;
+        best = v;
+      }
+    }
+    g.var = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e->exec) {
+    cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+  }
+  return ens_maps(ctx, e);
+}
+
 // Blend tables of every tile: per tile, per axis lo[Np], hi[Np] (doubles)
 // then flags[Np] (bytes), uploaded once.
 struct BlendTabs {
@@ -796,6 +1036,7 @@ int scarl_ctx_destroy(scarl_ctx* ctx) {
   for (auto& kv : ctx->plans) release(ctx, kv.second.tabs);
   for (auto& kv : ctx->twiddles) release(ctx, kv.second);
   for (auto& kv : ctx->dct_tabs) release(ctx, kv.second);
+  ens_free(ctx);
   for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
   if (ctx->pin_ev) cudaEventDestroy(ctx->pin_ev);
   if (ctx->pin) cudaFreeHost(ctx->pin);
@@ -1065,6 +1306,93 @@ int scarl_gen_padded(scarl_ctx* ctx, void* out, int dtype, const int Np[3], cons
   a.epi.out = dev;
   RC(run_passes(ctx, dtype, a));
   return finish_out(ctx, out, dev, n * dtype, host);
+}
+
+int scarl_ensemble_draw(uint64_t seed, long long first, int n, const int* choices, int nchoices,
+                        double lmin, double lmax, int* Np, double* corrL) {
+  return ensemble_draw(seed, first, n, choices, nchoices, lmin, lmax, Np, corrL);
+}
+
+int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* Np,
+                       const double* xStep, const double* corrL, int corrMod, double nu,
+                       int pad_policy, double pad_tol, const uint64_t* seeds,
+                       const uint32_t* streams, int margiFirst, double avg, double std_dev,
+                       int flags) {
+  RC(begin(ctx));
+  if (!out || !Np || !xStep || !corrL) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (n < 1 || n > 65536) return fail(ctx, SCARL_EINVAL, "ensemble size must be in [1, 65536]");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  if (corrMod < 1 || corrMod > 3) return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
+  if (corrMod == SCARL_CM_VON_KARMAN && !(nu > 0.0)) return fail(ctx, SCARL_EINVAL, "nu must be > 0");
+  if (pad_policy != SCARL_PAD_FULL && pad_policy != SCARL_PAD_AUTO)
+    return fail(ctx, SCARL_EINVAL, "unknown padding policy");
+  if (margiFirst < 0 || margiFirst > 2) return fail(ctx, SCARL_EINVAL, "First-order marginal not detected");
+  const double tol = pad_tol > 0.0 ? pad_tol : 1e-3;
+  std::string key;
+  {
+    char b[160];
+    std::snprintf(b, sizeof b, "%d|%d|%a|%d|%a|%d", dtype, corrMod, nu, pad_policy, tol, n);
+    key = b;
+    key.reserve(key.size() + (size_t)n * 96);
+    for (int i = 0; i < n; ++i) {
+      for (int d = 0; d < 3; ++d) {
+        if (Np[3 * i + d] < 1) return fail(ctx, SCARL_EINVAL, "Np must be >= 1");
+        if (!(xStep[3 * i + d] > 0.0) || !(corrL[3 * i + d] > 0.0))
+          return fail(ctx, SCARL_EINVAL, "xStep and corrL must be > 0");
+      }
+      std::snprintf(b, sizeof b, "|%d,%d,%d,%a,%a,%a,%a,%a,%a", Np[3 * i], Np[3 * i + 1],
+                    Np[3 * i + 2], xStep[3 * i], xStep[3 * i + 1], xStep[3 * i + 2], corrL[3 * i],
+                    corrL[3 * i + 1], corrL[3 * i + 2]);
+      key += b;
+    }
+  }
+  if (!ctx->ens || ctx->ens->key != key)
+    RC(ens_build(ctx, dtype, n, Np, xStep, corrL, corrMod, nu, pad_policy, tol, key));
+  EnsPlan* e = ctx->ens;
+  void* dev;
+  bool host;
+  RC(out_dev(ctx, out, e->total * dtype, &dev, &host));
+  double ms = 1.0, mu = 0.0;
+  if (margiFirst) RC(marginal_params(ctx, margiFirst, avg, std_dev, &ms, &mu));
+  bool changed = !e->uploaded;
+  for (int i = 0; i < n; ++i) {
+    GenArgs& a = e->args[i];
+    const uint64_t sd = seeds ? seeds[i] : (uint64_t)i;
+    const uint32_t k0 = (uint32_t)sd, k1 = (uint32_t)(sd >> 32), st = streams ? streams[i] : 0u;
+    void* o = static_cast<char*>(dev) + e->off[i] * dtype;
+    if (a.k0 != k0 || a.k1 != k1 || a.stream != st || a.epi.out != o || a.epi.marginal != margiFirst ||
+        a.epi.ms != ms || a.epi.mmu != mu) {
+      a.k0 = k0;
+      a.k1 = k1;
+      a.stream = st;
+      a.epi.out = o;
+      a.epi.marginal = margiFirst;
+      a.epi.ms = ms;
+      a.epi.mmu = mu;
+      changed = true;
+    }
+  }
+  if (changed) {
+    const size_t bytes = (size_t)n * sizeof(GenArgs);
+    void* pin;
+    RC(pinned(ctx, bytes, &pin));
+    std::memcpy(pin, e->args.data(), bytes);
+    RC(upload_pinned(ctx, e->dargs.p, bytes));
+    e->uploaded = true;
+  }
+  if ((flags & SCARL_ENS_AUTOTUNE) && !e->tuned) {
+    RC(ens_tune(ctx, e));
+    e->tuned = true;
+  }
+  const bool graph = !(flags & SCARL_ENS_NO_GRAPH) && !ctx->profile && !e->graph_failed;
+  if (graph && e->exec) {
+    CK(cudaGraphLaunch(e->exec, ctx->stream));
+    ctx->launches += (long long)e->groups.size();
+  } else {
+    RC(ens_launch(ctx, e));
+    if (graph) ens_capture(ctx, e);
+  }
+  return finish_out(ctx, out, dev, e->total * dtype, host);
 }
 
 int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen_opts* o_in,
@@ -1352,6 +1680,79 @@ int scarl_moments(scarl_ctx* ctx, const void* field, int dtype, long long xN, in
   const double ga = S / (double)(xN * nmc);
   if (gAvg) *gAvg = ga;
   if (gStd) *gStd = std::sqrt(S2 / (double)(xN * nmc) - ga * ga);
+  return SCARL_OK;
+}
+
+int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
+                   double* mean, double* var, double* cov) {
+  RC(begin(ctx));
+  if (!field || !L || !mean || !var || !cov) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  if (maxlag < 0) return fail(ctx, SCARL_EINVAL, "maxlag must be >= 0");
+  int Nc[3];
+  for (int d = 0; d < 3; ++d) {
+    if (L[d] < 1 || maxlag >= L[d]) return fail(ctx, SCARL_EINVAL, "maxlag must be below every extent");
+    int M = 8;
+    while (M < L[d] + maxlag) M <<= 1;
+    if (M > 4096) return fail(ctx, SCARL_EUNSUPPORTED, "L[d] + maxlag must be <= 4096");
+    Nc[d] = M / 2;
+  }
+  const size_t n = (size_t)L[0] * L[1] * L[2];
+  const void* dev;
+  RC(in_dev(ctx, ctx->stage_in, field, n * dtype, &dev));
+  // mean (FP64 sums)
+  const int nb = sums_blocks((int64_t)n);
+  RC(ensure(ctx, ctx->part, (size_t)nb * 2 * 8));
+  {
+    Prof p(ctx, "k_sums");
+    CK(launch_sums(dtype, dev, (int64_t)n, 1, (double*)ctx->part.p, nb, ctx->stream));
+  }
+  std::vector<double> h((size_t)nb * 2);
+  CK(cudaMemcpyAsync(h.data(), ctx->part.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->d2h += h.size() * 8;
+  double s1 = 0.0;
+  for (int b = 0; b < nb; ++b) s1 += h[2 * (size_t)b];
+  const double mu = s1 / (double)n;
+  // per axis: power pass, FP64 lag sums
+  const int H = maxlag + 1;
+  int nblk[3];
+  size_t pbytes = 0;
+  for (int d = 0; d < 3; ++d) {
+    nblk[d] = axis_power_blocks(dtype, L, d, Nc[d]);
+    if (nblk[d] < 1) return fail(ctx, SCARL_EDEVICE, "no launch configuration for the covariance pass");
+    pbytes = std::max(pbytes, (size_t)nblk[d] * (Nc[d] + 1) * 8);
+  }
+  RC(ensure(ctx, ctx->t1, pbytes));
+  RC(ensure(ctx, ctx->t2, (size_t)(2048 + 1) * 8 + (size_t)3 * H * 8));
+  double* bins = (double*)ctx->t2.p;
+  double* S = bins + 2048 + 1;
+  for (int d = 0; d < 3; ++d) {
+    const void* tw;
+    const void* tw64;
+    RC(twiddles(ctx, 2 * Nc[d], dtype, &tw));
+    RC(twiddles(ctx, 2 * Nc[d], 8, &tw64));
+    {
+      Prof p(ctx, "k_axis_power");
+      CK(launch_axis_power(dtype, dev, L, d, Nc[d], mu, tw, (double*)ctx->t1.p, nblk[d], ctx->stream));
+    }
+    {
+      Prof p(ctx, "k_cov_lags", 2);
+      CK(launch_cov_lags((const double*)ctx->t1.p, nblk[d], Nc[d], maxlag, (const double*)tw64, bins,
+                         S + (size_t)d * H, ctx->stream));
+    }
+  }
+  std::vector<double> hs((size_t)3 * H);
+  CK(cudaMemcpyAsync(hs.data(), S, hs.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->d2h += hs.size() * 8;
+  for (int d = 0; d < 3; ++d)
+    for (int lag = 0; lag < H; ++lag) {
+      const double pairs = (double)(L[d] - lag) * (double)(n / (size_t)L[d]);
+      cov[(size_t)d * H + lag] = hs[(size_t)d * H + lag] / pairs;
+    }
+  *mean = mu;
+  *var = cov[0];
   return SCARL_OK;
 }
 

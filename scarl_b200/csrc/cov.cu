@@ -1,0 +1,255 @@
+// cov.cu -- streamed axis-covariance estimator for large fields: the sample
+// covariance along each axis up to lag H,
+//   C_d(h) = sum over point pairs (x, x + h e_d) of (f(x) - mu)(f(x + h e_d) - mu),
+// accumulated in FP64.  (Stat_ScaRL's rebuild_Sk_FFT, SRC_F/Stat_ScaRL/
+// statistics_RF.f90:258-462, windows each line and wraps it around; this
+// estimator keeps the plain linear lag sum that a covariance model is checked
+// against.)
+//
+// Each line of L_d values, centred by the global mean, is zero-padded to
+// M = 2N >= L_d + H points and transformed as one complex DFT of length N
+// (even samples real, odd samples imaginary, then the even/odd split).  The
+// power |Y_k|^2, k = 0..N, is summed over all lines of the block in the
+// working precision and added to per-thread FP64 accumulators; one pass reads
+// the field once.  The circular autocorrelation of the padded line,
+//   S(h) = (1/M) sum_k |Y_k|^2 e^{-2 pi i k h / M},
+// equals the linear lag sum for h <= M - L_d (Wiener-Khinchin); the cosine
+// sum over k is formed in FP64 by k_cov_lags.
+#include <algorithm>
+
+#include "fft_engine.cuh"
+#include "scarl_internal.h"
+
+namespace scarl {
+
+namespace {
+
+constexpr int kCovE = 16;
+
+template <int N> __host__ __device__ constexpr int cov_E() { return N < kCovE ? N : kCovE; }
+// lines per block: ROW (x lines, lanes along a line) and column layouts
+template <int N, bool ROW> __host__ __device__ constexpr int cov_B() {
+  return ROW ? ((512 / (N / cov_E<N>())) < 1 ? 1 : ((512 / (N / cov_E<N>())) > 32 ? 32 : 512 / (N / cov_E<N>())))
+             : ((1024 / (N / cov_E<N>())) > 16 ? 16 : 1024 / (N / cov_E<N>()));
+}
+
+struct CovGeom {
+  const void* f;
+  int n;          // points per line (L_d)
+  int64_t na;     // lines along the fastest other axis
+  int64_t sa, sb; // element strides of the two other axes
+  int64_t st;     // element stride along the line
+  int64_t nlines;
+  double mu;
+  const void* tw;  // e^{2 pi i m / M}, m < M, working precision
+  double* partial; // gridDim.x * (N + 1)
+};
+
+template <typename T, int N, bool ROW>
+__global__ void __launch_bounds__(cov_B<N, ROW>() * (N / cov_E<N>()))
+    k_axis_power(const CovGeom g) {
+  using C = cplx_t<T>;
+  constexpr int E = cov_E<N>();
+  constexpr int B = cov_B<N, ROW>();
+  constexpr int TPL = N / E;
+  constexpr int NT = B * TPL;
+  constexpr int QB = (N + NT) / NT;  // bins per thread (bins 0..N)
+  constexpr SmemOrder O = ROW ? SmemOrder::LineFast : SmemOrder::BatchFast;
+  constexpr int LS = ROW ? line_slots<N, E>() : 0;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int b = ROW ? (int)threadIdx.x / TPL : (int)threadIdx.x % B;
+  const int t = ROW ? (int)threadIdx.x % TPL : (int)threadIdx.x / B;
+  const T* f = static_cast<const T*>(g.f);
+  const C* tw = static_cast<const C*>(g.tw);
+  double acc[QB];
+#pragma unroll
+  for (int q = 0; q < QB; ++q) acc[q] = 0.0;
+  const int64_t ngroups = (g.nlines + B - 1) / B;
+  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const int64_t l = grp * B + b;
+    const bool valid = l < g.nlines;
+    const int64_t base = valid ? (l % g.na) * g.sa + (l / g.na) * g.sb : 0;
+    auto val = [&](int i) -> T {
+      if (!valid || i >= g.n) return T(0);
+      return (T)((double)__ldg(f + base + (int64_t)i * g.st) - g.mu);
+    };
+    auto load = each_load<C, N, E>([&](int k) -> C { return mk(val(2 * k), val(2 * k + 1)); });
+    constexpr int RL = last_radix<N, E>();
+    C z[E];
+    auto store = [&](int j, const C* o) {
+      const int q = (j - t) / TPL;
+#pragma unroll
+      for (int r = 0; r < RL; ++r) z[q * RL + r] = o[r];
+    };
+    line_ifft<C, N, E, O, B, LS>(sm, b, t, tw, 2, load, store);
+    __syncthreads();  // every thread has left the transform's shared-memory stages
+    {
+      constexpr int NBL = E / RL;
+#pragma unroll
+      for (int q = 0; q < NBL; ++q) {
+        const int j = t + TPL * q;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) sm[b * N + j + r * (N / RL)] = z[q * RL + r];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < QB; ++q) {
+      const int k = (int)threadIdx.x + NT * q;
+      if (k > N) break;
+      const C w = __ldg(tw + k);
+      T s = T(0);
+      for (int bb = 0; bb < B; ++bb) {
+        const C zk = sm[bb * N + (k == N ? 0 : k)];
+        const C zc = cconj(sm[bb * N + (k == 0 || k == N ? 0 : N - k)]);
+        const C e = mk((zk.x + zc.x) * T(0.5), (zk.y + zc.y) * T(0.5));
+        // (zk - zc) / (2i)
+        const C od = mk((zk.y - zc.y) * T(0.5), -(zk.x - zc.x) * T(0.5));
+        const C y = cadd(e, cmul(w, od));
+        s += y.x * y.x + y.y * y.y;
+      }
+      acc[q] += (double)s;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < QB; ++q) {
+    const int k = (int)threadIdx.x + NT * q;
+    if (k <= N) g.partial[(int64_t)blockIdx.x * (N + 1) + k] = acc[q];
+  }
+}
+
+template <typename T, int N, bool ROW> size_t cov_smem() {
+  constexpr int E = cov_E<N>();
+  constexpr int B = cov_B<N, ROW>();
+  const size_t fft = (size_t)B * line_slots<N, E>() * sizeof(cplx_t<T>);
+  const size_t pw = (size_t)B * N * sizeof(cplx_t<T>);
+  return fft > pw ? fft : pw;
+}
+
+template <typename T, int N, bool ROW>
+cudaError_t run_power(CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
+  auto kern = k_axis_power<T, N, ROW>;
+  const size_t smem = cov_smem<T, N, ROW>();
+  const int threads = cov_B<N, ROW>() * (N / cov_E<N>());
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess) return e;
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t ngroups = (g.nlines + cov_B<N, ROW>() - 1) / cov_B<N, ROW>();
+  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>(ngroups, (int64_t)std::max(per_sm, 1) * sms));
+  if (blocks && want_blocks < 0) {  // query only
+    *blocks = nb;
+    return cudaSuccess;
+  }
+  const int grid = want_blocks > 0 ? want_blocks : nb;
+  kern<<<grid, threads, smem, s>>>(g);
+  return cudaGetLastError();
+}
+
+template <typename T, bool ROW>
+cudaError_t run_power_n(int N, CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
+  switch (N) {
+    case 4: return run_power<T, 4, ROW>(g, want_blocks, blocks, s);
+    case 8: return run_power<T, 8, ROW>(g, want_blocks, blocks, s);
+    case 16: return run_power<T, 16, ROW>(g, want_blocks, blocks, s);
+    case 32: return run_power<T, 32, ROW>(g, want_blocks, blocks, s);
+    case 64: return run_power<T, 64, ROW>(g, want_blocks, blocks, s);
+    case 128: return run_power<T, 128, ROW>(g, want_blocks, blocks, s);
+    case 256: return run_power<T, 256, ROW>(g, want_blocks, blocks, s);
+    case 512: return run_power<T, 512, ROW>(g, want_blocks, blocks, s);
+    case 1024: return run_power<T, 1024, ROW>(g, want_blocks, blocks, s);
+    case 2048: return run_power<T, 2048, ROW>(g, want_blocks, blocks, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+CovGeom geom(const void* f, const int L[3], int dir, double mu, const void* tw, double* partial) {
+  CovGeom g;
+  g.f = f;
+  g.n = L[dir];
+  g.mu = mu;
+  g.tw = tw;
+  g.partial = partial;
+  const int64_t L0 = L[0], L1 = L[1], L2 = L[2];
+  if (dir == 0) {  // x lines, consecutive in memory
+    g.na = L1; g.sa = L0; g.sb = L0 * L1; g.st = 1; g.nlines = L1 * L2;
+  } else if (dir == 1) {  // y lines, consecutive x in a group
+    g.na = L0; g.sa = 1; g.sb = L0 * L1; g.st = L0; g.nlines = L0 * L2;
+  } else {  // z lines
+    g.na = L0; g.sa = 1; g.sb = L0; g.st = L0 * L1; g.nlines = L0 * L1;
+  }
+  return g;
+}
+
+cudaError_t dispatch(int dt, int dir, int N, CovGeom g, int want, int* blocks, cudaStream_t s) {
+  if (dt == 8) return dir == 0 ? run_power_n<double, true>(N, g, want, blocks, s)
+                               : run_power_n<double, false>(N, g, want, blocks, s);
+  return dir == 0 ? run_power_n<float, true>(N, g, want, blocks, s)
+                  : run_power_n<float, false>(N, g, want, blocks, s);
+}
+
+// P_k = sum over blocks of the partial power (one thread per bin).
+__global__ void k_cov_bins(const double* __restrict__ partial, int nblocks, int nbins,
+                           double* __restrict__ bins) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nbins) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += partial[(int64_t)b * nbins + k];
+  bins[k] = s;
+}
+
+// S(h) = (1/M) [P_0 + (-1)^h P_N + 2 sum_{k=1}^{N-1} P_k cos(2 pi k h / M)],
+// one block per lag, FP64.
+__global__ void k_cov_lags(const double* __restrict__ bins, int N, const double2* __restrict__ tw64,
+                           double* __restrict__ S) {
+  const int h = blockIdx.x;
+  const int M = 2 * N;
+  double s = 0.0;
+  for (int k = 1 + threadIdx.x; k < N; k += blockDim.x)
+    s += bins[k] * tw64[(int)(((int64_t)k * h) % M)].x;
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0)
+      S[h] = (bins[0] + ((h & 1) ? -bins[N] : bins[N]) + 2.0 * s) / (double)M;
+  }
+}
+
+}  // namespace
+
+int axis_power_blocks(int dt, const int L[3], int dir, int N) {
+  int nb = -1;
+  CovGeom g = geom(nullptr, L, dir, 0.0, nullptr, nullptr);
+  if (dispatch(dt, dir, N, g, -1, &nb, nullptr) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return nb;
+}
+
+cudaError_t launch_axis_power(int dt, const void* f, const int L[3], int dir, int N, double mu,
+                              const void* tw, double* partial, int nblocks, cudaStream_t s) {
+  CovGeom g = geom(f, L, dir, mu, tw, partial);
+  return dispatch(dt, dir, N, g, nblocks, nullptr, s);
+}
+
+cudaError_t launch_cov_lags(const double* partial, int nblocks, int N, int maxlag,
+                            const double* tw64, double* bins, double* S, cudaStream_t s) {
+  k_cov_bins<<<(N + 1 + 255) / 256, 256, 0, s>>>(partial, nblocks, N + 1, bins);
+  k_cov_lags<<<maxlag + 1, 256, 0, s>>>(bins, N, reinterpret_cast<const double2*>(tw64), S);
+  return cudaGetLastError();
+}
+
+}  // namespace scarl

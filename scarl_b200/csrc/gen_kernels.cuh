@@ -72,13 +72,12 @@ template <> __device__ __forceinline__ double powT<double>(double s, double e) {
 // Pass 1: synthesise + inverse DFT along z.
 // ---------------------------------------------------------------------------
 template <typename T, int N, int E, int B, int SPEC>
-__global__ void __launch_bounds__(B*(N / E)) k_gen_z(const GenArgs a) {
+__device__ __forceinline__ void gen_z_body(const GenArgs& a, int bx, int ky) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int b = threadIdx.x % B, t = threadIdx.x / B;
-  const int kx = blockIdx.x * B + b;
-  const int ky = blockIdx.y;
+  const int kx = bx * B + b;
   const bool valid = kx < a.Hx;
   C* work = static_cast<C*>(a.work);
   const T* ax = static_cast<const T*>(a.ax);
@@ -151,14 +150,13 @@ __global__ void __launch_bounds__(B*(N / E)) k_gen_z(const GenArgs a) {
 // Pass 2: inverse DFT along y, in place, keep y < Ny.
 // ---------------------------------------------------------------------------
 template <typename T, int N, int E, int B>
-__global__ void __launch_bounds__(B*(N / E)) k_mid_y(const GenArgs a) {
+__device__ __forceinline__ void mid_y_body(const GenArgs& a, int bx, int z) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int b = threadIdx.x % B, t = threadIdx.x / B;
-  const int kx0 = blockIdx.x * B;
+  const int kx0 = bx * B;
   const int kx = kx0 + b;
-  const int z = blockIdx.y;
   const bool valid = kx < a.Hx;
   C* colblk = static_cast<C*>(a.work) + (size_t)z * a.P[1] * a.Hpad + kx0;
   const size_t pitch = (size_t)a.Hpad;
@@ -195,7 +193,7 @@ template <int N, int E> __host__ __device__ constexpr int c2r_line_stride() {
 }
 
 template <typename T, int N, int E, int B>
-__global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
+__device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
   using C = cplx_t<T>;
   constexpr int TPL = N / E;
   constexpr int LS = c2r_line_stride<N, E>();
@@ -205,7 +203,7 @@ __global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
   const int64_t nlines = (int64_t)Ny * Nz;
   const C* work = static_cast<const C*>(a.work);
   const int b = threadIdx.x / TPL, t = threadIdx.x % TPL;
-  const int64_t l = (int64_t)blockIdx.x * B + b;
+  const int64_t l = (int64_t)bx * B + b;
   const bool valid = l < nlines;
   const int y = valid ? (int)(l % Ny) : 0, z = valid ? (int)(l / Ny) : 0;
   {  // stage the raw half-spectrum line (N + 1 values, padded to 16 bytes)
@@ -246,5 +244,57 @@ __global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
   line_ifft<C, N, E, SmemOrder::LineFast, B, LS>(sm, b, t, twx, 2, load, store);
 }
 
+// ---------------------------------------------------------------------------
+// Kernels.  Single-tile launches take the argument block by value and use the
+// grid coordinates directly; batched launches cover the blocks of several
+// realisations of one line length with a flat grid, each block finding its
+// realisation in the group's block-offset table.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int batch_item(const BatchMap& m, int* local) {
+  const int blk = (int)blockIdx.x;
+  int lo = 0, hi = m.n;  // start[lo] <= blk < start[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(m.start + mid) <= blk) lo = mid;
+    else hi = mid;
+  }
+  *local = blk - __ldg(m.start + lo);
+  return __ldg(m.items + lo);
+}
+
+template <typename T, int N, int E, int B, int SPEC>
+__global__ void __launch_bounds__(B*(N / E)) k_gen_z(const GenArgs a) {
+  gen_z_body<T, N, E, B, SPEC>(a, blockIdx.x, blockIdx.y);
+}
+template <typename T, int N, int E, int B, int SPEC>
+__global__ void __launch_bounds__(B*(N / E)) k_gen_z_batch(const BatchMap m) {
+  int loc;
+  const GenArgs a = m.args[batch_item(m, &loc)];
+  const int gx = (a.Hx + B - 1) / B;
+  gen_z_body<T, N, E, B, SPEC>(a, loc % gx, loc / gx);
+}
+
+template <typename T, int N, int E, int B>
+__global__ void __launch_bounds__(B*(N / E)) k_mid_y(const GenArgs a) {
+  mid_y_body<T, N, E, B>(a, blockIdx.x, blockIdx.y);
+}
+template <typename T, int N, int E, int B>
+__global__ void __launch_bounds__(B*(N / E)) k_mid_y_batch(const BatchMap m) {
+  int loc;
+  const GenArgs a = m.args[batch_item(m, &loc)];
+  const int gx = (a.Hx + B - 1) / B;
+  mid_y_body<T, N, E, B>(a, loc % gx, loc / gx);
+}
+
+template <typename T, int N, int E, int B>
+__global__ void __launch_bounds__(B*(N / E)) k_c2r_x(const GenArgs a) {
+  c2r_x_body<T, N, E, B>(a, blockIdx.x);
+}
+template <typename T, int N, int E, int B>
+__global__ void __launch_bounds__(B*(N / E)) k_c2r_x_batch(const BatchMap m) {
+  int loc;
+  const GenArgs a = m.args[batch_item(m, &loc)];
+  c2r_x_body<T, N, E, B>(a, loc);
+}
 
 }  // namespace scarl

@@ -44,9 +44,9 @@ __host__ __device__ constexpr bool variant_ok() {
   return threads >= 1 && threads <= 1024 && smem <= 220 * 1024 && (N % Ee) == 0;
 }
 
-template <typename K>
+template <typename K, typename A>
 inline cudaError_t launch_k(K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                            const GenArgs& a) {
+                            const A& a) {
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -55,42 +55,64 @@ inline cudaError_t launch_k(K kernel, dim3 grid, dim3 block, size_t smem, cudaSt
   return cudaGetLastError();
 }
 
+// Each run_*_v launches one variant: with bm == nullptr a single tile (grid
+// from a), else the batched kernel over bm->total blocks.  With blocks != 0
+// nothing is launched and *blocks receives the tile's block count.
 template <typename T, int N, int E0, int B, int SPEC>
-inline cudaError_t run_gen_z_v(const GenArgs& a, cudaStream_t s) {
+inline cudaError_t run_gen_z_v(const GenArgs& a, const BatchMap* bm, int* blocks, cudaStream_t s) {
   constexpr int E = eff_E<N, E0>();
   if constexpr (!variant_ok<T, N, E, B, false>()) {
     return cudaErrorInvalidConfiguration;
   } else {
     dim3 grid((a.Hx + B - 1) / B, a.P[1], 1);
+    if (blocks) {
+      *blocks = (int)(grid.x * grid.y);
+      return cudaSuccess;
+    }
     dim3 block(B * (N / E));
     size_t smem = (size_t)B * line_slots<N, E>() * sizeof(cplx_t<T>);
+    if (bm) {
+      if constexpr (SPEC == SPEC_PHILOX)
+        return launch_k(k_gen_z_batch<T, N, E, B, SPEC>, dim3(bm->total), block, smem, s, *bm);
+      return cudaErrorInvalidConfiguration;
+    }
     return launch_k(k_gen_z<T, N, E, B, SPEC>, grid, block, smem, s, a);
   }
 }
 
 template <typename T, int N, int E0, int B>
-inline cudaError_t run_mid_y_v(const GenArgs& a, cudaStream_t s) {
+inline cudaError_t run_mid_y_v(const GenArgs& a, const BatchMap* bm, int* blocks, cudaStream_t s) {
   constexpr int E = eff_E<N, E0>();
   if constexpr (!variant_ok<T, N, E, B, false>()) {
     return cudaErrorInvalidConfiguration;
   } else {
     dim3 grid((a.Hx + B - 1) / B, a.Nout[2], 1);
+    if (blocks) {
+      *blocks = (int)(grid.x * grid.y);
+      return cudaSuccess;
+    }
     dim3 block(B * (N / E));
     size_t smem = (size_t)B * line_slots<N, E>() * sizeof(cplx_t<T>);
+    if (bm) return launch_k(k_mid_y_batch<T, N, E, B>, dim3(bm->total), block, smem, s, *bm);
     return launch_k(k_mid_y<T, N, E, B>, grid, block, smem, s, a);
   }
 }
 
 template <typename T, int N, int E0, int B>
-inline cudaError_t run_c2r_x_v(const GenArgs& a, cudaStream_t s) {
+inline cudaError_t run_c2r_x_v(const GenArgs& a, const BatchMap* bm, int* blocks, cudaStream_t s) {
   constexpr int E = eff_E<N, E0>();
   if constexpr (!variant_ok<T, N, E, B, true>()) {
     return cudaErrorInvalidConfiguration;
   } else {
     const int64_t nlines = (int64_t)a.Nout[1] * a.Nout[2];
     dim3 grid((unsigned)((nlines + B - 1) / B), 1, 1);
+    if (blocks) {
+      *blocks = (int)grid.x;
+      return cudaSuccess;
+    }
     dim3 block(B * (N / E));
     size_t smem = (size_t)B * c2r_line_stride<N, E>() * sizeof(cplx_t<T>);
+    if (bm) return launch_k(k_c2r_x_batch<T, N, E, B>, dim3(bm->total), block, smem, s, *bm);
     return launch_k(k_c2r_x<T, N, E, B>, grid, block, smem, s, a);
   }
 }
@@ -99,31 +121,35 @@ inline cudaError_t run_c2r_x_v(const GenArgs& a, cudaStream_t s) {
 // below 128 (64 for pass 3) have only variant 0; SPEC_INJECT / SPEC_SHINO
 // pass-1 kernels only variant 0.
 template <typename T, int N>
-inline cudaError_t run_pass_n(int pass, int v, const GenArgs& a, cudaStream_t s) {
+inline cudaError_t run_pass_n(int pass, int v, const GenArgs& a, const BatchMap* bm, int* nb,
+                              cudaStream_t s) {
   using CV = ColVars<T>;
   using RV = RowVars<T>;
   constexpr bool tuned_col = N >= 128;
   constexpr bool tuned_row = N >= 64;
-#define SCARL_COLV(I)                                                                        \
-  case I:                                                                                    \
-    if constexpr (I < CV::n && tuned_col) {                                                  \
-      if (pass == 1) return run_gen_z_v<T, N, CV::v[I].E, CV::v[I].B, SPEC_PHILOX>(a, s);    \
-      return run_mid_y_v<T, N, CV::v[I].E, CV::v[I].B>(a, s);                                \
-    }                                                                                        \
+#define SCARL_COLV(I)                                                                     \
+  case I:                                                                                 \
+    if constexpr (I < CV::n && tuned_col) {                                               \
+      if (pass == 1)                                                                      \
+        return run_gen_z_v<T, N, CV::v[I].E, CV::v[I].B, SPEC_PHILOX>(a, bm, nb, s);      \
+      return run_mid_y_v<T, N, CV::v[I].E, CV::v[I].B>(a, bm, nb, s);                     \
+    }                                                                                     \
     return cudaErrorInvalidConfiguration;
-#define SCARL_ROWV(I)                                                                        \
-  case I:                                                                                    \
-    if constexpr (I < RV::n && tuned_row) return run_c2r_x_v<T, N, RV::v[I].E, RV::v[I].B>(a, s); \
+#define SCARL_ROWV(I)                                                                     \
+  case I:                                                                                 \
+    if constexpr (I < RV::n && tuned_row)                                                 \
+      return run_c2r_x_v<T, N, RV::v[I].E, RV::v[I].B>(a, bm, nb, s);                     \
     return cudaErrorInvalidConfiguration;
   if (pass == 1 && a.spec != SPEC_PHILOX) {
     if (v != 0) return cudaErrorInvalidConfiguration;
-    if (a.spec == SPEC_INJECT) return run_gen_z_v<T, N, CV::v[0].E, CV::v[0].B, SPEC_INJECT>(a, s);
-    return run_gen_z_v<T, N, CV::v[0].E, CV::v[0].B, SPEC_SHINO>(a, s);
+    if (a.spec == SPEC_INJECT)
+      return run_gen_z_v<T, N, CV::v[0].E, CV::v[0].B, SPEC_INJECT>(a, bm, nb, s);
+    return run_gen_z_v<T, N, CV::v[0].E, CV::v[0].B, SPEC_SHINO>(a, bm, nb, s);
   }
   if (pass == 1 || pass == 2) {
     if (v == 0) {
-      if (pass == 1) return run_gen_z_v<T, N, CV::v[0].E, CV::v[0].B, SPEC_PHILOX>(a, s);
-      return run_mid_y_v<T, N, CV::v[0].E, CV::v[0].B>(a, s);
+      if (pass == 1) return run_gen_z_v<T, N, CV::v[0].E, CV::v[0].B, SPEC_PHILOX>(a, bm, nb, s);
+      return run_mid_y_v<T, N, CV::v[0].E, CV::v[0].B>(a, bm, nb, s);
     }
     switch (v) {
       SCARL_COLV(1)
@@ -135,7 +161,7 @@ inline cudaError_t run_pass_n(int pass, int v, const GenArgs& a, cudaStream_t s)
     }
   }
   if (pass == 3) {
-    if (v == 0) return run_c2r_x_v<T, N, RV::v[0].E, RV::v[0].B>(a, s);
+    if (v == 0) return run_c2r_x_v<T, N, RV::v[0].E, RV::v[0].B>(a, bm, nb, s);
     switch (v) {
       SCARL_ROWV(1)
       SCARL_ROWV(2)
@@ -147,24 +173,6 @@ inline cudaError_t run_pass_n(int pass, int v, const GenArgs& a, cudaStream_t s)
 #undef SCARL_COLV
 #undef SCARL_ROWV
   return cudaErrorInvalidValue;
-}
-
-template <typename T>
-inline cudaError_t run_pass(int pass, int v, const GenArgs& a, cudaStream_t s) {
-  const int N = pass == 1 ? a.P[2] : (pass == 2 ? a.P[1] : a.P[0] / 2);
-  switch (N) {
-    case 4: return run_pass_n<T, 4>(pass, v, a, s);
-    case 8: return run_pass_n<T, 8>(pass, v, a, s);
-    case 16: return run_pass_n<T, 16>(pass, v, a, s);
-    case 32: return run_pass_n<T, 32>(pass, v, a, s);
-    case 64: return run_pass_n<T, 64>(pass, v, a, s);
-    case 128: return run_pass_n<T, 128>(pass, v, a, s);
-    case 256: return run_pass_n<T, 256>(pass, v, a, s);
-    case 512: return run_pass_n<T, 512>(pass, v, a, s);
-    case 1024: return run_pass_n<T, 1024>(pass, v, a, s);
-    case 2048: return run_pass_n<T, 2048>(pass, v, a, s);
-    default: return cudaErrorInvalidValue;
-  }
 }
 
 }  // namespace scarl

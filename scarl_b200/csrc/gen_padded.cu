@@ -1,17 +1,57 @@
 // gen_padded.cu -- dispatch of the padded periodic-grid generator passes
-// (kernels in gen_kernels.cuh, variants in gen_launch.cuh, instantiated in
-// gen_f32.cu / gen_f64.cu) and the FP64 spectral normalisation sum.
+// (kernels in gen_kernels.cuh, variants in gen_launch.cuh, instantiated per
+// precision and line length by gen_inst.cu) and the FP64 spectral
+// normalisation sum.
 #include "gen_launch.cuh"
 
 namespace scarl {
 
-cudaError_t run_pass_f32(int pass, int v, const GenArgs& a, cudaStream_t s);
-cudaError_t run_pass_f64(int pass, int v, const GenArgs& a, cudaStream_t s);
+// Defined and explicitly instantiated in gen_inst.cu.
+template <typename T, int N>
+cudaError_t run_pass_len(int pass, int v, const GenArgs& a, const BatchMap* bm, int* nb,
+                         cudaStream_t s);
+
+template <typename T>
+static cudaError_t run_pass_t(int pass, int v, const GenArgs& a, const BatchMap* bm, int* nb,
+                              cudaStream_t s) {
+  const int N = pass == 1 ? a.P[2] : (pass == 2 ? a.P[1] : a.P[0] / 2);
+  switch (N) {
+    case 4: return run_pass_len<T, 4>(pass, v, a, bm, nb, s);
+    case 8: return run_pass_len<T, 8>(pass, v, a, bm, nb, s);
+    case 16: return run_pass_len<T, 16>(pass, v, a, bm, nb, s);
+    case 32: return run_pass_len<T, 32>(pass, v, a, bm, nb, s);
+    case 64: return run_pass_len<T, 64>(pass, v, a, bm, nb, s);
+    case 128: return run_pass_len<T, 128>(pass, v, a, bm, nb, s);
+    case 256: return run_pass_len<T, 256>(pass, v, a, bm, nb, s);
+    case 512: return run_pass_len<T, 512>(pass, v, a, bm, nb, s);
+    case 1024: return run_pass_len<T, 1024>(pass, v, a, bm, nb, s);
+    case 2048: return run_pass_len<T, 2048>(pass, v, a, bm, nb, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static cudaError_t run_pass_dt(int dt, int pass, int v, const GenArgs& a, const BatchMap* bm,
+                               int* nb, cudaStream_t s) {
+  if (pass < 1 || pass > 3) return cudaErrorInvalidValue;
+  return dt == 8 ? run_pass_t<double>(pass, v, a, bm, nb, s)
+                 : run_pass_t<float>(pass, v, a, bm, nb, s);
+}
 
 cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a, cudaStream_t s) {
   if (pass < 1 || pass > 3) return cudaErrorInvalidValue;
-  const int v = a.var[pass - 1];
-  return dt == 8 ? run_pass_f64(pass, v, a, s) : run_pass_f32(pass, v, a, s);
+  return run_pass_dt(dt, pass, a.var[pass - 1], a, nullptr, nullptr, s);
+}
+
+cudaError_t launch_gen_pass_batch(int dt, int pass, int v, const GenArgs& rep, const BatchMap& m,
+                                  cudaStream_t s) {
+  if (m.n < 1 || m.total < 1) return cudaErrorInvalidValue;
+  return run_pass_dt(dt, pass, v, rep, &m, nullptr, s);
+}
+
+int gen_pass_blocks(int dt, int pass, int v, const GenArgs& a) {
+  int nb = 0;
+  if (run_pass_dt(dt, pass, v, a, nullptr, &nb, nullptr) != cudaSuccess) return -1;
+  return nb;
 }
 
 int gen_variant_count(int dt, int pass) {

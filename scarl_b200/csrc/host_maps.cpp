@@ -597,4 +597,44 @@ int read_input_sem(const char* folderp, char* out_folder, size_t flen, int* nSam
   return SCARL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Ensemble draws (no counterpart in the reference).  Philox4x32-10 (Salmon et
+// al., SC11) on the host: realisation r reads the block at counter
+// {r, r >> 32, 0, 2}, key {seed, seed >> 32}.
+// ---------------------------------------------------------------------------
+static void philox_host(const uint32_t ctr[4], uint32_t k0, uint32_t k1, uint32_t out[4]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    c1 = (uint32_t)p1;
+    c3 = (uint32_t)p0;
+    c0 = n0;
+    c2 = n2;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+int ensemble_draw(uint64_t seed, long long first, int n, const int* choices, int nchoices,
+                  double lmin, double lmax, int* Np, double* corrL) {
+  if (n < 0 || nchoices < 1 || !choices || !Np || !corrL || first < 0) return SCARL_EINVAL;
+  for (int i = 0; i < n; ++i) {
+    const uint64_t r = (uint64_t)first + (uint64_t)i;
+    const uint32_t ctr[4] = {(uint32_t)r, (uint32_t)(r >> 32), 0u, 2u};
+    uint32_t w[4];
+    philox_host(ctr, (uint32_t)seed, (uint32_t)(seed >> 32), w);
+    for (int d = 0; d < 3; ++d)
+      Np[3 * i + d] = choices[(int)(((uint64_t)w[d] * (uint64_t)nchoices) >> 32)];
+    const double u = (double)w[3] * 0x1p-32 + 0x1p-33;
+    corrL[3 * i] = corrL[3 * i + 1] = corrL[3 * i + 2] = lmin + (lmax - lmin) * u;
+  }
+  return SCARL_OK;
+}
+
 }  // namespace scarl

@@ -30,6 +30,8 @@ int shino_sizes(const int Np[3], const double xRange[3], const double corrL[3], 
 double axis_correlation(int corrMod, double nu, double l, double r);
 int pad_size(int policy, int corrMod, double nu, const double corrL[3], const double xStep[3],
              const int Np[3], double tol, int P[3]);
+int ensemble_draw(uint64_t seed, long long first, int n, const int* choices, int nchoices,
+                  double lmin, double lmax, int* Np, double* corrL);
 int read_config(const char* path, int* gen_meth, int* c_info, int* d_sample, int* one_file,
                 int* one_hdf_ds, char* input_file, size_t len);
 int read_extra_config(const char* path, int* found, int topo[3]);

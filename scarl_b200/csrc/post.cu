@@ -170,7 +170,20 @@ __global__ void __launch_bounds__(kSumT) k_sums(const T* __restrict__ f, int64_t
   const int64_t chunk = (xN + nb - 1) / nb;
   const int64_t lo = (int64_t)blockIdx.x * chunk, hi = (lo + chunk < xN) ? lo + chunk : xN;
   double s = 0.0, s2 = 0.0;
-  for (int64_t i = lo + threadIdx.x; i < hi; i += kSumT) {
+  constexpr int U = 8;  // independent loads in flight per thread
+  int64_t i = lo + threadIdx.x;
+  for (; i + (U - 1) * kSumT < hi; i += U * kSumT) {
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = __ldg(p + i + u * kSumT);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const double d = (double)v[u];
+      s += d;
+      s2 += d * d;
+    }
+  }
+  for (; i < hi; i += kSumT) {
     const double v = (double)p[i];
     s += v;
     s2 += v * v;

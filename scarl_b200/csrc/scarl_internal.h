@@ -74,9 +74,26 @@ struct GenArgs {
   int var[3];            // launch variant of each pass (autotuned, 0 = default)
 };
 
+// One batched launch of a pass over several realisations that share the
+// pass' line length: block b of the flat grid belongs to items[i] where
+// start[i] <= b < start[i + 1] (device arrays, n + 1 offsets).
+struct BatchMap {
+  const GenArgs* args;   // argument blocks of every realisation (device)
+  const int* items;      // realisations of this launch (device, n entries)
+  const int* start;      // block offsets (device, n + 1 entries)
+  int n;
+  int total;             // start[n], the launch's grid size
+};
+
 // Launchers (return cudaSuccess or the launch error).  dt: 4 = FP32, 8 = FP64.
 // pass: 1 = synthesis + z, 2 = y, 3 = C2R x + epilogue.
 cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a, cudaStream_t s);
+// Batched form: rep is the host copy of one member's arguments (line length
+// and spectrum mode), v the launch variant.
+cudaError_t launch_gen_pass_batch(int dt, int pass, int v, const GenArgs& rep, const BatchMap& m,
+                                  cudaStream_t s);
+// Blocks one realisation needs in a pass with launch variant v.
+int gen_pass_blocks(int dt, int pass, int v, const GenArgs& a);
 // Number of launch variants of a pass (valid ones depend on the line length).
 int gen_variant_count(int dt, int pass);
 // FP64 sum over the full periodic grid of S(k) dk^3: separable tables r*
@@ -126,5 +143,14 @@ cudaError_t launch_lag_cov(int dt, const void* f, const int L[3], int dir, doubl
                            double sd, const double* win, int nkeep, double* partial, int nparts,
                            cudaStream_t s);
 int lag_cov_parts(const int L[3], int dir);
+
+// Streamed axis covariance (cov.cu): per-block FP64 power of the centred,
+// zero-padded lines along axis dir (complex length N, padded length 2N),
+// then S(h) for h <= maxlag.  bins holds N + 1 doubles.
+int axis_power_blocks(int dt, const int L[3], int dir, int N);
+cudaError_t launch_axis_power(int dt, const void* f, const int L[3], int dir, int N, double mu,
+                              const void* tw, double* partial, int nblocks, cudaStream_t s);
+cudaError_t launch_cov_lags(const double* partial, int nblocks, int N, int maxlag,
+                            const double* tw64, double* bins, double* S, cudaStream_t s);
 
 }  // namespace scarl

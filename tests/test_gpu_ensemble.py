@@ -1,0 +1,125 @@
+"""Batched ensembles of uneven grids (one batched launch per line length and
+pass, replayed from a CUDA graph) against the per-realisation generator and
+the oracle.  Tolerances: FP64 rel-L2 <= 1e-12 against the oracle, FP32
+rel-L2 <= 1e-5; batched and single-tile launches of one variant agree
+bit for bit."""
+import numpy as np
+import pytest
+
+import scarl_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+SMALL_AXES = (16, 24, 32, 40, 48, 64)
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    s = np.max(np.abs(b))
+    return np.linalg.norm((a - b) / s) / np.linalg.norm(b / s)
+
+
+def _pads(Np, cl, cm, nu=0.5, tol=1e-3, policy=S.PAD_AUTO):
+    return [S.pad_size(policy, cm, c, (1, 1, 1), n, nu, tol) for n, c in zip(Np, cl)]
+
+
+@pytest.mark.parametrize("cm,nu", [(3, 0.5), (1, 0.5), (2, 1.5)])
+def test_ensemble_fp64_vs_oracle(ctx, oracle, cm, nu):
+    Np, cl = S.ensemble_draw(7, 0, 10, SMALL_AXES, 2.0, 8.0)
+    seeds = np.arange(100, 110, dtype=np.uint64)
+    streams = np.arange(10, dtype=np.uint32) % 3
+    out = S.gen_ensemble(ctx, Np, cl, corrMod=cm, nu=nu, seeds=seeds, streams=streams,
+                         dtype=S.F64)
+    fields = S.ensemble_fields(out, Np)
+    for i, (n, c, P) in enumerate(zip(Np, cl, _pads(Np, cl, cm, nu))):
+        ref = oracle.gen_padded(n, P, (1, 1, 1), c, cm, nu, 1, seed=int(seeds[i]),
+                                stream=int(streams[i]))
+        assert rel(fields[i], ref) < TOL64, i
+
+
+def test_ensemble_fp32_matches_single_tile_launches(ctx, oracle):
+    """Same launch variants: the batched kernels reproduce scarl_gen_padded
+    bit for bit, and both stay within the FP32 tolerance of the oracle."""
+    Np, cl = S.ensemble_draw(3, 0, 12, SMALL_AXES, 2.0, 8.0)
+    out = S.gen_ensemble(ctx, Np, cl, corrMod=3, dtype=S.F32)
+    fields = S.ensemble_fields(out, Np)
+    for i, (n, c, P) in enumerate(zip(Np, cl, _pads(Np, cl, 3))):
+        one = S.gen_padded(ctx, n, (1, 1, 1), c, 3, 0.5, pad=P, seed=i, dtype=S.F32)
+        np.testing.assert_array_equal(fields[i], one)
+        ref = oracle.gen_padded(n, P, (1, 1, 1), c, 3, 0.5, 1, seed=i)
+        assert rel(fields[i], ref) < TOL32
+
+
+def test_ensemble_graph_replay_and_reseeding(ctx):
+    Np, cl = S.ensemble_draw(11, 0, 9, SMALL_AXES, 2.0, 8.0)
+    eager = S.gen_ensemble(ctx, Np, cl, seeds=np.arange(9, dtype=np.uint64), graph=False)
+    a = S.gen_ensemble(ctx, Np, cl, seeds=np.arange(9, dtype=np.uint64))   # builds the graph
+    b = S.gen_ensemble(ctx, Np, cl, seeds=np.arange(9, dtype=np.uint64))   # replays it
+    np.testing.assert_array_equal(a, eager)
+    np.testing.assert_array_equal(b, eager)
+    c = S.gen_ensemble(ctx, Np, cl, seeds=np.arange(9, 18, dtype=np.uint64))
+    d = S.gen_ensemble(ctx, Np, cl, seeds=np.arange(9, 18, dtype=np.uint64), graph=False)
+    np.testing.assert_array_equal(c, d)
+    fa, fc = S.ensemble_fields(a, Np), S.ensemble_fields(c, Np)
+    assert all(not np.allclose(x, y) for x, y in zip(fa, fc))
+
+
+def test_ensemble_device_output_and_marginal(ctx):
+    torch = pytest.importorskip("torch")
+    Np, cl = S.ensemble_draw(5, 0, 8, SMALL_AXES, 2.0, 8.0)
+    total = int(S.ensemble_offsets(Np)[-1])
+    dev = torch.empty(total, dtype=torch.float64, device="cuda")
+    S.gen_ensemble(ctx, Np, cl, dtype=S.F64, out=dev)
+    ctx.sync()
+    host = S.gen_ensemble(ctx, Np, cl, dtype=S.F64)
+    np.testing.assert_array_equal(dev.cpu().numpy(), host)
+    logn = S.gen_ensemble(ctx, Np, cl, dtype=S.F64, margiFirst=2, avg=1.0, std_dev=0.3)
+    s2 = np.log(1.0 + 0.09)
+    np.testing.assert_allclose(logn, np.exp(host * np.sqrt(s2) - s2 / 2), rtol=1e-13)
+
+
+def test_ensemble_autotune_keeps_results_in_tolerance(oracle):
+    with S.Context(0) as c:
+        Np, cl = S.ensemble_draw(9, 0, 16, (64, 96, 128, 160), 4.0, 16.0)
+        out = S.gen_ensemble(c, Np, cl, autotune=True)
+        again = S.gen_ensemble(c, Np, cl)
+        np.testing.assert_array_equal(out, again)
+        fields = S.ensemble_fields(out, Np)
+        for i in (0, 7, 15):
+            P = _pads(Np[i:i + 1], cl[i:i + 1], 3)[0]
+            ref = oracle.gen_padded(Np[i], P, (1, 1, 1), cl[i], 3, 0.5, 1, seed=i)
+            assert rel(fields[i], ref) < TOL32
+
+
+def test_ensemble_256_uneven_realisations(ctx, oracle):
+    """The 256-realisation workload (axes in {64..256}, l in [4, 32],
+    exponential, seeds 0-255, FP32): finite, unit-variance fields, the
+    replayed graph reproduces the first run, and the smallest realisations
+    match the oracle."""
+    Np, cl = S.ensemble_draw(0, 0, 256)
+    out = S.gen_ensemble(ctx, Np, cl, corrMod=3)
+    again = S.gen_ensemble(ctx, Np, cl, corrMod=3)
+    np.testing.assert_array_equal(out, again)
+    assert np.all(np.isfinite(out))
+    fields = S.ensemble_fields(out, Np)
+    # the mean square of one correlated field scatters around the target
+    # variance 1; its mean over the ensemble is tight
+    ms = np.array([np.mean(f.astype(np.float64) ** 2) for f in fields])
+    assert abs(ms.mean() - 1.0) < 0.1
+    vol = np.prod(Np.astype(np.int64), axis=1)
+    for i in np.argsort(vol)[:2]:
+        P = _pads(Np[i:i + 1], cl[i:i + 1], 3)[0]
+        ref = oracle.gen_padded(Np[i], P, (1, 1, 1), cl[i], 3, 0.5, 1, seed=int(i))
+        assert rel(fields[i], ref) < TOL32
+
+
+def test_ensemble_errors(ctx):
+    with pytest.raises(S.ScarlError):
+        S.gen_ensemble(ctx, [[16, 16, 0]], [[2, 2, 2]])
+    with pytest.raises(S.ScarlError):
+        S.gen_ensemble(ctx, [[16, 16, 16]], [[2, -1, 2]])
+    with pytest.raises(S.ScarlError):
+        S.gen_ensemble(ctx, [[16, 16, 16]], [[2, 2, 2]], corrMod=9)

@@ -201,3 +201,19 @@ def test_pad_size_auto_is_minimal(cm, nu):
                     assert corr(cl[d], (P[d] // 2 - Np[d] + 1) * dx[d]) > tol
     full = S.pad_size(S.PAD_FULL, cm, (40, 20, 10), (1, 1, 1), (297, 277, 267))
     assert list(full) == [1024, 1024, 1024]
+
+
+def test_ensemble_draw_matches_oracle(oracle):
+    """Shapes and correlation lengths of ensemble realisations: library and
+    oracle draw the same Philox words, bit-exact."""
+    for seed, first, n in ((0, 0, 256), (12345, 1000, 64), (2 ** 40 + 3, 2 ** 33, 16)):
+        Np, cl = S.ensemble_draw(seed, first, n)
+        rNp, rcl = oracle.ensemble_draw(seed, first, n, S.ENSEMBLE_AXES, 4.0, 32.0)
+        np.testing.assert_array_equal(Np, rNp)
+        np.testing.assert_array_equal(cl, rcl)
+    Np, cl = S.ensemble_draw(0, 0, 256)
+    assert set(np.unique(Np)) <= set(S.ENSEMBLE_AXES) and len(np.unique(Np)) == 6
+    assert np.all((cl >= 4) & (cl <= 32)) and np.all(cl[:, 0] == cl[:, 2])
+    # the first realisations do not depend on how many are drawn
+    np.testing.assert_array_equal(S.ensemble_draw(0, 0, 10)[0], Np[:10])
+    np.testing.assert_array_equal(S.ensemble_draw(0, 5, 3)[0], Np[5:8])
