@@ -265,6 +265,70 @@ def bench_ensemble(S, ctx, stream, steps, warmup):
             "host_output_equals_device_output": same}
 
 
+def bench_large_field(S, ctx, stream, steps):
+    """2048 x 2048 x 1024 FP32 field, Gaussian l = (64, 64, 32), Gaussian
+    marginal (variance 1), 4 x 4 x 1 tiles with a 128-point overlap, AUTO
+    padding; then the streamed FP64 mean, variance and axis covariance up to
+    lag 256 of the finished field."""
+    import torch
+    ctx.set_stream(stream.cuda_stream)
+    s = S.make_sample((0, 0, 0), (2047, 2047, 1023), (64, 64, 32), (127 / 64, 127 / 64, 0),
+                      (65, 65, 33), corrMod=1, margiFirst=1, avg=0.0, std_dev=1.0, seedBase=0)
+    lay = S.sample_layout(s, 1, 16, (4, 4, 1))
+    L = [int(v) for v in lay["L"]]
+    n = L[0] * L[1] * L[2]
+    field = torch.empty(n, dtype=torch.float32, device="cuda")
+    P = [int(v) for v in S.pad_size(S.PAD_AUTO, 1, (64, 64, 32), lay["xStep"], lay["Np"], 0.5, PAD_TOL)]
+
+    def gen():
+        S.generate_sample(ctx, s, dtype=S.F32, nb_procs=16, topo=(4, 4, 1), pad_policy=S.PAD_AUTO,
+                          pad_tol=PAD_TOL, autotune=True, out=field)
+
+    gen()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        gen()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_gen = e0.elapsed_time(e1) / steps
+    S.axis_cov(ctx, field, L, 256)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        mean, var, cov = S.axis_cov(ctx, field, L, 256)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_stat = e0.elapsed_time(e1) / steps
+    ctx.profile(True)
+    ctx.profile_reset()
+    S.axis_cov(ctx, field, L, 256)
+    torch.cuda.synchronize()
+    st = ctx.profile_stats()
+    ctx.profile(False)
+    del field
+    torch.cuda.empty_cache()
+    kern = {}
+    for k in ("k_sums", "k_axis_power", "k_cov_lags"):
+        if k in st:
+            tot, cnt = st[k]
+            kern[k] = {"launches": cnt, "avg_ms": round(tot / cnt, 4)}
+            if k != "k_cov_lags":
+                kern[k]["gbs"] = round(n * 4 / (tot / cnt * 1e-3) / 1e9, 1)
+    return {"workload": "2048x2048x1024 FP32, Gaussian l=(64,64,32), Gaussian marginal var 1, "
+                        "4x4x1 tiles, overlap 128, AUTO padding; streamed FP64 mean, variance and "
+                        "axis covariance up to lag 256",
+            "points": n, "padded_grid": P, "value": round(n / (ms_gen * 1e-3) / 1e6, 2),
+            "unit": "Mpoints/s", "ms_generate": round(ms_gen, 3),
+            "ms_statistics": round(ms_stat, 3),
+            "statistics_field_reads_gbs": round(4 * n * 4 / (ms_stat * 1e-3) / 1e9, 1),
+            "statistics_kernels": kern, "mean": mean, "var": var,
+            "cov_at_l": [float(cov[0, 64]), float(cov[1, 64]), float(cov[2, 32])],
+            "target_at_l": float(__import__("math").exp(-__import__("math").pi))}
+
+
 def config_of(lay, P):
     return {"workload": "512^3 deck -> 513^3 field, exponential, l=(40,20,10), lognormal mean 1 "
                         "CV 0.3, 2x2x2 tiles, overlap 2l, padded periodic C2R FP32",
@@ -282,6 +346,7 @@ def main():
     ap.add_argument("--impl", default="scarl", choices=["scarl", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-large-field", action="store_true")
     ap.add_argument("--profile-tile", action="store_true",
                     help="generate one field once (no timing) for profiler captures; launch "
                          "variants come from SCARL_TUNE_CACHE when set")
@@ -465,6 +530,10 @@ def main():
     if not args.no_ensemble:
         ens = bench_ensemble(S, ctx, stream, max(3, min(args.steps, 20)), args.warmup)
 
+    large = None
+    if not args.no_large_field:
+        large = bench_large_field(S, ctx, stream, 3)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = cpu_sample(lay, P_auto, 1, 0)
@@ -479,7 +548,7 @@ def main():
                 "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "roofline": roof,
                 "kernels": kern, "launch_variants": tuned, "plain_path": plain,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-                "ensemble": ens}
+                "ensemble": ens, "large_field": large}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

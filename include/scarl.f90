@@ -45,6 +45,7 @@ module scarl_gpu
     integer(c_int32_t) :: stream = 0
     integer(c_int) :: autotune = 0
     type(c_ptr) :: phiK = c_null_ptr
+    integer(c_int) :: gen_meth = SCARL_FFT
   end type scarl_gen_opts
 
   interface
@@ -76,6 +77,18 @@ module scarl_gpu
       integer(c_int), intent(in) :: Np(3)
       real(c_double), intent(in) :: xRange(3), corrL(3)
       integer(c_int), value :: corrMod, seed, rank
+      type(c_ptr), value :: phiK, gammaK
+    end function
+
+    ! gen_Std_Gauss_FFT_MPI (SRC_F/fftw_ScaRL.f90:424) on one GPU, Np = L
+    integer(c_int) function scarl_gen_std_gauss_fft_mpi(ctx, data_real_3D, xRange, corrL, &
+        corrMod, seed, rank, L, Np, phiK, gammaK) bind(C, name="scarl_gen_std_gauss_fft_mpi")
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_double), intent(inout) :: data_real_3D(*)
+      real(c_double), intent(in) :: xRange(3), corrL(3)
+      integer(c_int), value :: corrMod, seed, rank
+      integer(c_int), intent(in) :: L(3), Np(3)
       type(c_ptr), value :: phiK, gammaK
     end function
 

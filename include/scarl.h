@@ -114,6 +114,10 @@ typedef struct {
   uint32_t stream;        /* realisation stream (ensembles), 0 by default */
   int autotune;           /* 1 = autotune each new grid shape on first use */
   const double* phiK;     /* DCT generator: injected phases, nb x (Np/2)^3 */
+  int gen_meth;           /* SCARL_FFT (0 = default): overlapping tiles blended by the
+                             partition of unity; SCARL_FFT_MPI: the whole re-fitted grid as
+                             one global transform (DCT: spectrum over every kz, phases
+                             L0/2 x L1/2 x L2) */
 } scarl_gen_opts;
 
 /* ------------------------------------------------------------------ */
@@ -209,6 +213,16 @@ int scarl_read_input_sem(const char* folder, char* output_folder, size_t folder_
 int scarl_gen_std_gauss_fft(scarl_ctx* ctx, double* data_real_3D, const int Np[3],
                             const double xRange[3], const double corrL[3], int corrMod,
                             int seed, int rank, const double* phiK, const double* gammaK);
+
+/* Drop-in for gen_Std_Gauss_FFT_MPI (SRC_F/fftw_ScaRL.f90:424-583) on one GPU:
+ * the global DCT-III over the L grid of the spectrum on (L0/2, L1/2, L2), Gaussian
+ * model, FP64.  The MPI communicator has no counterpart: the whole transform runs
+ * on the GPU, so Np must equal L (one rank).  phiK / gammaK: injected
+ * (L0/2)(L1/2)L2 phases / amplitudes or NULL (Philox uniforms / 1). */
+int scarl_gen_std_gauss_fft_mpi(scarl_ctx* ctx, double* data_real_3D, const double xRange[3],
+                                const double corrL[3], int corrMod, int seed, int rank,
+                                const int L[3], const int Np[3], const double* phiK,
+                                const double* gammaK);
 
 /* Drop-in for gen_std_gauss_Shino_FFT + build_Sk_mtx (SRC_F/fftw_ScaRL.f90:
  * 157-255, SRC_F/spectra_ScaRL.f90:10-142), FP64: Park-Miller phases from

@@ -64,6 +64,7 @@ def _declare(L):
     L.so_c2c_3d.argtypes = [_d, _i, C.c_int]
     L.so_c2r_3d_crop.argtypes = [_d, _i, _i, _d]
     L.so_gen_std_gauss_fft.argtypes = [_d, _i, _d, _d, _d, _d]
+    L.so_gen_std_gauss_fft_mpi.argtypes = [_d, _i, _d, _d, _d, _d]
     L.so_padded_size_literal.restype = C.c_int
     L.so_padded_size_literal.argtypes = [C.c_int]
     L.so_shino_sizes.restype = C.c_int
@@ -308,6 +309,15 @@ def gen_std_gauss_fft(Np, xRange, corrL, phiK, gammaK=None):
     g = None if gammaK is None else np.asfortranarray(gammaK, dtype=np.float64)
     out = np.empty(tuple(int(v) for v in Np), order="F")
     lib().so_gen_std_gauss_fft(_dp(out), pn, px, pc, _dp(ph), None if g is None else _dp(g))
+    return out
+
+
+def gen_std_gauss_fft_mpi(L, xRange, corrL, phiK, gammaK=None):
+    n, pn = _ia(L); x, px = _da(xRange); c, pc = _da(corrL)
+    ph = np.asfortranarray(phiK, dtype=np.float64)
+    g = None if gammaK is None else np.asfortranarray(gammaK, dtype=np.float64)
+    out = np.empty(tuple(int(v) for v in L), order="F")
+    lib().so_gen_std_gauss_fft_mpi(_dp(out), pn, px, pc, _dp(ph), None if g is None else _dp(g))
     return out
 
 

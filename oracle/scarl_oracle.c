@@ -789,12 +789,13 @@ void so_c2r_3d_crop(const double* Hd, const int P[3], const int Nout[3], double*
  * The region outside the octant is uninitialised in the reference
  * (:317, :370); it is zero here.  gamma is the injected amplitude (the
  * reference overwrites it with 1, :367): gammaK == NULL means 1. */
-void so_gen_std_gauss_fft(double* out, const int Np[3], const double xRange[3],
-                          const double corrL[3], const double* phiK, const double* gammaK) {
+static void so_dct_generator(double* out, const int Np[3], const double xRange[3],
+                             const double corrL[3], const double* phiK, const double* gammaK,
+                             int full_z) {
   int K[3];
   double dk[3];
   for (int d = 0; d < 3; ++d) {
-    K[d] = Np[d] / 2;
+    K[d] = (full_z && d == 2) ? Np[d] : Np[d] / 2;
     double delta_x = xRange[d] / (double)(Np[d] - 1);
     double k_max = 1.0 / delta_x;
     dk[d] = k_max / (double)(Np[d] - 1);
@@ -816,6 +817,19 @@ void so_gen_std_gauss_fft(double* out, const int Np[3], const double xRange[3],
       }
   so_dct3_3d(Sk, out, Np);
   free(Sk);
+}
+
+void so_gen_std_gauss_fft(double* out, const int Np[3], const double xRange[3],
+                          const double corrL[3], const double* phiK, const double* gammaK) {
+  so_dct_generator(out, Np, xRange, corrL, phiK, gammaK, 0);
+}
+
+/* gen_Std_Gauss_FFT_MPI (SRC_F/fftw_ScaRL.f90:424-583) for one rank: the same
+ * spectrum and DCT-III with the spectrum over every kz (:469-476); phases
+ * (L0/2)(L1/2)L2 in x-fastest order. */
+void so_gen_std_gauss_fft_mpi(double* out, const int L[3], const double xRange[3],
+                              const double corrL[3], const double* phiK, const double* gammaK) {
+  so_dct_generator(out, L, xRange, corrL, phiK, gammaK, 1);
 }
 
 /* SRC_F/fftw_ScaRL.f90:194: sz_c = 2**ceiling(log(dble(2*Np))/log(2d0)). */

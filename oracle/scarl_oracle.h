@@ -86,6 +86,8 @@ void so_c2r_3d_crop(const double* H, const int P[3], const int Nout[3], double* 
 /* ---------------- generators ---------------- */
 void so_gen_std_gauss_fft(double* out, const int Np[3], const double xRange[3],
                           const double corrL[3], const double* phiK, const double* gammaK);
+void so_gen_std_gauss_fft_mpi(double* out, const int L[3], const double xRange[3],
+                              const double corrL[3], const double* phiK, const double* gammaK);
 int so_padded_size_literal(int Np);
 int so_shino_sizes(const int Np[3], const double xRange[3], const double corrL[3],
                    int sz_c[3], int sz_Sk[3], double delta_k[3]);

@@ -45,7 +45,8 @@ class GenOpts(C.Structure):
                 ("topo_shape", C.c_int * 3), ("pad", C.c_int * 3),
                 ("pad_policy", C.c_int), ("pad_tol", C.c_double),
                 ("no_spectral_normalisation", C.c_int), ("normalize_field", C.c_int),
-                ("stream", C.c_uint32), ("autotune", C.c_int), ("phiK", C.POINTER(C.c_double))]
+                ("stream", C.c_uint32), ("autotune", C.c_int), ("phiK", C.POINTER(C.c_double)),
+                ("gen_meth", C.c_int)]
 
 
 _vp = C.c_void_p
@@ -89,6 +90,8 @@ SIGNATURES = {
                                        C.POINTER(Sample), C.c_int]),
     "scarl_gen_std_gauss_fft": (C.c_int, [_vp, _vp, _ip, _dp, _dp, C.c_int, C.c_int, C.c_int,
                                           _vp, _vp]),
+    "scarl_gen_std_gauss_fft_mpi": (C.c_int, [_vp, _vp, _dp, _dp, C.c_int, C.c_int, C.c_int, _ip,
+                                              _ip, _vp, _vp]),
     "scarl_gen_std_gauss_shino_fft": (C.c_int, [_vp, _vp, _ip, _dp, _dp, _ip, C.c_int,
                                                 C.c_int, C.c_int]),
     "scarl_gen_padded": (C.c_int, [_vp, _vp, C.c_int, _ip, _ip, _dp, _dp, C.c_int, C.c_double,

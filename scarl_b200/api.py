@@ -258,6 +258,22 @@ def gen_std_gauss_FFT(ctx, Np, xRange, corrL, corrMod=1, seed=0, rank=0, phiK=No
     return out
 
 
+def gen_std_gauss_FFT_MPI(ctx, xRange, corrL, corrMod=1, seed=0, rank=0, L=None, Np=None,
+                          phiK=None, gammaK=None, out=None):
+    """Drop-in for gen_Std_Gauss_FFT_MPI (SRC_F/fftw_ScaRL.f90:424-583) on one
+    GPU: global DCT-III over L (Np == L), FP64."""
+    L = tuple(int(v) for v in L)
+    Np = L if Np is None else tuple(int(v) for v in Np)
+    out = _alloc_out(out, L, F64)
+    ph = None if phiK is None else np.asfortranarray(phiK, dtype=np.float64)
+    ga = None if gammaK is None else np.asfortranarray(gammaK, dtype=np.float64)
+    _check(lib().scarl_gen_std_gauss_fft_mpi(ctx.handle, _ptr(out), _d3(xRange), _d3(corrL),
+                                             corrMod, seed, rank, _i3(L), _i3(Np),
+                                             None if ph is None else _ptr(ph),
+                                             None if ga is None else _ptr(ga)), ctx)
+    return out
+
+
 def gen_std_gauss_Shino_FFT(ctx, Np, xRange, corrL, pointsPerCorrL=(5, 5, 5), corrMod=1, seed=0,
                             rank=0, out=None):
     """Drop-in for gen_std_gauss_Shino_FFT (SRC_F/fftw_ScaRL.f90:157-255), FP64."""
@@ -354,9 +370,11 @@ def axis_correlation(corrMod, l, r, nu=0.5):
 
 def generate_sample(ctx, sample, generator=GEN_PADDED, dtype=F32, nb_procs=1, topo=None,
                     pad=None, pad_policy=PAD_FULL, pad_tol=1e-3, normalise_spectrum=True,
-                    normalize_field=False, stream=0, phiK=None, autotune=False, out=None):
-    """One deck sample end to end (layout, tiles, PoU blend, marginal)."""
-    lay = sample_layout(sample, 1, nb_procs, topo)
+                    normalize_field=False, stream=0, phiK=None, autotune=False, out=None,
+                    gen_meth=1):
+    """One deck sample end to end (layout, tiles, PoU blend, marginal).
+    gen_meth 2 (FFT_MPI): the whole re-fitted grid as one global transform."""
+    lay = sample_layout(sample, gen_meth, nb_procs, topo)
     out = _alloc_out(out, tuple(int(v) for v in lay["L"]), dtype)
     o = GenOpts()
     o.generator, o.dtype, o.nb_procs = generator, dtype, nb_procs
@@ -369,6 +387,7 @@ def generate_sample(ctx, sample, generator=GEN_PADDED, dtype=F32, nb_procs=1, to
     o.normalize_field = int(bool(normalize_field))
     o.stream = int(stream)
     o.autotune = int(bool(autotune))
+    o.gen_meth = int(gen_meth)
     keep = None
     if phiK is not None:
         keep = np.ascontiguousarray(phiK, dtype=np.float64)

@@ -911,16 +911,18 @@ int dct_table(scarl_ctx* ctx, int N, const double** out) {
 }
 
 // gen_std_gauss_FFT on the device into dev_out (Np doubles).
+// full_z: the spectrum spans every kz (gen_Std_Gauss_FFT_MPI,
+// SRC_F/fftw_ScaRL.f90:469-476), else the (Np/2)^3 octant.
 int dct_tile(scarl_ctx* ctx, double* dev_out, const int Np[3], const double xRange[3],
              const double corrL[3], const double* phi_dev, const double* gamma_dev,
-             uint32_t key) {
+             uint32_t key, bool full_z = false) {
   DctArgs a;
   std::memset(&a, 0, sizeof a);
   size_t ktot = 1, t1n, t2n;
   std::vector<double> ex;
   for (int d = 0; d < 3; ++d) {
     a.Np[d] = Np[d];
-    a.K[d] = Np[d] / 2;
+    a.K[d] = (full_z && d == 2) ? Np[d] : Np[d] / 2;
     a.corrL[d] = corrL[d];
     ktot *= (size_t)a.K[d];
   }
@@ -1248,6 +1250,31 @@ int scarl_gen_std_gauss_fft(scarl_ctx* ctx, double* data, const int Np[3], const
   return finish_out(ctx, data, dev, n * 8, host);
 }
 
+int scarl_gen_std_gauss_fft_mpi(scarl_ctx* ctx, double* data, const double xRange[3],
+                                const double corrL[3], int corrMod, int seed, int rank,
+                                const int L[3], const int Np[3], const double* phiK,
+                                const double* gammaK) {
+  RC(begin(ctx));
+  if (!data || !xRange || !corrL || !L || !Np) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (corrMod != SCARL_CM_GAUSSIAN) return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
+  for (int d = 0; d < 3; ++d) {
+    if (L[d] < 2) return fail(ctx, SCARL_EINVAL, "L must be >= 2");
+    if (Np[d] != L[d])
+      return fail(ctx, SCARL_EUNSUPPORTED, "the global transform runs on one GPU: Np must equal L (one rank)");
+  }
+  const size_t n = (size_t)L[0] * L[1] * L[2];
+  const size_t nk = (size_t)(L[0] / 2) * (L[1] / 2) * L[2];
+  void* dev;
+  bool host;
+  RC(out_dev(ctx, data, n * 8, &dev, &host));
+  const void *phi = nullptr, *gam = nullptr;
+  RC(in_dev(ctx, ctx->stage_in, phiK, nk * 8, &phi));
+  RC(in_dev(ctx, ctx->stage_in2, gammaK, nk * 8, &gam));
+  RC(dct_tile(ctx, (double*)dev, L, xRange, corrL, (const double*)phi, (const double*)gam,
+              (uint32_t)((uint32_t)seed + (uint32_t)rank), true));
+  return finish_out(ctx, data, dev, n * 8, host);
+}
+
 int scarl_gen_std_gauss_shino_fft(scarl_ctx* ctx, double* data, const int Np[3],
                                   const double xRange[3], const double corrL[3],
                                   const int ppcl[3], int corrMod, int seed, int rank) {
@@ -1407,15 +1434,29 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   if (dt != SCARL_F32 && dt != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
   if (gen != SCARL_GEN_PADDED && dt != SCARL_F64)
     return fail(ctx, SCARL_EUNSUPPORTED, "the reference generators (DCT, Shino) run in FP64 only");
+  const int gm = o.gen_meth ? o.gen_meth : SCARL_FFT;
+  if (gm != SCARL_FFT && gm != SCARL_FFT_MPI) return fail(ctx, SCARL_EINVAL, "ERROR! Generation Method not implemented");
+  if (gm == SCARL_FFT_MPI && gen == SCARL_GEN_SHINO)
+    return fail(ctx, SCARL_EUNSUPPORTED, "the Shino generator has no global (FFT_MPI) form");
   char msg[256];
-  if (verify_inputs(s, SCARL_FFT, msg, sizeof msg) != SCARL_OK) return fail(ctx, SCARL_EINVAL, msg);
+  if (verify_inputs(s, gm, msg, sizeof msg) != SCARL_OK) return fail(ctx, SCARL_EINVAL, msg);
   if (gen != SCARL_GEN_PADDED && s->corrMod != SCARL_CM_GAUSSIAN)
     return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
   const int nb_procs = o.nb_procs > 0 ? o.nb_procs : 1;
   const bool topo_given = o.topo_shape[0] > 0 && o.topo_shape[1] > 0 && o.topo_shape[2] > 0;
   scarl_layout lay;
-  if (sample_layout(s, SCARL_FFT, nb_procs, topo_given ? o.topo_shape : nullptr, &lay) != SCARL_OK)
+  if (sample_layout(s, gm, nb_procs, topo_given ? o.topo_shape : nullptr, &lay) != SCARL_OK)
     return fail(ctx, SCARL_EINVAL, "ERROR! procs grid dimensions do not agree with the total number of procs");
+  if (gm == SCARL_FFT_MPI) {
+    // the slabs of the FFTW-MPI layout form one global transform on the GPU:
+    // a single tile of the re-fitted grid, no partition of unity
+    for (int d = 0; d < 3; ++d) {
+      lay.Np[d] = lay.L[d];
+      lay.Np_ovlp[d] = 0;
+      lay.topo_shape[d] = 1;
+    }
+    lay.nb_tiles = 1;
+  }
   for (int d = 0; d < 3; ++d)
     if (lay.Np_ovlp[d] < 0) return fail(ctx, SCARL_EUNSUPPORTED, "negative overlap (discontinuous mesh) is not supported");
   if (lay.nb_tiles > 4096) return fail(ctx, SCARL_EINVAL, "too many tiles");
@@ -1445,9 +1486,10 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   epi.marginal = o.normalize_field ? 0 : s->margiFirst;
   epi.ms = ms;
   epi.mmu = mmu;
-  epi.apply_pou = 1;
+  epi.apply_pou = gm == SCARL_FFT ? 1 : 0;
   const size_t ntile = (size_t)lay.Np[0] * lay.Np[1] * lay.Np[2];
-  const size_t nk = (size_t)(lay.Np[0] / 2) * (lay.Np[1] / 2) * (lay.Np[2] / 2);
+  const size_t nk = (size_t)(lay.Np[0] / 2) * (lay.Np[1] / 2) *
+                    (gm == SCARL_FFT_MPI ? lay.Np[2] : lay.Np[2] / 2);
   PaddedPlan* pl = nullptr;
   int P[3];
   if (gen == SCARL_GEN_PADDED) {
@@ -1503,7 +1545,8 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
       RC(run_passes(ctx, 8, a));
     } else {
       const double* phi = phi_all ? (const double*)phi_all + nk * r : nullptr;
-      RC(dct_tile(ctx, (double*)ctx->tile.p, lay.Np, t.xRange, s->corrL, phi, nullptr, (uint32_t)seedStart));
+      RC(dct_tile(ctx, (double*)ctx->tile.p, lay.Np, t.xRange, s->corrL, phi, nullptr, (uint32_t)seedStart,
+                  gm == SCARL_FFT_MPI));
       Prof p(ctx, "k_blend_tile");
       CK(launch_blend_tile(8, ctx->tile.p, lay.Np, e, ctx->stream));
     }

@@ -24,13 +24,23 @@ namespace scarl {
 
 namespace {
 
-constexpr int kCovE = 16;
-
-template <int N> __host__ __device__ constexpr int cov_E() { return N < kCovE ? N : kCovE; }
-// lines per block: ROW (x lines, lanes along a line) and column layouts
-template <int N, bool ROW> __host__ __device__ constexpr int cov_B() {
-  return ROW ? ((512 / (N / cov_E<N>())) < 1 ? 1 : ((512 / (N / cov_E<N>())) > 32 ? 32 : 512 / (N / cov_E<N>())))
-             : ((1024 / (N / cov_E<N>())) > 16 ? 16 : 1024 / (N / cov_E<N>()));
+// values per thread: 16 complex in FP32, 8 in FP64
+template <typename T, int N> __host__ __device__ constexpr int cov_E() {
+  return N < (sizeof(T) == 4 ? 16 : 8) ? N : (sizeof(T) == 4 ? 16 : 8);
+}
+// lines per block, for 512-thread blocks at most: ROW (x lines, lanes along
+// a line) up to 32 lines, column layouts (lanes across lines) up to 16
+template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_B() {
+  constexpr int tpl = N / cov_E<T, N>();
+  constexpr int cap = ROW ? 32 : 16;
+  return (512 / tpl) < 1 ? 1 : ((512 / tpl) > cap ? cap : 512 / tpl);
+}
+template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_threads() {
+  return cov_B<T, N, ROW>() * (N / cov_E<T, N>());
+}
+// resident blocks asked of the compiler: 1024 threads per SM, at most 32 blocks
+template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_minb() {
+  return (1024 / cov_threads<T, N, ROW>()) > 32 ? 32 : 1024 / cov_threads<T, N, ROW>();
 }
 
 struct CovGeom {
@@ -46,11 +56,11 @@ struct CovGeom {
 };
 
 template <typename T, int N, bool ROW>
-__global__ void __launch_bounds__(cov_B<N, ROW>() * (N / cov_E<N>()))
+__global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>())
     k_axis_power(const CovGeom g) {
   using C = cplx_t<T>;
-  constexpr int E = cov_E<N>();
-  constexpr int B = cov_B<N, ROW>();
+  constexpr int E = cov_E<T, N>();
+  constexpr int B = cov_B<T, N, ROW>();
   constexpr int TPL = N / E;
   constexpr int NT = B * TPL;
   constexpr int QB = (N + NT) / NT;  // bins per thread (bins 0..N)
@@ -66,33 +76,24 @@ __global__ void __launch_bounds__(cov_B<N, ROW>() * (N / cov_E<N>()))
 #pragma unroll
   for (int q = 0; q < QB; ++q) acc[q] = 0.0;
   const int64_t ngroups = (g.nlines + B - 1) / B;
+  const T mu = (T)g.mu;
   for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     const int64_t l = grp * B + b;
     const bool valid = l < g.nlines;
     const int64_t base = valid ? (l % g.na) * g.sa + (l / g.na) * g.sb : 0;
     auto val = [&](int i) -> T {
       if (!valid || i >= g.n) return T(0);
-      return (T)((double)__ldg(f + base + (int64_t)i * g.st) - g.mu);
+      return __ldg(f + base + (int64_t)i * g.st) - mu;
     };
     auto load = each_load<C, N, E>([&](int k) -> C { return mk(val(2 * k), val(2 * k + 1)); });
     constexpr int RL = last_radix<N, E>();
-    C z[E];
+    // outputs go straight to shared memory (line b at b * N), after every
+    // thread has left the transform's shared-memory reads
     auto store = [&](int j, const C* o) {
-      const int q = (j - t) / TPL;
 #pragma unroll
-      for (int r = 0; r < RL; ++r) z[q * RL + r] = o[r];
+      for (int r = 0; r < RL; ++r) sm[b * N + j + r * (N / RL)] = o[r];
     };
-    line_ifft<C, N, E, O, B, LS>(sm, b, t, tw, 2, load, store);
-    __syncthreads();  // every thread has left the transform's shared-memory stages
-    {
-      constexpr int NBL = E / RL;
-#pragma unroll
-      for (int q = 0; q < NBL; ++q) {
-        const int j = t + TPL * q;
-#pragma unroll
-        for (int r = 0; r < RL; ++r) sm[b * N + j + r * (N / RL)] = z[q * RL + r];
-      }
-    }
+    line_ifft<C, N, E, O, B, LS, true>(sm, b, t, tw, 2, load, store);
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < QB; ++q) {
@@ -121,8 +122,8 @@ __global__ void __launch_bounds__(cov_B<N, ROW>() * (N / cov_E<N>()))
 }
 
 template <typename T, int N, bool ROW> size_t cov_smem() {
-  constexpr int E = cov_E<N>();
-  constexpr int B = cov_B<N, ROW>();
+  constexpr int E = cov_E<T, N>();
+  constexpr int B = cov_B<T, N, ROW>();
   const size_t fft = (size_t)B * line_slots<N, E>() * sizeof(cplx_t<T>);
   const size_t pw = (size_t)B * N * sizeof(cplx_t<T>);
   return fft > pw ? fft : pw;
@@ -132,7 +133,7 @@ template <typename T, int N, bool ROW>
 cudaError_t run_power(CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
   auto kern = k_axis_power<T, N, ROW>;
   const size_t smem = cov_smem<T, N, ROW>();
-  const int threads = cov_B<N, ROW>() * (N / cov_E<N>());
+  const int threads = cov_threads<T, N, ROW>();
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -143,7 +144,7 @@ cudaError_t run_power(CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
   int sms = 148;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t ngroups = (g.nlines + cov_B<N, ROW>() - 1) / cov_B<N, ROW>();
+  const int64_t ngroups = (g.nlines + cov_B<T, N, ROW>() - 1) / cov_B<T, N, ROW>();
   const int nb = (int)std::max<int64_t>(1, std::min<int64_t>(ngroups, (int64_t)std::max(per_sm, 1) * sms));
   if (blocks && want_blocks < 0) {  // query only
     *blocks = nb;

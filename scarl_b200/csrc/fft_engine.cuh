@@ -129,8 +129,10 @@ __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, i
 // takes the last stage's RL outputs v[r] = y[j + r N/RL] together, so a
 // caller can issue all its memory reads for them before its writes.  sm holds
 // B lines laid out by O with skew SK = R1 (line stride LS for LineFast).  All
-// threads of the block must call.
-template <typename C, int N, int E, SmemOrder O, int B, int LS, class Load, class Store>
+// threads of the block must call.  With SYNC_STORE every thread has finished
+// its shared-memory reads before the first store, so store may write sm.
+template <typename C, int N, int E, SmemOrder O, int B, int LS, bool SYNC_STORE = false,
+          class Load, class Store>
 __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, const C* __restrict__ tw,
                                           int twmul, Load&& load, Store&& store) {
   using P = StagePlan<N, E>;
@@ -179,6 +181,7 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
 #pragma unroll
       for (int r = 0; r < RL; ++r) v[q * RL + r] = sm[sidx<O, B, LS, SK>(j + r * (N / RL), b)];
     }
+    if constexpr (SYNC_STORE) __syncthreads();
 #pragma unroll
     for (int q = 0; q < NBL; ++q) {
       const int j = t + TPL * q;

@@ -315,3 +315,50 @@ def test_generate_sample_auto_padding_vs_oracle(ctx, oracle, cm, nu):
     ref, _ = oracle.generate_sample(3, *args, cm, nu, 2, 1.0, 0.3, 9, 8, None, pad=P)
     out, _ = S.generate_sample(ctx, s, dtype=S.F64, nb_procs=8, pad_policy=S.PAD_AUTO)
     assert rel(out, ref) < TOL64
+
+
+# ---------------------------------------------------------------------------
+# global (FFT_MPI) path: one transform over the whole re-fitted grid
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("L", [(16, 12, 10), (33, 20, 17), (64, 48, 40)])
+def test_gen_std_gauss_fft_mpi_vs_oracle(ctx, oracle, L):
+    rng = np.random.default_rng(sum(L))
+    phi = rng.random((L[0] // 2, L[1] // 2, L[2]))
+    gam = rng.random((L[0] // 2, L[1] // 2, L[2]))
+    xr = tuple((n - 1) * 0.5 for n in L)
+    ref = oracle.gen_std_gauss_fft_mpi(L, xr, (3, 2, 4), phi, gam)
+    out = S.gen_std_gauss_FFT_MPI(ctx, xr, (3, 2, 4), 1, 5, 0, L=L, phiK=phi, gammaK=gam)
+    assert rel(out, ref) < TOL64
+    with pytest.raises(S.ScarlError) as e:
+        S.gen_std_gauss_FFT_MPI(ctx, xr, (3, 2, 4), 1, 5, 0, L=L, Np=(L[0], L[1], L[2] // 2))
+    assert e.value.code == 5
+
+
+def test_generate_sample_fft_mpi_global(ctx, oracle):
+    """gen_meth = FFT_MPI: the slabs of 3 ranks re-fit the grid (L2 a multiple
+    of 3); the GPU generates it as one global DCT field with the marginal."""
+    s = S.make_sample((0, 0, 0), (30, 20, 25), (4, 3, 5), (1, 1, 1), (5, 4, 6), corrMod=1,
+                      margiFirst=1, avg=2.0, std_dev=0.5)
+    lay = S.sample_layout(s, 2, 3)
+    L = [int(v) for v in lay["L"]]
+    assert L[2] % 3 == 0 and list(lay["Np_ovlp"]) == [0, 0, 0]
+    rng = np.random.default_rng(2)
+    phi = rng.random((L[0] // 2, L[1] // 2, L[2]))
+    out, glay = S.generate_sample(ctx, s, generator=S.GEN_DCT, dtype=S.F64, nb_procs=3,
+                                  gen_meth=2, phiK=phi.reshape(-1, order="F"))
+    assert list(glay["L"]) == L
+    xr = [(n - 1) * float(dx) for n, dx in zip(L, lay["xStep"])]
+    base = oracle.gen_std_gauss_fft_mpi(L, xr, (4, 3, 5), phi)
+    # the reference's DCT field is unnormalised, so the Gaussian marginal
+    # (x * std + avg) is the one that stays finite
+    assert rel(out, base * 0.5 + 2.0) < TOL64
+    # the padded method over the global grid: one tile, no blend
+    s.margiFirst = 2
+    pad, _ = S.generate_sample(ctx, s, dtype=S.F64, nb_procs=3, gen_meth=2, pad_policy=S.PAD_AUTO)
+    s.margiFirst = 1
+    s.avg, s.std_dev = 0.0, 1.0
+    std, _ = S.generate_sample(ctx, s, dtype=S.F64, nb_procs=3, gen_meth=2, pad_policy=S.PAD_AUTO)
+    P = S.pad_size(S.PAD_AUTO, 1, (4, 3, 5), lay["xStep"], L)
+    ref2 = oracle.gen_padded(L, P, lay["xStep"], (4, 3, 5), 1, 0.5, 1, seed=1)
+    assert rel(std, ref2) < TOL64
+    assert np.all(pad > 0)
