@@ -188,19 +188,22 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def bench_ensemble(S, ctx, stream, steps, warmup):
+def bench_ensemble(S, ctx, stream, steps, warmup, rank=0, dist=None):
     """The 256-realisation ensemble of uneven grids: axes from {64, ..., 256},
     isotropic l in [4, 32], exponential, seeds 0-255, FP32, AUTO padding.
     Batched launches replayed from a CUDA graph against the same realisations
     generated one scarl_gen_padded call at a time (same padded grids)."""
     import numpy as np
     import torch
+    from scarl_b200 import replicas as R
     ctx.set_stream(stream.cuda_stream)
-    Np, cl = S.ensemble_draw(0, 0, 256)
+    # rank k generates realisations 256k .. 256k + 255 (weak scaling)
+    first = 256 * rank
+    Np, cl = S.ensemble_draw(0, first, 256)
     off = S.ensemble_offsets(Np)
     total = int(off[-1])
     out = torch.empty(total, dtype=torch.float32, device="cuda")
-    seeds = np.arange(256, dtype=np.uint64)
+    seeds = R.realisation_seeds(first, first + 256)
     P = [[int(v) for v in S.pad_size(S.PAD_AUTO, 3, c, (1, 1, 1), n, 0.5, PAD_TOL)]
          for n, c in zip(Np, cl)]
 
@@ -209,20 +212,22 @@ def bench_ensemble(S, ctx, stream, steps, warmup):
 
     def single():
         for i in range(256):
-            S.gen_padded(ctx, Np[i], (1, 1, 1), cl[i], 3, 0.5, pad=P[i], seed=i,
+            S.gen_padded(ctx, Np[i], (1, 1, 1), cl[i], 3, 0.5, pad=P[i], seed=int(seeds[i]),
                          out=out[int(off[i]):int(off[i + 1])])
 
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
     def timed(fn, k):
+        if dist is not None:
+            dist.barrier()
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(k):
             fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / k
+        return R.max_over_ranks(e0.elapsed_time(e1) / k, dist, "cuda")
 
     for _ in range(warmup):
         batched()
@@ -241,16 +246,19 @@ def bench_ensemble(S, ctx, stream, steps, warmup):
     c0 = ctx.counters()
     t0 = time.perf_counter()
     k = max(2, steps // 5)
+    if dist is not None:
+        dist.barrier()
     for _ in range(k):
         S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_tol=PAD_TOL, seeds=seeds, autotune=True, out=hnp)
-    e2e_s = (time.perf_counter() - t0) / k
+    e2e_s = R.max_over_ranks((time.perf_counter() - t0) / k, dist, "cuda")
     c1 = ctx.counters()
     ctx.set_stream(stream.cuda_stream)
     same = bool(torch.equal(torch.from_numpy(hnp).cuda(), ref))
-    pvol = sum(p[0] * p[1] * p[2] for p in P)
-    return {"workload": "256 realisations, axes uniform in {64,96,128,160,192,256}, isotropic "
-                        "l uniform in [4,32], exponential, seeds 0-255, FP32, AUTO padding "
-                        f"(image error <= {PAD_TOL:g})",
+    pvol = int(R.sum_over_ranks(sum(p[0] * p[1] * p[2] for p in P), dist, "cuda"))
+    total = int(R.sum_over_ranks(total, dist, "cuda"))
+    return {"workload": "256 realisations per GPU, axes uniform in {64,96,128,160,192,256}, "
+                        "isotropic l uniform in [4,32], exponential, seeds 0-255 (rank k: "
+                        f"256k-256k+255), FP32, AUTO padding (image error <= {PAD_TOL:g})",
             "points": total, "padded_points": pvol,
             "value": round(total / (ms_b * 1e-3) / 1e6, 2), "unit": "Mpoints/s",
             "ms_per_ensemble": round(ms_b, 3), "gpu_launches_per_ensemble": int(launches),
@@ -265,15 +273,17 @@ def bench_ensemble(S, ctx, stream, steps, warmup):
             "host_output_equals_device_output": same}
 
 
-def bench_large_field(S, ctx, stream, steps):
+def bench_large_field(S, ctx, stream, steps, rank=0, dist=None):
     """2048 x 2048 x 1024 FP32 field, Gaussian l = (64, 64, 32), Gaussian
     marginal (variance 1), 4 x 4 x 1 tiles with a 128-point overlap, AUTO
     padding; then the streamed FP64 mean, variance and axis covariance up to
     lag 256 of the finished field."""
     import torch
+    from scarl_b200 import replicas as R
     ctx.set_stream(stream.cuda_stream)
     s = S.make_sample((0, 0, 0), (2047, 2047, 1023), (64, 64, 32), (127 / 64, 127 / 64, 0),
-                      (65, 65, 33), corrMod=1, margiFirst=1, avg=0.0, std_dev=1.0, seedBase=0)
+                      (65, 65, 33), corrMod=1, margiFirst=1, avg=0.0, std_dev=1.0,
+                      seedBase=R.replica_seed_base(rank))
     lay = S.sample_layout(s, 1, 16, (4, 4, 1))
     L = [int(v) for v in lay["L"]]
     n = L[0] * L[1] * L[2]
@@ -288,20 +298,25 @@ def bench_large_field(S, ctx, stream, steps):
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
     e0.record(stream)
     for _ in range(steps):
         gen()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_gen = e0.elapsed_time(e1) / steps
+    ms_gen = R.max_over_ranks(e0.elapsed_time(e1) / steps, dist, "cuda")
     S.axis_cov(ctx, field, L, 256)
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     e0.record(stream)
     for _ in range(steps):
         mean, var, cov = S.axis_cov(ctx, field, L, 256)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_stat = e0.elapsed_time(e1) / steps
+    ms_stat = R.max_over_ranks(e0.elapsed_time(e1) / steps, dist, "cuda")
+    world = dist.get_world_size() if dist is not None else 1
     ctx.profile(True)
     ctx.profile_reset()
     S.axis_cov(ctx, field, L, 256)
@@ -320,10 +335,11 @@ def bench_large_field(S, ctx, stream, steps):
     return {"workload": "2048x2048x1024 FP32, Gaussian l=(64,64,32), Gaussian marginal var 1, "
                         "4x4x1 tiles, overlap 128, AUTO padding; streamed FP64 mean, variance and "
                         "axis covariance up to lag 256",
-            "points": n, "padded_grid": P, "value": round(n / (ms_gen * 1e-3) / 1e6, 2),
+            "points": n * world, "padded_grid": P,
+            "value": round(world * n / (ms_gen * 1e-3) / 1e6, 2),
             "unit": "Mpoints/s", "ms_generate": round(ms_gen, 3),
             "ms_statistics": round(ms_stat, 3),
-            "statistics_field_reads_gbs": round(4 * n * 4 / (ms_stat * 1e-3) / 1e9, 1),
+            "statistics_field_reads_gbs": round(world * 4 * n * 4 / (ms_stat * 1e-3) / 1e9, 1),
             "statistics_kernels": kern, "mean": mean, "var": var,
             "cov_at_l": [float(cov[0, 64]), float(cov[1, 64]), float(cov[2, 32])],
             "target_at_l": float(__import__("math").exp(-__import__("math").pi))}
@@ -391,7 +407,8 @@ def main():
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     sample, lay = layout_of(S)
-    sample.seedBase = 1000 * rank  # independent replica per rank
+    from scarl_b200 import replicas as R
+    sample.seedBase = R.replica_seed_base(rank)  # independent replica per rank
     L = [int(v) for v in lay["L"]]
     npts = L[0] * L[1] * L[2]
     field = torch.empty(npts, dtype=torch.float32, device="cuda")
@@ -432,10 +449,7 @@ def main():
     clocks = clk.stop()
     ms = e0.elapsed_time(e1) / args.steps
     launches = ctx.counters()["launches"] - launches0
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = R.max_over_ranks(ms, dist, "cuda")
     value = world * npts / (ms * 1e-3) / 1e6
 
     # ---- the plain path: the reference's full padding, same timing method
@@ -448,10 +462,7 @@ def main():
     torch.cuda.synchronize()
     barrier()
     ms_full = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms_full], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_full = float(t.item())
+    ms_full = R.max_over_ranks(ms_full, dist, "cuda")
     plain = {"value": round(world * npts / (ms_full * 1e-3) / 1e6, 2), "ms_per_step": round(ms_full, 4),
              "padded_grid": P_full, "pad_policy": "full, 2^ceil(log2(2 Np)) (SRC_F/fftw_ScaRL.f90:194)"}
 
@@ -512,10 +523,7 @@ def main():
                           pad_tol=PAD_TOL, autotune=True, out=hnp)
     e2e_s = (time.perf_counter() - t0) / args.steps
     c1 = ctx.counters()
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = R.max_over_ranks(e2e_s, dist, "cuda")
     e2e = {"value": round(world * npts / e2e_s / 1e6, 2), "unit": "Mpoints/s",
            "h2d_bytes_per_step": (c1["h2d_bytes"] - c0["h2d_bytes"]) // args.steps,
            "d2h_bytes_per_step": (c1["d2h_bytes"] - c0["d2h_bytes"]) // args.steps,
@@ -528,11 +536,11 @@ def main():
 
     ens = None
     if not args.no_ensemble:
-        ens = bench_ensemble(S, ctx, stream, max(3, min(args.steps, 20)), args.warmup)
+        ens = bench_ensemble(S, ctx, stream, max(3, min(args.steps, 20)), args.warmup, rank, dist)
 
     large = None
     if not args.no_large_field:
-        large = bench_large_field(S, ctx, stream, 3)
+        large = bench_large_field(S, ctx, stream, 3, rank, dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
