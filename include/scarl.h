@@ -355,6 +355,60 @@ int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3],
 int scarl_rebuild_corrL(const double* SkTot, const int L[3], const double xStep[3],
                         double corrL_out[3]);
 
+/* ------------------------------------------------------------------ */
+/* Output files (SRC_F/write_output.f90, SRC_F/hdf5_ScaRL.f90)         */
+/* ------------------------------------------------------------------ */
+/* HDF5 + XDMF files of one generated sample, the three layouts of
+ * SRC_F/main_ScaRL.f90:590-668: one_file && one_hdf_ds -> folder/name.h5
+ * with dataset "samples" (write_hdf5_multi_proc_3D_1ds, :313-451) and
+ * name.xmf; one_file only -> name.h5 with one dataset "sample_1_p<rank>" per
+ * tile (write_hdf5_multi_proc_3D) and a global name.xmf; neither -> one
+ * file name_proc_<rank, 5 digits>.h5/.xmf per tile (write_hdf5_single_proc_3D)
+ * and the global name.xmf.  Every .h5 carries the root attributes of
+ * write_HDF5_attributes (:722-813); with ntimes > 0 also "times" (1 x ntimes)
+ * and "time_labels" (ntimes strings of 20 characters, time_labels holds
+ * ntimes x 20 characters, space or NUL padded) as write_time_on_hdf5 does.
+ * field: the L0 x L1 x L2 global field (device or host), written in its own
+ * precision (the reference writes FP64).  The files use the classic HDF5
+ * format (superblock 0, symbol-table groups, contiguous datasets) written by
+ * this library's own encoder; no HDF5 library is needed. */
+int scarl_write_sample_h5(scarl_ctx* ctx, const char* folder, const char* output_name,
+                          const void* field, int dtype, const scarl_sample* s,
+                          const scarl_layout* lay, int one_file, int one_hdf_ds,
+                          const char* time_labels, const double* times, int ntimes);
+/* [host] write_constant_field (SRC_F/write_output.f90:144-178), the output
+ * of a sample with std_dev = 0: folder/name.h5 holding a 2 x 2 x 2 dataset
+ * "samples" of avg with the reference's attribute values, and name.xmf. */
+int scarl_write_constant_field_h5(const char* folder, const char* output_name,
+                                  const double xMinGlob[3], const double xMaxGlob[3], double avg);
+/* Stat_ScaRL's step for one result file (SRC_F/Stat_ScaRL/main_Stat.f90:59-104)
+ * on the GPU: the sample attributes and dataset dset_name are read, the FP64
+ * mean and standard deviation computed (calculate_average_and_stdVar_MPI);
+ * with calc_corrL also the directional spectra (rebuild_Sk, literal Tukey
+ * window) and correlation lengths (rebuild_corrL), which are then added to
+ * the result file's root attributes (write_StatisticsOnH5: globalAvg,
+ * globalStdDev, evntAvg, evntStdDev, corrL_out, Sk_1..Sk_3).  Always writes
+ * folder/STAT_<file name> (makeStatFile).  corrL_out may be NULL. */
+int scarl_stat_file(scarl_ctx* ctx, const char* res_path, const char* dset_name, int calc_corrL,
+                    double* globalAvg, double* globalStdDev, double* corrL_out);
+/* [host] Dataset names of a classic-format HDF5 file, one per line. */
+int scarl_h5_list(const char* path, char* names, size_t len, char* msg, size_t msg_len);
+/* [host] Overwrites the raw bytes of a contiguous dataset in place (nbytes
+ * must equal its size), as write_time_on_hdf5 (SRC_F/write_output.f90:
+ * 819-911) reopens a result file to write its times. */
+int scarl_h5_overwrite_dataset(const char* path, const char* name, const void* data,
+                               unsigned long long nbytes, char* msg, size_t msg_len);
+/* [host] A numeric dataset of a classic-format HDF5 file (contiguous
+ * layout), converted to dtype into out; dims receives its extents in
+ * column-major order (HDF5 order reversed, 1 for missing axes), rank its
+ * rank.  out == NULL: extents only. */
+int scarl_h5_read_dataset(const char* path, const char* name, void* out, int dtype,
+                          long long dims[3], int* rank, char* msg, size_t msg_len);
+/* [host] A numeric attribute of the root group (object NULL or "") or of a
+ * dataset, as doubles; count receives its number of elements. */
+int scarl_h5_read_attr(const char* path, const char* object, const char* name, double* out,
+                       int max_count, int* count, char* msg, size_t msg_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,19 @@ SIGNATURES = {
                                            C.c_int, C.c_uint64, C.c_uint32, _vp, C.c_char_p,
                                            C.c_size_t]),
     "scarl_generate_sample": (C.c_int, [_vp, C.POINTER(Sample), C.POINTER(GenOpts), _vp]),
+    "scarl_write_sample_h5": (C.c_int, [_vp, C.c_char_p, C.c_char_p, _vp, C.c_int,
+                                        C.POINTER(Sample), C.POINTER(Layout), C.c_int, C.c_int,
+                                        C.c_char_p, _dp, C.c_int]),
+    "scarl_write_constant_field_h5": (C.c_int, [C.c_char_p, C.c_char_p, _dp, _dp, C.c_double]),
+    "scarl_stat_file": (C.c_int, [_vp, C.c_char_p, C.c_char_p, C.c_int, _dp, _dp, _dp]),
+    "scarl_h5_overwrite_dataset": (C.c_int, [C.c_char_p, C.c_char_p, _vp, C.c_ulonglong,
+                                             C.c_char_p, C.c_size_t]),
+    "scarl_h5_list": (C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]),
+    "scarl_h5_read_dataset": (C.c_int, [C.c_char_p, C.c_char_p, _vp, C.c_int,
+                                        C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.c_char_p,
+                                        C.c_size_t]),
+    "scarl_h5_read_attr": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _dp, C.c_int,
+                                     C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
     "scarl_axis_cov": (C.c_int, [_vp, _vp, C.c_int, _ip, C.c_int, _dp, _dp, _dp]),
     "scarl_ensemble_draw": (C.c_int, [C.c_uint64, C.c_longlong, C.c_int, _ip, C.c_int, C.c_double,
                                       C.c_double, _ip, _dp]),

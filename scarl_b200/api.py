@@ -473,6 +473,108 @@ def axis_cov(ctx, field, L, maxlag):
     return m.value, v.value, cov.reshape(3, maxlag + 1)
 
 
+# ---------------------------------------------------------------------------
+# Output files (HDF5 + XDMF, self-written classic-format encoder)
+# ---------------------------------------------------------------------------
+def _layout_struct(layout):
+    lay = Layout()
+    lay.L = _i3(layout["L"])
+    lay.Np = _i3(layout["Np"])
+    lay.Np_ovlp = _i3(layout["Np_ovlp"])
+    lay.topo_shape = _i3(layout["topo"])
+    lay.nb_tiles = int(layout["nb_tiles"])
+    lay.xStep = _d3(layout["xStep"])
+    return lay
+
+
+def write_sample_h5(ctx, folder, output_name, field, sample, layout, one_file=True,
+                    one_hdf_ds=True, times=None, time_labels=None):
+    """HDF5 + XDMF files of one generated field (write_hdf5_multi_proc_3D_1ds,
+    write_hdf5_multi_proc_3D or write_hdf5_single_proc_3D by one_file /
+    one_hdf_ds).  field: the column-major global field (numpy or device
+    tensor); ctx may be None for host fields."""
+    lay = _layout_struct(layout)
+    nt = 0 if times is None else len(times)
+    tv = None if times is None else np.ascontiguousarray(times, dtype=np.float64)
+    lab = None
+    if nt:
+        labels = list(time_labels or [""] * nt)
+        lab = "".join(str(x)[:20].ljust(20) for x in labels).encode()
+    f = field if hasattr(field, "data_ptr") else np.asfortranarray(field)
+    _check(lib().scarl_write_sample_h5(None if ctx is None else ctx.handle, str(folder).encode(),
+                                       str(output_name).encode(), _ptr(f), _dtype_of(f),
+                                       C.byref(sample), C.byref(lay), int(bool(one_file)),
+                                       int(bool(one_hdf_ds)), lab,
+                                       None if tv is None else tv.ctypes.data_as(C.POINTER(C.c_double)),
+                                       nt), ctx)
+
+
+def write_constant_field_h5(folder, output_name, xMinGlob, xMaxGlob, avg):
+    """write_constant_field: the file of a sample with std_dev = 0."""
+    _check(lib().scarl_write_constant_field_h5(str(folder).encode(), str(output_name).encode(),
+                                               _d3(xMinGlob), _d3(xMaxGlob), float(avg)))
+
+
+def stat_file(ctx, res_path, dset_name="samples", calculate_corrL=True):
+    """Stat_ScaRL's step for one result file on the GPU: FP64 moments, with
+    calculate_corrL the spectra and correlation lengths written back to the
+    file; always writes STAT_<file> beside it.  Returns (avg, std, corrL)."""
+    a, s = C.c_double(), C.c_double()
+    cl = (C.c_double * 3)()
+    _check(lib().scarl_stat_file(ctx.handle, str(res_path).encode(), dset_name.encode(),
+                                 int(bool(calculate_corrL)), C.byref(a), C.byref(s), cl), ctx)
+    return a.value, s.value, np.array(cl[:]) if calculate_corrL else None
+
+
+def _h5_check(rc, msg):
+    if rc != _lib.OK:
+        raise ScarlError(rc, msg.value.decode(errors="replace"))
+
+
+def h5_list(path):
+    buf = C.create_string_buffer(1 << 16)
+    msg = C.create_string_buffer(512)
+    _h5_check(lib().scarl_h5_list(str(path).encode(), buf, len(buf), msg, len(msg)), msg)
+    return [n for n in buf.value.decode().split("\n") if n]
+
+
+def h5_overwrite_dataset(path, name, data):
+    """Overwrites a dataset's raw bytes in place (same size)."""
+    a = np.ascontiguousarray(data)
+    msg = C.create_string_buffer(512)
+    _h5_check(lib().scarl_h5_overwrite_dataset(str(path).encode(), name.encode(),
+                                               C.c_void_p(a.ctypes.data), a.nbytes, msg, len(msg)),
+              msg)
+
+
+def h5_read_dataset(path, name, dtype=F64):
+    """A numeric dataset as a column-major numpy array (HDF5 dims reversed)."""
+    dims = (C.c_longlong * 3)()
+    rank = C.c_int()
+    msg = C.create_string_buffer(512)
+    _h5_check(lib().scarl_h5_read_dataset(str(path).encode(), name.encode(), None, dtype, dims,
+                                          C.byref(rank), msg, len(msg)), msg)
+    shape = tuple(int(d) for d in dims[:max(rank.value, 1)])
+    out = np.empty(shape, dtype=_np_dtype(dtype), order="F")
+    _h5_check(lib().scarl_h5_read_dataset(str(path).encode(), name.encode(), _ptr(out), dtype, dims,
+                                          C.byref(rank), msg, len(msg)), msg)
+    return out
+
+
+def h5_read_attr(path, name, obj=None):
+    """A numeric attribute of the root group (obj None) or a dataset."""
+    cnt = C.c_int()
+    msg = C.create_string_buffer(512)
+    o = b"" if obj is None else obj.encode()
+    _h5_check(lib().scarl_h5_read_attr(str(path).encode(), o, name.encode(), None, 0, C.byref(cnt),
+                                       msg, len(msg)), msg)
+    out = np.empty(max(cnt.value, 1))
+    _h5_check(lib().scarl_h5_read_attr(str(path).encode(), o, name.encode(),
+                                       out.ctypes.data_as(C.POINTER(C.c_double)), cnt.value,
+                                       C.byref(cnt), msg, len(msg)), msg)
+    return out[:cnt.value]
+
+
 def rebuild_corrL(SkTot, L, xStep):
     out = (C.c_double * 3)()
     s = np.ascontiguousarray(SkTot, dtype=np.float64)

@@ -19,7 +19,7 @@ CUDA_SOURCES = ["gen_padded.cu", "dct_literal.cu", "post.cu", "stats.cu", "cov.c
 # gen_inst.cu once per (precision, line-length group): the generator pass
 # instantiations compile in parallel
 INSTANCES = [(dt, n) for dt in (4, 8) for n in (0, 256, 512, 1024, 2048)]
-HOST_SOURCES = ["api.cpp", "host_maps.cpp"]
+HOST_SOURCES = ["api.cpp", "host_maps.cpp", "h5io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
           "-I", CSRC, "-I", INCLUDE]

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -16,6 +17,7 @@
 #include <vector>
 
 #include "../../include/scarl.h"
+#include "h5io.h"
 #include "host_maps.h"
 #include "scarl_internal.h"
 
@@ -994,6 +996,170 @@ int shino_args(scarl_ctx* ctx, const int Np[3], const double xRange[3], const do
 
 // ===========================================================================
 // C ABI
+// ---------------------------------------------------------------------------
+// HDF5 / XDMF output of a sample (SRC_F/write_output.f90).
+// ---------------------------------------------------------------------------
+std::string f25(double v) {
+  char b[64];
+  std::snprintf(b, sizeof b, "%25.10f", v);
+  return b;
+}
+
+std::string dim_text(const int n[3]) {  // slowest first, SRC_F/write_output.f90:488-497
+  return std::to_string(n[2]) + " " + std::to_string(n[1]) + " " + std::to_string(n[0]);
+}
+
+std::string pad5(int r) {  // num2str(rank, 5)
+  char b[32];
+  std::snprintf(b, sizeof b, "%05d", r);
+  return b;
+}
+
+// write_XMF_elements (SRC_F/write_output.f90:455-559)
+bool xmf_elements(const std::string& path, const std::string& h5name, const double xMin[3],
+                  const double xMax[3], const int n[3], const std::string& ds, int prec) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  double st[3];
+  for (int d = 0; d < 3; ++d) st[d] = (xMax[d] - xMin[d]) / (double)(n[d] - 1);
+  const std::string dt = dim_text(n);
+  std::fprintf(f, "<?xml version=\"1.0\" ?>\n<Xdmf Version=\"2.0\">\n <Domain>\n");
+  std::fprintf(f, "   <DataItem Name=\"RF_1\" Format=\"HDF\" DataType=\"Float\" Precision=\"%d\" Dimensions=\"%s\">\n", prec, dt.c_str());
+  std::fprintf(f, "        ./%s:/%s\n   </DataItem>\n", h5name.c_str(), ds.c_str());
+  std::fprintf(f, "  <Grid GridType=\"Collection\" CollectionType=\"Spatial\">\n   <Grid Name=\"Group1\">\n");
+  std::fprintf(f, "     <Topology TopologyType=\"3DCoRectMesh\" Dimensions=\"%s\"/>\n", dt.c_str());
+  std::fprintf(f, "     <Geometry GeometryType=\"ORIGIN_DXDYDZ\">\n");
+  std::fprintf(f, "   <DataItem Name=\"origin\" Format=\"XML\" DataType=\"Float\" Precision=\"8\" Dimensions=\"3\">\n");
+  for (int d = 2; d >= 0; --d) std::fprintf(f, " %s\n", f25(xMin[d]).c_str());
+  std::fprintf(f, "   </DataItem>\n   <DataItem Name=\"step\" Format=\"XML\" DataType=\"Float\" Precision=\"8\" Dimensions=\"3\">\n");
+  for (int d = 2; d >= 0; --d) std::fprintf(f, " %s\n", f25(st[d]).c_str());
+  std::fprintf(f, "   </DataItem>\n     </Geometry>\n");
+  std::fprintf(f, "     <Attribute Name=\"RF1\" Center=\"Node\" AttributeType=\"Scalar\">\n       <DataItem Reference=\"XML\">\n");
+  std::fprintf(f, "         /Xdmf/Domain/DataItem[@Name=\"RF_1\"]\n       </DataItem>\n     </Attribute>\n");
+  std::fprintf(f, "   </Grid>\n  </Grid>\n </Domain>\n</Xdmf>\n");
+  return std::fclose(f) == 0;
+}
+
+// write_XMF_global (SRC_F/write_output.f90:564-656)
+bool xmf_global(const std::string& path, const std::vector<std::string>& h5list,
+                const std::vector<std::array<double, 3>>& c0, const double xStep[3], const int n[3],
+                int prec) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  const std::string dt = dim_text(n);
+  const int np = (int)h5list.size();
+  std::fprintf(f, "<?xml version=\"1.0\" ?>\n<Xdmf Version=\"2.0\">\n <Domain>\n");
+  for (int i = 0; i < np; ++i) {
+    std::fprintf(f, "   <DataItem Name=\"RF_1_p%d\" Format=\"HDF\" DataType=\"Float\" Precision=\"%d\" Dimensions=\"%s\">\n", i, prec, dt.c_str());
+    std::fprintf(f, "        ./%s:/sample_1_p%d\n   </DataItem>\n", h5list[i].c_str(), i);
+  }
+  std::fprintf(f, "  <Grid GridType=\"Collection\" CollectionType=\"Spatial\">\n");
+  for (int i = 0; i < np; ++i) {
+    std::fprintf(f, "   <Grid Name=\"Proc_%d\">\n", i);
+    std::fprintf(f, "     <Topology TopologyType=\"3DCoRectMesh\" Dimensions=\"%s\"/>\n", dt.c_str());
+    std::fprintf(f, "     <Geometry GeometryType=\"ORIGIN_DXDYDZ\">\n");
+    std::fprintf(f, "   <DataItem Name=\"origin\" Format=\"XML\" DataType=\"Float\" Precision=\"8\" Dimensions=\"3\">\n");
+    for (int d = 2; d >= 0; --d) std::fprintf(f, " %s\n", f25(c0[i][d]).c_str());
+    std::fprintf(f, "   </DataItem>\n   <DataItem Name=\"step\" Format=\"XML\" DataType=\"Float\" Precision=\"8\" Dimensions=\"3\">\n");
+    for (int d = 2; d >= 0; --d) std::fprintf(f, " %s\n", f25(xStep[d]).c_str());
+    std::fprintf(f, "   </DataItem>\n     </Geometry>\n");
+    std::fprintf(f, "     <Attribute Name=\"RF_1\" Center=\"Node\" AttributeType=\"Scalar\">\n       <DataItem Reference=\"XML\">\n");
+    std::fprintf(f, "         /Xdmf/Domain/DataItem[@Name=\"RF_1_p%d\"]\n       </DataItem>\n     </Attribute>\n", i);
+    std::fprintf(f, "   </Grid>\n");
+  }
+  std::fprintf(f, "  </Grid>\n </Domain>\n</Xdmf>\n");
+  return std::fclose(f) == 0;
+}
+
+// Root attributes of write_HDF5_attributes (SRC_F/write_output.f90:722-813),
+// in its order.
+std::vector<h5::Attr> sample_attrs(const scarl_sample* s, const scarl_layout& lay,
+                                   const double xMaxEff[3]) {
+  std::vector<h5::Attr> a;
+  const int nb = lay.nb_tiles, ndim = 3, nmc = 1, method = SCARL_FFT, seed = s->seedBase;
+  a.push_back(h5::attr_i32("nb_procs", &nb, 1, true));
+  a.push_back(h5::attr_i32("nDim", &ndim, 1, true));
+  a.push_back(h5::attr_i32("Nmc", &nmc, 1, true));
+  a.push_back(h5::attr_i32("method", &method, 1, true));
+  a.push_back(h5::attr_i32("seedStart", &seed, 1, true));
+  a.push_back(h5::attr_i32("corrMod", &s->corrMod, 1, true));
+  a.push_back(h5::attr_i32("margiFirst", &s->margiFirst, 1, true));
+  a.push_back(h5::attr_i32("nFields", lay.topo_shape, 3));
+  a.push_back(h5::attr_i32("Np", lay.Np, 3));
+  a.push_back(h5::attr_i32("Np_ovlp", lay.Np_ovlp, 3));
+  a.push_back(h5::attr_i32("L", lay.L, 3));
+  double ov[3];
+  for (int d = 0; d < 3; ++d) ov[d] = (double)(lay.Np_ovlp[d] - 1) * lay.xStep[d];  // main_ScaRL.f90:460
+  a.push_back(h5::attr_f64("xMinGlob", s->xMinGlob, 3));
+  a.push_back(h5::attr_f64("xMaxGlob", xMaxEff, 3));
+  a.push_back(h5::attr_f64("xStep", lay.xStep, 3));
+  a.push_back(h5::attr_f64("corrL", s->corrL, 3));
+  a.push_back(h5::attr_f64("overlap", ov, 3));
+  return a;
+}
+
+// "times" (ranks x labels, one rank here) and "time_labels" (20-character
+// Fortran strings), write_time_on_hdf5 (SRC_F/write_output.f90:819-911).
+void time_datasets(const char* labels, const double* times, int nt, std::vector<h5::Dataset>* ds) {
+  if (nt <= 0 || !times) return;
+  h5::Dataset t;
+  t.name = "times";
+  t.kind = h5::F64;
+  t.dims = {1, (uint64_t)nt};
+  t.nbytes = (uint64_t)nt * 8;
+  std::vector<double> tv(times, times + nt);
+  t.write = [tv](FILE* f) { return std::fwrite(tv.data(), 8, tv.size(), f) == tv.size(); };
+  ds->push_back(t);
+  h5::Dataset l;
+  l.name = "time_labels";
+  l.kind = h5::STR;
+  l.strsize = 20;
+  l.dims = {(uint64_t)nt};
+  l.nbytes = (uint64_t)nt * 20;
+  std::string lv((size_t)nt * 20, ' ');
+  if (labels)
+    for (int i = 0; i < nt; ++i)
+      for (int c = 0; c < 20 && labels[i * 20 + c]; ++c) lv[(size_t)i * 20 + c] = labels[i * 20 + c];
+  l.write = [lv](FILE* f) { return std::fwrite(lv.data(), 1, lv.size(), f) == lv.size(); };
+  ds->push_back(l);
+}
+
+// Writes the block [o, o + n) of a column-major field of extent L to f,
+// staging through pinned memory when the field is on the device.
+bool write_block(scarl_ctx* ctx, FILE* f, const void* field, bool dev, int dt, const int L[3],
+                 const int o[3], const int n[3]) {
+  const size_t line = (size_t)n[0] * dt;
+  const bool whole = o[0] == 0 && o[1] == 0 && o[2] == 0 && n[0] == L[0] && n[1] == L[1] && n[2] == L[2];
+  if (!dev) {
+    const char* p = static_cast<const char*>(field);
+    if (whole) return std::fwrite(p, 1, line * n[1] * n[2], f) == line * n[1] * n[2];
+    for (int z = 0; z < n[2]; ++z)
+      for (int y = 0; y < n[1]; ++y) {
+        const size_t at = ((size_t)(o[2] + z) * L[1] + (o[1] + y)) * L[0] + o[0];
+        if (std::fwrite(p + at * dt, 1, line, f) != line) return false;
+      }
+    return true;
+  }
+  const size_t plane = line * n[1];
+  const size_t zper = std::max<size_t>(1, ((size_t)64 << 20) / plane);
+  void* pin;
+  if (pinned(ctx, std::min<size_t>(zper, n[2]) * plane, &pin) != SCARL_OK) return false;
+  for (int z0 = 0; z0 < n[2]; z0 += (int)zper) {
+    const int nz = (int)std::min<size_t>(zper, (size_t)(n[2] - z0));
+    for (int z = 0; z < nz; ++z) {
+      const char* src = static_cast<const char*>(field) +
+                        (((size_t)(o[2] + z0 + z) * L[1] + o[1]) * L[0] + o[0]) * dt;
+      if (cudaMemcpy2DAsync(static_cast<char*>(pin) + (size_t)z * plane, line, src, (size_t)L[0] * dt,
+                            line, n[1], cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
+        return false;
+    }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return false;
+    ctx->d2h += plane * nz;
+    if (std::fwrite(pin, 1, plane * nz, f) != plane * nz) return false;
+  }
+  return true;
+}
+
 // ===========================================================================
 extern "C" {
 
@@ -1226,6 +1392,345 @@ int scarl_rebuild_corrL(const double* SkTot, const int L[3], const double xStep[
     off += nk;
   }
   return SCARL_OK;
+}
+
+// ---- Stat_ScaRL front end ----
+int scarl_stat_file(scarl_ctx* ctx, const char* res_path, const char* dset_name, int calc_corrL,
+                    double* globalAvg, double* globalStdDev, double* corrL_out) {
+  RC(begin(ctx));
+  if (!res_path || !dset_name || !globalAvg || !globalStdDev) return fail(ctx, SCARL_EINVAL, "null argument");
+  h5::RObject root;
+  std::vector<h5::RObject> ds;
+  std::string err;
+  int rc = h5::read_file(res_path, &root, &ds, &err);
+  if (rc) return fail(ctx, rc == 5 ? SCARL_EUNSUPPORTED : (rc == 6 ? SCARL_EIO : SCARL_EINVAL), err);
+  const h5::RObject* d = nullptr;
+  for (const auto& o : ds)
+    if (o.name == dset_name) d = &o;
+  if (!d || !d->is_dataset || d->kind == h5::STR)
+    return fail(ctx, SCARL_EINVAL, std::string("no numeric dataset ") + dset_name + " in " + res_path);
+  if (d->dims.size() != 3) return fail(ctx, SCARL_EUNSUPPORTED, "the sample dataset must be 3D");
+  auto find = [&](const char* n) -> const h5::Attr* {
+    for (const auto& a : root.attrs)
+      if (a.name == n) return &a;
+    return nullptr;
+  };
+  // read_RF_h5_File_Attributes (SRC_F/Stat_ScaRL/main_Stat.f90:133-194)
+  const char* needed[] = {"nb_procs", "nDim", "Nmc", "method", "seedStart", "corrMod", "margiFirst",
+                          "nFields", "Np", "Np_ovlp", "L", "xMinGlob", "xMaxGlob", "xStep", "corrL",
+                          "overlap"};
+  for (const char* n : needed)
+    if (!find(n)) return fail(ctx, SCARL_EINVAL, std::string("attribute ") + n + " missing in " + res_path);
+  const h5::Attr* xs = find("xStep");
+  if (xs->kind != h5::F64 || xs->data.size() != 24) return fail(ctx, SCARL_EINVAL, "xStep must hold 3 doubles");
+  double xStep[3];
+  std::memcpy(xStep, xs->data.data(), 24);
+  const int L[3] = {(int)d->dims[2], (int)d->dims[1], (int)d->dims[0]};
+  const size_t n = (size_t)L[0] * L[1] * L[2];
+  const int dt = d->kind == h5::F32 ? SCARL_F32 : SCARL_F64;
+  // read_RF_h5_File_Table: the whole dataset, then one upload
+  std::vector<double> h64;
+  std::vector<float> h32;
+  if (dt == SCARL_F64) h64.resize(n);
+  else h32.resize(n);
+  if (h5::read_values(res_path, *d, dt == SCARL_F64 ? h64.data() : nullptr,
+                      dt == SCARL_F32 ? h32.data() : nullptr, &err))
+    return fail(ctx, SCARL_EIO, err);
+  RC(ensure(ctx, ctx->tile, n * dt));
+  CK(cudaMemcpyAsync(ctx->tile.p, dt == SCARL_F64 ? (const void*)h64.data() : (const void*)h32.data(),
+                     n * dt, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += n * dt;
+  double evA = 0.0, evS = 0.0;
+  RC(scarl_moments(ctx, ctx->tile.p, dt, (long long)n, 1, &evA, &evS, globalAvg, globalStdDev));
+  std::vector<h5::Attr> stats;
+  stats.push_back(h5::attr_f64("globalAvg", globalAvg, 1, true));
+  stats.push_back(h5::attr_f64("globalStdDev", globalStdDev, 1, true));
+  stats.push_back(h5::attr_f64("evntAvg", &evA, 1));
+  stats.push_back(h5::attr_f64("evntStdDev", &evS, 1));
+  if (calc_corrL) {
+    std::vector<double> sk((size_t)L[0] / 2 + L[1] / 2 + L[2] / 2);
+    double cl[3];
+    RC(scarl_rebuild_sk(ctx, ctx->tile.p, dt, L, *globalAvg, *globalStdDev, 1, sk.data()));
+    RC(scarl_rebuild_corrL(sk.data(), L, xStep, cl));
+    if (corrL_out) std::memcpy(corrL_out, cl, sizeof cl);
+    stats.push_back(h5::attr_f64("corrL_out", cl, 3));
+    size_t off = 0;
+    for (int k = 0; k < 3; ++k) {
+      const int nk = L[k] / 2;
+      stats.push_back(h5::attr_f64("Sk_" + std::to_string(k + 1), sk.data() + off, nk));
+      off += (size_t)nk;
+    }
+    // write_StatisticsOnH5 on the result file (main_Stat.f90:90-96)
+    if (h5::append_root_attrs(res_path, stats, &err)) return fail(ctx, SCARL_EIO, err);
+  }
+  // makeStatFile (main_Stat.f90:635-790): folder/STAT_<file> with the
+  // sample's attributes, the result file's size in MB and the statistics
+  const std::string rp = res_path;
+  const size_t slash = rp.find_last_of('/');
+  const std::string folder = slash == std::string::npos ? std::string(".") : rp.substr(0, slash);
+  const std::string fname = slash == std::string::npos ? rp : rp.substr(slash + 1);
+  double mb = 0.0;
+  if (FILE* f = std::fopen(res_path, "rb")) {
+    std::fseek(f, 0, SEEK_END);
+    mb = (double)std::ftell(f) / (1024.0 * 1024.0);
+    std::fclose(f);
+  }
+  std::vector<h5::Attr> out;
+  for (const char* nme : {"nb_procs", "nDim", "Nmc", "method", "seedStart", "corrMod", "margiFirst"})
+    out.push_back(*find(nme));
+  out.push_back(h5::attr_f64("old_file_mb_size", &mb, 1, true));
+  for (const char* nme : {"nFields", "Np", "Np_ovlp", "L", "xMinGlob", "xMaxGlob", "xStep", "corrL", "overlap"})
+    out.push_back(*find(nme));
+  out.insert(out.end(), stats.begin(), stats.end());
+  if (h5::write_file(folder + "/STAT_" + fname, out, {}, &err)) return fail(ctx, SCARL_EIO, err);
+  return SCARL_OK;
+}
+
+// ---- output files ----
+int scarl_write_sample_h5(scarl_ctx* ctx, const char* folder, const char* output_name,
+                          const void* field, int dtype, const scarl_sample* s,
+                          const scarl_layout* lay, int one_file, int one_hdf_ds,
+                          const char* time_labels, const double* times, int ntimes) {
+  if (ctx) RC(begin(ctx));
+  if (!folder || !output_name || !field || !s || !lay) return fail(ctx, SCARL_EINVAL, "null argument");
+  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  const bool dev = is_device_ptr(field);
+  if (dev && !ctx) return SCARL_EINVAL;  // device fields are copied through a context
+  if (lay->nb_tiles < 1 || lay->nb_tiles != lay->topo_shape[0] * lay->topo_shape[1] * lay->topo_shape[2])
+    return fail(ctx, SCARL_EINVAL, "inconsistent layout");
+  const h5::Kind kind = dtype == SCARL_F64 ? h5::F64 : h5::F32;
+  const std::string dir = std::string(folder) + "/";
+  const std::string name = output_name;
+  const int nb = lay->nb_tiles;
+  std::vector<scarl_tile> tiles(nb);
+  for (int r = 0; r < nb; ++r) tile_geometry(lay, s->xMinGlob, r, &tiles[r]);
+  double xMaxEff[3];  // main_ScaRL.f90:462-467 (xMaxGlob re-derived from the last tile)
+  for (int d = 0; d < 3; ++d) xMaxEff[d] = tiles[nb - 1].coord_N[d];
+  const std::vector<h5::Attr> root = sample_attrs(s, *lay, xMaxEff);
+  std::string err;
+  auto tile_dataset = [&](int r, bool pos) {
+    h5::Dataset d;
+    d.name = "sample_1_p" + std::to_string(r);
+    d.kind = kind;
+    d.dims = {(uint64_t)lay->Np[2], (uint64_t)lay->Np[1], (uint64_t)lay->Np[0]};
+    d.nbytes = (uint64_t)lay->Np[0] * lay->Np[1] * lay->Np[2] * dtype;
+    d.attrs.push_back(h5::attr_f64("xMin", tiles[r].coord_0, 3));
+    d.attrs.push_back(h5::attr_f64("xMax", tiles[r].coord_N, 3));
+    if (pos) {
+      d.attrs.push_back(h5::attr_i32("pos_0", tiles[r].pos_0, 3));
+      d.attrs.push_back(h5::attr_i32("pos_N", tiles[r].pos_N, 3));
+    }
+    int o[3];
+    for (int k = 0; k < 3; ++k) o[k] = tiles[r].pos_0[k] - 1;
+    const int* Np = lay->Np;
+    const int* L = lay->L;
+    d.write = [=](FILE* f) { return write_block(ctx, f, field, dev, dtype, L, o, Np); };
+    return d;
+  };
+  if (one_file && one_hdf_ds) {  // write_hdf5_multi_proc_3D_1ds
+    std::vector<h5::Dataset> ds;
+    h5::Dataset d;
+    d.name = "samples";
+    d.kind = kind;
+    d.dims = {(uint64_t)lay->L[2], (uint64_t)lay->L[1], (uint64_t)lay->L[0]};
+    d.nbytes = (uint64_t)lay->L[0] * lay->L[1] * lay->L[2] * dtype;
+    const int one[3] = {1, 1, 1};
+    d.attrs.push_back(h5::attr_f64("xMin", tiles[0].coord_0, 3));
+    d.attrs.push_back(h5::attr_f64("xMax", xMaxEff, 3));
+    d.attrs.push_back(h5::attr_i32("pos_0", one, 3));
+    d.attrs.push_back(h5::attr_i32("pos_N", lay->L, 3));
+    const int zero[3] = {0, 0, 0};
+    const int* L = lay->L;
+    d.write = [=](FILE* f) { return write_block(ctx, f, field, dev, dtype, L, zero, L); };
+    ds.push_back(d);
+    time_datasets(time_labels, times, ntimes, &ds);
+    if (h5::write_file(dir + name + ".h5", root, ds, &err)) return fail(ctx, SCARL_EIO, err);
+    if (!xmf_elements(dir + name + ".xmf", name + ".h5", tiles[0].coord_0, xMaxEff, lay->L, "samples", dtype))
+      return fail(ctx, SCARL_EIO, "cannot write " + dir + name + ".xmf");
+    return SCARL_OK;
+  }
+  std::vector<std::string> h5list(nb);
+  std::vector<std::array<double, 3>> c0(nb);
+  for (int r = 0; r < nb; ++r)
+    for (int d = 0; d < 3; ++d) c0[r][d] = tiles[r].coord_0[d];
+  if (one_file) {  // write_hdf5_multi_proc_3D: one dataset per tile
+    std::vector<h5::Dataset> ds;
+    for (int r = 0; r < nb; ++r) ds.push_back(tile_dataset(r, true));
+    time_datasets(time_labels, times, ntimes, &ds);
+    if (h5::write_file(dir + name + ".h5", root, ds, &err)) return fail(ctx, SCARL_EIO, err);
+    for (int r = 0; r < nb; ++r) h5list[r] = name + ".h5";
+  } else {  // write_hdf5_single_proc_3D: one file per tile
+    for (int r = 0; r < nb; ++r) {
+      const std::string base = name + "_proc_" + pad5(r);
+      std::vector<h5::Dataset> ds = {tile_dataset(r, false)};
+      time_datasets(time_labels, times, ntimes, &ds);
+      if (h5::write_file(dir + base + ".h5", root, ds, &err)) return fail(ctx, SCARL_EIO, err);
+      if (!xmf_elements(dir + base + ".xmf", base + ".h5", tiles[r].coord_0, tiles[r].coord_N, lay->Np,
+                        "sample_1_p" + std::to_string(r), dtype))
+        return fail(ctx, SCARL_EIO, "cannot write " + dir + base + ".xmf");
+      h5list[r] = base + ".h5";
+    }
+  }
+  if (!xmf_global(dir + name + ".xmf", h5list, c0, lay->xStep, lay->Np, dtype))
+    return fail(ctx, SCARL_EIO, "cannot write " + dir + name + ".xmf");
+  return SCARL_OK;
+}
+
+// write_constant_field (SRC_F/write_output.f90:144-178): a 2 x 2 x 2 field of
+// avg with the attribute values the reference gives it.
+int scarl_write_constant_field_h5(const char* folder, const char* output_name,
+                                  const double xMinGlob[3], const double xMaxGlob[3], double avg) {
+  if (!folder || !output_name || !xMinGlob || !xMaxGlob) return SCARL_EINVAL;
+  const std::string dir = std::string(folder) + "/", name = output_name;
+  const int one = 1, three = 3, m1 = -1;
+  const int ones[3] = {1, 1, 1}, twos[3] = {2, 2, 2}, zeros[3] = {0, 0, 0};
+  double xStep[3];
+  for (int d = 0; d < 3; ++d) xStep[d] = xMaxGlob[d] - xMinGlob[d];
+  const double neg[3] = {-1.0, -1.0, -1.0}, zero3[3] = {0.0, 0.0, 0.0};
+  std::vector<h5::Attr> root;
+  root.push_back(h5::attr_i32("nb_procs", &one, 1, true));
+  root.push_back(h5::attr_i32("nDim", &three, 1, true));
+  root.push_back(h5::attr_i32("Nmc", &one, 1, true));
+  root.push_back(h5::attr_i32("method", &m1, 1, true));
+  root.push_back(h5::attr_i32("seedStart", &m1, 1, true));
+  root.push_back(h5::attr_i32("corrMod", &m1, 1, true));
+  root.push_back(h5::attr_i32("margiFirst", &m1, 1, true));
+  root.push_back(h5::attr_i32("nFields", ones, 3));
+  root.push_back(h5::attr_i32("Np", twos, 3));
+  root.push_back(h5::attr_i32("Np_ovlp", zeros, 3));
+  root.push_back(h5::attr_i32("L", twos, 3));
+  root.push_back(h5::attr_f64("xMinGlob", xMinGlob, 3));
+  root.push_back(h5::attr_f64("xMaxGlob", xMaxGlob, 3));
+  root.push_back(h5::attr_f64("xStep", xStep, 3));
+  root.push_back(h5::attr_f64("corrL", neg, 3));
+  root.push_back(h5::attr_f64("overlap", zero3, 3));
+  h5::Dataset d;
+  d.name = "samples";
+  d.kind = h5::F64;
+  d.dims = {2, 2, 2};
+  d.nbytes = 64;
+  d.attrs.push_back(h5::attr_f64("xMin", xMinGlob, 3));
+  d.attrs.push_back(h5::attr_f64("xMax", xMaxGlob, 3));
+  d.write = [avg](FILE* f) {
+    const double v[8] = {avg, avg, avg, avg, avg, avg, avg, avg};
+    return std::fwrite(v, 8, 8, f) == 8;
+  };
+  std::string err;
+  if (h5::write_file(dir + name + ".h5", root, {d}, &err)) return SCARL_EIO;
+  if (!xmf_elements(dir + name + ".xmf", name + ".h5", xMinGlob, xMaxGlob, twos, "samples", 8))
+    return SCARL_EIO;
+  return SCARL_OK;
+}
+
+static int copy_msg(char* msg, size_t len, const std::string& m) {
+  if (msg && len) {
+    std::snprintf(msg, len, "%s", m.c_str());
+  }
+  return 0;
+}
+
+int scarl_h5_overwrite_dataset(const char* path, const char* name, const void* data,
+                               unsigned long long nbytes, char* msg, size_t msg_len) {
+  if (!path || !name || !data) return SCARL_EINVAL;
+  std::string err;
+  const int rc = h5::overwrite_dataset(path, name, data, nbytes, &err);
+  if (rc) {
+    copy_msg(msg, msg_len, err);
+    return rc == 6 ? SCARL_EIO : (rc == 5 ? SCARL_EUNSUPPORTED : SCARL_EINVAL);
+  }
+  return SCARL_OK;
+}
+
+int scarl_h5_list(const char* path, char* names, size_t len, char* msg, size_t msg_len) {
+  if (!path || !names || !len) return SCARL_EINVAL;
+  h5::RObject root;
+  std::vector<h5::RObject> ds;
+  std::string err;
+  const int rc = h5::read_file(path, &root, &ds, &err);
+  if (rc) {
+    copy_msg(msg, msg_len, err);
+    return rc == 5 ? SCARL_EUNSUPPORTED : (rc == 6 ? SCARL_EIO : SCARL_EINVAL);
+  }
+  std::string all;
+  for (const auto& d : ds) all += d.name + "\n";
+  if (all.size() + 1 > len) {
+    copy_msg(msg, msg_len, "name buffer too small");
+    return SCARL_EINVAL;
+  }
+  std::memcpy(names, all.c_str(), all.size() + 1);
+  return SCARL_OK;
+}
+
+int scarl_h5_read_dataset(const char* path, const char* name, void* out, int dtype,
+                          long long dims[3], int* rank, char* msg, size_t msg_len) {
+  if (!path || !name || !dims || !rank) return SCARL_EINVAL;
+  h5::RObject root;
+  std::vector<h5::RObject> ds;
+  std::string err;
+  const int rc = h5::read_file(path, &root, &ds, &err);
+  if (rc) {
+    copy_msg(msg, msg_len, err);
+    return rc == 5 ? SCARL_EUNSUPPORTED : (rc == 6 ? SCARL_EIO : SCARL_EINVAL);
+  }
+  for (const auto& d : ds) {
+    if (d.name != name) continue;
+    if (d.dims.size() > 3) {
+      copy_msg(msg, msg_len, "datasets of rank > 3 are not supported");
+      return SCARL_EUNSUPPORTED;
+    }
+    *rank = (int)d.dims.size();
+    for (int k = 0; k < 3; ++k) dims[k] = 1;
+    for (int k = 0; k < *rank; ++k) dims[k] = (long long)d.dims[*rank - 1 - k];  // column-major order
+    if (!out) return SCARL_OK;
+    if (dtype != SCARL_F32 && dtype != SCARL_F64) return SCARL_EINVAL;
+    if (h5::read_values(path, d, dtype == SCARL_F64 ? (double*)out : nullptr,
+                        dtype == SCARL_F32 ? (float*)out : nullptr, &err)) {
+      copy_msg(msg, msg_len, err);
+      return SCARL_EIO;
+    }
+    return SCARL_OK;
+  }
+  copy_msg(msg, msg_len, std::string("no dataset ") + name);
+  return SCARL_EINVAL;
+}
+
+int scarl_h5_read_attr(const char* path, const char* object, const char* name, double* out,
+                       int max_count, int* count, char* msg, size_t msg_len) {
+  if (!path || !name || !count) return SCARL_EINVAL;
+  h5::RObject root;
+  std::vector<h5::RObject> ds;
+  std::string err;
+  const int rc = h5::read_file(path, &root, &ds, &err);
+  if (rc) {
+    copy_msg(msg, msg_len, err);
+    return rc == 5 ? SCARL_EUNSUPPORTED : (rc == 6 ? SCARL_EIO : SCARL_EINVAL);
+  }
+  const h5::RObject* o = nullptr;
+  if (!object || !*object) o = &root;
+  for (const auto& d : ds)
+    if (object && d.name == object) o = &d;
+  if (!o) {
+    copy_msg(msg, msg_len, std::string("no object ") + (object ? object : ""));
+    return SCARL_EINVAL;
+  }
+  for (const auto& a : o->attrs) {
+    if (a.name != name) continue;
+    if (a.kind == h5::STR) {
+      copy_msg(msg, msg_len, "string attribute");
+      return SCARL_EUNSUPPORTED;
+    }
+    const int es = a.kind == h5::F64 ? 8 : 4;
+    const int n = (int)(a.data.size() / es);
+    *count = n;
+    for (int i = 0; i < n && i < max_count && out; ++i) {
+      if (a.kind == h5::F64) std::memcpy(&out[i], &a.data[(size_t)i * 8], 8);
+      else if (a.kind == h5::F32) { float f; std::memcpy(&f, &a.data[(size_t)i * 4], 4); out[i] = f; }
+      else { int32_t v; std::memcpy(&v, &a.data[(size_t)i * 4], 4); out[i] = v; }
+    }
+    return SCARL_OK;
+  }
+  copy_msg(msg, msg_len, std::string("no attribute ") + name);
+  return SCARL_EINVAL;
 }
 
 // ---- generation ----
