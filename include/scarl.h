@@ -60,6 +60,7 @@ extern "C" {
 /* ---- padded grid policies ---- */
 #define SCARL_PAD_FULL 0     /* 2^ceil(log2(2 Np)), SRC_F/fftw_ScaRL.f90:194 */
 #define SCARL_PAD_AUTO 1     /* smallest power of two with image error <= tol */
+#define SCARL_PAD_LEARNED 2  /* the context's trained predictor, full padding as fallback */
 
 typedef struct scarl_ctx scarl_ctx;
 
@@ -107,7 +108,7 @@ typedef struct {
   int nb_procs;           /* tiles requested (mpirun -np), 0 = 1 */
   int topo_shape[3];      /* explicit topology (extra_config_ScaRL.txt); 0 = decide */
   int pad[3];             /* explicit padded grid per axis; 0 = chosen by pad_policy */
-  int pad_policy;         /* SCARL_PAD_FULL (default) or SCARL_PAD_AUTO */
+  int pad_policy;         /* SCARL_PAD_FULL (default), SCARL_PAD_AUTO or SCARL_PAD_LEARNED */
   double pad_tol;         /* SCARL_PAD_AUTO image tolerance, 0 = 1e-3 */
   int no_spectral_normalisation; /* 1 = raw Riemann-sum amplitudes */
   int normalize_field;    /* 1 = normalize_field (disabled in the reference) */
@@ -343,17 +344,59 @@ int scarl_rebuild_sk(scarl_ctx* ctx, const void* field, int dtype, const int L[3
  * one field L[0] x L[1] x L[2] (column-major, device or host pointer), FP64
  * accumulation on the GPU:
  *   cov[d (maxlag + 1) + h] = sum over point pairs (x, x + h e_d) of
- *       (f(x) - mean)(f(x + h e_d) - mean) / number of such pairs,
- * mean over all points, var = cov[0].  One moment pass plus one pass per
+ *       (f(x) - m)(f(x + h e_d) - m) / number of such pairs,
+ * m = *known_mean when given (an ensemble of known mean), else the mean over
+ * all points; *mean receives the sample mean, var = cov[0].  One moment pass plus one pass per
  * axis over the field.  No direct counterpart: rebuild_Sk_FFT
  * (statistics_RF.f90:258-462) windows and wraps each line; this is the
  * plain linear estimator a covariance model is checked against.  Needs
  * maxlag < L[d] and L[d] + maxlag <= 4096. */
 int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
-                   double* mean, double* var, double* cov);
+                   const double* known_mean, double* mean, double* var, double* cov);
 /* [host] rebuild_corrL (statistics_RF.f90:468-486). */
 int scarl_rebuild_corrL(const double* SkTot, const int L[3], const double xStep[3],
                         double corrL_out[3]);
+
+/* ------------------------------------------------------------------ */
+/* Learned padding / overlap predictor (no counterpart in the          */
+/* reference)                                                          */
+/* ------------------------------------------------------------------ */
+/* Labels from the method's expected axis covariance (FP64, GPU): for axis
+ * i (corrMod[i], nu[i], correlation length ell_pts[i] in grid points, N[i]
+ * <= 256 points) the smallest padded length P[i] whose covariance differs
+ * by <= 0.01 from the infinitely padded method's over lags 0..N-1, and the
+ * smallest overlap W[i] whose partition-of-unity blend keeps the covariance
+ * error <= 0.01.  saturated[i] = 1 when even 16 N did not reach it. */
+int scarl_pad_labels(scarl_ctx* ctx, int n, const int* corrMod, const double* nu,
+                     const double* ell_pts, const int* N, int* P, int* W, int* saturated);
+/* The same covariance error at given padded lengths P[i] (N <= P <= 8192). */
+int scarl_pad_error(scarl_ctx* ctx, int n, const int* corrMod, const double* nu,
+                    const double* ell_pts, const int* N, const int* P, double* err);
+/* [host] Network inputs (16 per axis) and targets (log2 of the image
+ * distance P - N + 1 and of W, in correlation lengths; 2 per axis). */
+int scarl_mlp_features(int n, const int* corrMod, const double* nu, const double* ell_pts,
+                       const int* N, float* X);
+int scarl_mlp_targets(int n, const double* ell_pts, const int* N, const int* P, const int* W,
+                      float* T);
+/* The context's MLP (16 -> 64 -> 64 -> 2, ReLU; BF16 weights and
+ * activations, FP32 accumulation; 5378 FP32 master parameters in the order
+ * W1[64][16] b1 W2[64][64] b2 W3[2][64] b3). */
+int scarl_mlp_init(scarl_ctx* ctx, uint64_t seed);
+int scarl_mlp_params(scarl_ctx* ctx, float* get, const float* set);
+/* Mean-squared-error loss and its gradient over n samples (no update). */
+int scarl_mlp_grad(scarl_ctx* ctx, const float* X, const float* T, int n, float* grad,
+                   double* loss);
+/* steps full-batch Adam steps (learning rate lr); loss_hist: steps losses or NULL. */
+int scarl_mlp_train(scarl_ctx* ctx, const float* X, const float* T, int n, int steps, float lr,
+                    double* loss_hist);
+int scarl_mlp_predict(scarl_ctx* ctx, const float* X, int n, float* Y);
+/* Padded grid and overlap width per axis from the trained model, with a
+ * 2^0.25 safety margin; full padding (SRC_F/fftw_ScaRL.f90:194) when the
+ * inputs leave the trained range or the prediction exceeds it (fallback:
+ * bit 0 out of range, bit 1 capped).  W may be NULL. */
+int scarl_pad_size_learned(scarl_ctx* ctx, int corrMod, double nu, const double corrL[3],
+                           const double xStep[3], const int Np[3], int P[3], int W[3],
+                           int* fallback);
 
 /* ------------------------------------------------------------------ */
 /* Output files (SRC_F/write_output.f90, SRC_F/hdf5_ScaRL.f90)         */

@@ -15,10 +15,12 @@ STATUS_NAMES = {0: "SCARL_OK", 1: "SCARL_EINVAL", 2: "SCARL_ENOMEM", 3: "SCARL_E
                 4: "SCARL_ETIMEOUT", 5: "SCARL_EUNSUPPORTED", 6: "SCARL_EIO"}
 FFT, FFT_MPI = 1, 2
 CM_GAUSSIAN, CM_VON_KARMAN, CM_EXPONENTIAL = 1, 2, 3
+MLP_PARAMS = 5378
+MLP_IN = 16
 FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
 F32, F64 = 4, 8
 GEN_DCT, GEN_SHINO, GEN_PADDED = 1, 2, 3
-PAD_FULL, PAD_AUTO = 0, 1
+PAD_FULL, PAD_AUTO, PAD_LEARNED = 0, 1, 2
 
 
 class Sample(C.Structure):
@@ -100,6 +102,18 @@ SIGNATURES = {
                                            C.c_int, C.c_uint64, C.c_uint32, _vp, C.c_char_p,
                                            C.c_size_t]),
     "scarl_generate_sample": (C.c_int, [_vp, C.POINTER(Sample), C.POINTER(GenOpts), _vp]),
+    "scarl_pad_labels": (C.c_int, [_vp, C.c_int, _ip, _dp, _dp, _ip, _ip, _ip, _ip]),
+    "scarl_pad_error": (C.c_int, [_vp, C.c_int, _ip, _dp, _dp, _ip, _ip, _dp]),
+    "scarl_mlp_features": (C.c_int, [C.c_int, _ip, _dp, _dp, _ip, C.POINTER(C.c_float)]),
+    "scarl_mlp_targets": (C.c_int, [C.c_int, _dp, _ip, _ip, _ip, C.POINTER(C.c_float)]),
+    "scarl_mlp_init": (C.c_int, [_vp, C.c_uint64]),
+    "scarl_mlp_params": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "scarl_mlp_grad": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
+                                 C.POINTER(C.c_float), _dp]),
+    "scarl_mlp_train": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
+                                  C.c_int, C.c_float, _dp]),
+    "scarl_mlp_predict": (C.c_int, [_vp, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float)]),
+    "scarl_pad_size_learned": (C.c_int, [_vp, C.c_int, C.c_double, _dp, _dp, _ip, _ip, _ip, _ip]),
     "scarl_write_sample_h5": (C.c_int, [_vp, C.c_char_p, C.c_char_p, _vp, C.c_int,
                                         C.POINTER(Sample), C.POINTER(Layout), C.c_int, C.c_int,
                                         C.c_char_p, _dp, C.c_int]),
@@ -113,7 +127,7 @@ SIGNATURES = {
                                         C.c_size_t]),
     "scarl_h5_read_attr": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _dp, C.c_int,
                                      C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
-    "scarl_axis_cov": (C.c_int, [_vp, _vp, C.c_int, _ip, C.c_int, _dp, _dp, _dp]),
+    "scarl_axis_cov": (C.c_int, [_vp, _vp, C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp]),
     "scarl_ensemble_draw": (C.c_int, [C.c_uint64, C.c_longlong, C.c_int, _ip, C.c_int, C.c_double,
                                       C.c_double, _ip, _dp]),
     "scarl_gen_ensemble": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _ip, _dp, _dp, C.c_int,

@@ -461,15 +461,17 @@ def rebuild_Sk(ctx, field, L, avg, stdDev, tukey_literal=True):
     return out
 
 
-def axis_cov(ctx, field, L, maxlag):
+def axis_cov(ctx, field, L, maxlag, known_mean=None):
     """Mean, variance and covariance (3, maxlag + 1) along each axis of one
-    field (numpy array or device tensor, column-major L), FP64 sums."""
+    field (numpy array or device tensor, column-major L), FP64 sums; the
+    lag products are centred by known_mean when given, else the sample mean."""
     L = [int(v) for v in L]
     cov = np.zeros(3 * (maxlag + 1))
     m, v = C.c_double(), C.c_double()
+    km = None if known_mean is None else C.byref(C.c_double(float(known_mean)))
     _check(lib().scarl_axis_cov(ctx.handle, _ptr(field), _dtype_of(field), _i3(L), int(maxlag),
-                                C.byref(m), C.byref(v), cov.ctypes.data_as(C.POINTER(C.c_double))),
-           ctx)
+                                km, C.byref(m), C.byref(v),
+                                cov.ctypes.data_as(C.POINTER(C.c_double))), ctx)
     return m.value, v.value, cov.reshape(3, maxlag + 1)
 
 

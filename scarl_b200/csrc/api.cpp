@@ -93,6 +93,11 @@ struct scarl_ctx {
   std::map<long long, int> tune;          // (dtype, pass, N) -> launch variant
   std::map<std::string, bool> tuned_shapes;
   EnsPlan* ens = nullptr;
+  // learned padding model: FP32 master parameters, Adam moments, gradient,
+  // BF16 copies
+  Buf mlp_p, mlp_m, mlp_v, mlp_g, mlp_wb;
+  bool mlp_ready = false;
+  int mlp_step = 0;
 };
 
 namespace {
@@ -997,6 +1002,72 @@ int shino_args(scarl_ctx* ctx, const int Np[3], const double xRange[3], const do
 // ===========================================================================
 // C ABI
 // ---------------------------------------------------------------------------
+// Learned padding: labels, features, the MLP's host side.
+// ---------------------------------------------------------------------------
+constexpr double kLearnTol = 0.01;       // covariance error the labels hold
+constexpr double kLearnMargin = 0.25;    // safety margin on predictions (log2 units)
+
+// Matern / Gaussian axis description for the label kernels.
+PadLabelIn label_in(int corrMod, double nu, double ell_pts, int N) {
+  PadLabelIn c;
+  c.N = N;
+  c.ell = ell_pts;
+  if (corrMod == SCARL_CM_GAUSSIAN) {
+    c.kind = 1;
+    c.nu = 0.0;
+    c.q = 0.0;
+  } else {
+    const double v = corrMod == SCARL_CM_EXPONENTIAL ? 0.5 : nu;
+    const double a = ell_pts * std::tgamma(v) / (2.0 * std::sqrt(M_PI) * std::tgamma(v + 0.5));
+    c.kind = 2;
+    c.nu = v;
+    c.q = 4.0 * M_PI * M_PI * a * a;
+  }
+  return c;
+}
+
+// Network inputs of one axis (16 values; the trained range is l/N in
+// [0.01, 0.3], N in [64, 256], nu in [0.3, 1.5]).
+void mlp_feat(int corrMod, double nu, double ell_pts, int N, float* f) {
+  for (int i = 0; i < kMlpIn; ++i) f[i] = 0.f;
+  const double r = ell_pts / (double)N;
+  f[0] = (float)(4.0 * r);
+  f[1] = (float)(std::log2(r) / 4.0);
+  f[2] = (float)(std::log2((double)N) - 7.0);
+  f[3] = (float)(std::log2(ell_pts) / 4.0);
+  f[4] = corrMod == SCARL_CM_GAUSSIAN ? 1.f : 0.f;
+  f[5] = corrMod == SCARL_CM_EXPONENTIAL ? 1.f : 0.f;
+  f[6] = corrMod == SCARL_CM_VON_KARMAN ? 1.f : 0.f;
+  f[7] = corrMod == SCARL_CM_VON_KARMAN ? (float)(nu - 0.9) : 0.f;
+}
+
+bool mlp_in_range(int corrMod, double nu, double ell_pts, int N) {
+  const double r = ell_pts / (double)N;
+  if (!(r >= 0.008 && r <= 0.32) || N < 48 || N > 320) return false;
+  if (corrMod == SCARL_CM_VON_KARMAN && !(nu >= 0.28 && nu <= 1.55)) return false;
+  return corrMod >= 1 && corrMod <= 3;
+}
+
+int mlp_alloc(scarl_ctx* ctx) {
+  for (Buf* b : {&ctx->mlp_p, &ctx->mlp_m, &ctx->mlp_v, &ctx->mlp_g})
+    RC(ensure(ctx, *b, (size_t)kMlpParams * 4));
+  RC(ensure(ctx, ctx->mlp_wb, (size_t)kMlpParams * 2));
+  return SCARL_OK;
+}
+
+// Inputs (FP32 host rows of 16) as BF16 on the device, in ctx->stage_in.
+int mlp_inputs(scarl_ctx* ctx, const float* X, int n, const void** dev) {
+  RC(ensure(ctx, ctx->stage_in2, (size_t)n * kMlpIn * 4));
+  RC(ensure(ctx, ctx->stage_in, (size_t)n * kMlpIn * 2));
+  CK(cudaMemcpyAsync(ctx->stage_in2.p, X, (size_t)n * kMlpIn * 4, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += (size_t)n * kMlpIn * 4;
+  CK(launch_to_bf16((const float*)ctx->stage_in2.p, ctx->stage_in.p, n * kMlpIn, ctx->stream));
+  ctx->launches += 1;
+  *dev = ctx->stage_in.p;
+  return SCARL_OK;
+}
+
+// ---------------------------------------------------------------------------
 // HDF5 / XDMF output of a sample (SRC_F/write_output.f90).
 // ---------------------------------------------------------------------------
 std::string f25(double v) {
@@ -1205,6 +1276,7 @@ int scarl_ctx_destroy(scarl_ctx* ctx) {
   for (auto& kv : ctx->twiddles) release(ctx, kv.second);
   for (auto& kv : ctx->dct_tabs) release(ctx, kv.second);
   ens_free(ctx);
+  for (Buf* b : {&ctx->mlp_p, &ctx->mlp_m, &ctx->mlp_v, &ctx->mlp_g, &ctx->mlp_wb}) release(ctx, *b);
   for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
   if (ctx->pin_ev) cudaEventDestroy(ctx->pin_ev);
   if (ctx->pin) cudaFreeHost(ctx->pin);
@@ -1483,6 +1555,251 @@ int scarl_stat_file(scarl_ctx* ctx, const char* res_path, const char* dset_name,
     out.push_back(*find(nme));
   out.insert(out.end(), stats.begin(), stats.end());
   if (h5::write_file(folder + "/STAT_" + fname, out, {}, &err)) return fail(ctx, SCARL_EIO, err);
+  return SCARL_OK;
+}
+
+// ---- learned padding ----
+int scarl_pad_labels(scarl_ctx* ctx, int n, const int* corrMod, const double* nu,
+                     const double* ell_pts, const int* N, int* P, int* W, int* saturated) {
+  RC(begin(ctx));
+  if (n < 1 || !corrMod || !ell_pts || !N || !P || !W) return fail(ctx, SCARL_EINVAL, "null argument");
+  std::vector<PadLabelIn> in(n);
+  for (int i = 0; i < n; ++i) {
+    if (N[i] < 2 || N[i] > 256 || !(ell_pts[i] > 0.0) || corrMod[i] < 1 || corrMod[i] > 3)
+      return fail(ctx, SCARL_EINVAL, "label inputs: N in [2, 256], l > 0, corrMod 1..3");
+    in[i] = label_in(corrMod[i], nu ? nu[i] : 0.5, ell_pts[i], N[i]);
+  }
+  RC(ensure(ctx, ctx->t1, (size_t)n * sizeof(PadLabelIn)));
+  RC(ensure(ctx, ctx->t2, (size_t)n * sizeof(PadLabelOut)));
+  CK(cudaMemcpyAsync(ctx->t1.p, in.data(), (size_t)n * sizeof(PadLabelIn), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += (size_t)n * sizeof(PadLabelIn);
+  {
+    Prof p(ctx, "k_pad_labels");
+    CK(launch_pad_labels((const PadLabelIn*)ctx->t1.p, (PadLabelOut*)ctx->t2.p, n, kLearnTol, ctx->stream));
+  }
+  std::vector<PadLabelOut> out(n);
+  CK(cudaMemcpyAsync(out.data(), ctx->t2.p, (size_t)n * sizeof(PadLabelOut), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->d2h += (size_t)n * sizeof(PadLabelOut);
+  for (int i = 0; i < n; ++i) {
+    P[i] = out[i].P;
+    W[i] = out[i].W;
+    if (saturated) saturated[i] = out[i].saturated;
+  }
+  return SCARL_OK;
+}
+
+int scarl_pad_error(scarl_ctx* ctx, int n, const int* corrMod, const double* nu,
+                    const double* ell_pts, const int* N, const int* P, double* err) {
+  RC(begin(ctx));
+  if (n < 1 || !corrMod || !ell_pts || !N || !P || !err) return fail(ctx, SCARL_EINVAL, "null argument");
+  std::vector<PadLabelIn> in(n);
+  for (int i = 0; i < n; ++i) {
+    if (N[i] < 2 || N[i] > 256 || P[i] < N[i] || P[i] > 8192 || !(ell_pts[i] > 0.0) || corrMod[i] < 1 || corrMod[i] > 3)
+      return fail(ctx, SCARL_EINVAL, "error inputs: N in [2, 256], N <= P <= 8192, l > 0");
+    in[i] = label_in(corrMod[i], nu ? nu[i] : 0.5, ell_pts[i], N[i]);
+  }
+  RC(ensure(ctx, ctx->t1, (size_t)n * (sizeof(PadLabelIn) + sizeof(int))));
+  RC(ensure(ctx, ctx->t2, (size_t)n * 8));
+  CK(cudaMemcpyAsync(ctx->t1.p, in.data(), (size_t)n * sizeof(PadLabelIn), cudaMemcpyHostToDevice, ctx->stream));
+  int* dP = (int*)((char*)ctx->t1.p + (size_t)n * sizeof(PadLabelIn));
+  CK(cudaMemcpyAsync(dP, P, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += (size_t)n * (sizeof(PadLabelIn) + sizeof(int));
+  {
+    Prof p(ctx, "k_pad_error");
+    CK(launch_pad_error((const PadLabelIn*)ctx->t1.p, dP, (double*)ctx->t2.p, n, ctx->stream));
+  }
+  CK(cudaMemcpyAsync(err, ctx->t2.p, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->d2h += (size_t)n * 8;
+  return SCARL_OK;
+}
+
+int scarl_mlp_features(int n, const int* corrMod, const double* nu, const double* ell_pts,
+                       const int* N, float* X) {
+  if (n < 0 || (n && (!corrMod || !ell_pts || !N || !X))) return SCARL_EINVAL;
+  for (int i = 0; i < n; ++i) {
+    if (!(ell_pts[i] > 0.0) || N[i] < 1) return SCARL_EINVAL;
+    mlp_feat(corrMod[i], nu ? nu[i] : 0.5, ell_pts[i], N[i], X + (size_t)i * kMlpIn);
+  }
+  return SCARL_OK;
+}
+
+int scarl_mlp_targets(int n, const double* ell_pts, const int* N, const int* P, const int* W,
+                      float* T) {
+  if (n < 0 || (n && (!ell_pts || !N || !P || !W || !T))) return SCARL_EINVAL;
+  for (int i = 0; i < n; ++i) {
+    const double d = std::max(1, P[i] - N[i] + 1);
+    T[2 * i] = (float)std::log2(d / ell_pts[i]);
+    T[2 * i + 1] = (float)std::log2((double)std::max(W[i], 1) / ell_pts[i]);
+  }
+  return SCARL_OK;
+}
+
+int scarl_mlp_init(scarl_ctx* ctx, uint64_t seed) {
+  RC(begin(ctx));
+  RC(mlp_alloc(ctx));
+  std::vector<float> p(kMlpParams, 0.f);
+  uint64_t st = seed * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+  auto next = [&]() {  // splitmix64
+    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  auto normal = [&]() {
+    const double u1 = ((next() >> 11) + 0.5) * 0x1p-53, u2 = ((next() >> 11) + 0.5) * 0x1p-53;
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2);
+  };
+  const int H = kMlpHidden, I = kMlpIn, O = kMlpOut;
+  size_t o = 0;
+  for (int i = 0; i < H * I; ++i) p[o++] = (float)(normal() * std::sqrt(2.0 / 8.0));  // 8 live inputs
+  o += H;
+  for (int i = 0; i < H * H; ++i) p[o++] = (float)(normal() * std::sqrt(2.0 / H));
+  o += H;
+  for (int i = 0; i < O * H; ++i) p[o++] = (float)(normal() * std::sqrt(1.0 / H));
+  CK(cudaMemcpy(ctx->mlp_p.p, p.data(), (size_t)kMlpParams * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemset(ctx->mlp_m.p, 0, (size_t)kMlpParams * 4));
+  CK(cudaMemset(ctx->mlp_v.p, 0, (size_t)kMlpParams * 4));
+  CK(cudaMemset(ctx->mlp_g.p, 0, (size_t)kMlpParams * 4));
+  CK(launch_to_bf16((const float*)ctx->mlp_p.p, ctx->mlp_wb.p, kMlpParams, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->h2d += (size_t)kMlpParams * 4;
+  ctx->mlp_ready = true;
+  ctx->mlp_step = 0;
+  return SCARL_OK;
+}
+
+int scarl_mlp_params(scarl_ctx* ctx, float* get, const float* set) {
+  RC(begin(ctx));
+  if (set) {
+    RC(mlp_alloc(ctx));
+    CK(cudaMemcpy(ctx->mlp_p.p, set, (size_t)kMlpParams * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemset(ctx->mlp_m.p, 0, (size_t)kMlpParams * 4));
+    CK(cudaMemset(ctx->mlp_v.p, 0, (size_t)kMlpParams * 4));
+    CK(cudaMemset(ctx->mlp_g.p, 0, (size_t)kMlpParams * 4));
+    CK(launch_to_bf16((const float*)ctx->mlp_p.p, ctx->mlp_wb.p, kMlpParams, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->mlp_ready = true;
+    ctx->mlp_step = 0;
+  }
+  if (get) {
+    if (!ctx->mlp_ready) return fail(ctx, SCARL_EINVAL, "no model: call scarl_mlp_init or set parameters");
+    CK(cudaMemcpy(get, ctx->mlp_p.p, (size_t)kMlpParams * 4, cudaMemcpyDeviceToHost));
+  }
+  return SCARL_OK;
+}
+
+int scarl_mlp_grad(scarl_ctx* ctx, const float* X, const float* T, int n, float* grad, double* loss) {
+  RC(begin(ctx));
+  if (!ctx->mlp_ready) return fail(ctx, SCARL_EINVAL, "no model");
+  if (n < 1 || !X || !T || !grad || !loss) return fail(ctx, SCARL_EINVAL, "null argument");
+  const void* xb;
+  RC(mlp_inputs(ctx, X, n, &xb));
+  RC(ensure(ctx, ctx->tile, (size_t)n * kMlpOut * 4));
+  CK(cudaMemcpyAsync(ctx->tile.p, T, (size_t)n * kMlpOut * 4, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += (size_t)n * kMlpOut * 4;
+  RC(ensure(ctx, ctx->part, 8));
+  CK(cudaMemsetAsync(ctx->part.p, 0, 8, ctx->stream));
+  CK(cudaMemsetAsync(ctx->mlp_g.p, 0, (size_t)kMlpParams * 4, ctx->stream));
+  {
+    Prof p(ctx, "k_mlp_train");
+    CK(launch_mlp_train(xb, (const float*)ctx->tile.p, n, ctx->mlp_wb.p, (const float*)ctx->mlp_p.p,
+                        (float*)ctx->mlp_g.p, (double*)ctx->part.p, ctx->stream));
+  }
+  CK(cudaMemcpyAsync(grad, ctx->mlp_g.p, (size_t)kMlpParams * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(loss, ctx->part.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemsetAsync(ctx->mlp_g.p, 0, (size_t)kMlpParams * 4, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SCARL_OK;
+}
+
+int scarl_mlp_train(scarl_ctx* ctx, const float* X, const float* T, int n, int steps, float lr,
+                    double* loss_hist) {
+  RC(begin(ctx));
+  if (!ctx->mlp_ready) return fail(ctx, SCARL_EINVAL, "no model: call scarl_mlp_init first");
+  if (n < 1 || steps < 1 || !X || !T || !(lr > 0.f)) return fail(ctx, SCARL_EINVAL, "bad training arguments");
+  const void* xb;
+  RC(mlp_inputs(ctx, X, n, &xb));
+  RC(ensure(ctx, ctx->tile, (size_t)n * kMlpOut * 4));
+  CK(cudaMemcpyAsync(ctx->tile.p, T, (size_t)n * kMlpOut * 4, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d += (size_t)n * kMlpOut * 4;
+  RC(ensure(ctx, ctx->part, (size_t)steps * 8));
+  CK(cudaMemsetAsync(ctx->part.p, 0, (size_t)steps * 8, ctx->stream));
+  CK(cudaMemsetAsync(ctx->mlp_g.p, 0, (size_t)kMlpParams * 4, ctx->stream));
+  for (int t = 0; t < steps; ++t) {
+    {
+      Prof p(ctx, "k_mlp_train");
+      CK(launch_mlp_train(xb, (const float*)ctx->tile.p, n, ctx->mlp_wb.p, (const float*)ctx->mlp_p.p,
+                          (float*)ctx->mlp_g.p, (double*)ctx->part.p + t, ctx->stream));
+    }
+    Prof p(ctx, "k_mlp_adam");
+    CK(launch_mlp_adam((float*)ctx->mlp_p.p, (float*)ctx->mlp_g.p, (float*)ctx->mlp_m.p,
+                       (float*)ctx->mlp_v.p, ctx->mlp_wb.p, lr, ++ctx->mlp_step, ctx->stream));
+  }
+  if (loss_hist) {
+    CK(cudaMemcpyAsync(loss_hist, ctx->part.p, (size_t)steps * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->d2h += (size_t)steps * 8;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SCARL_OK;
+}
+
+int scarl_mlp_predict(scarl_ctx* ctx, const float* X, int n, float* Y) {
+  RC(begin(ctx));
+  if (!ctx->mlp_ready) return fail(ctx, SCARL_EINVAL, "no model");
+  if (n < 1 || !X || !Y) return fail(ctx, SCARL_EINVAL, "null argument");
+  const void* xb;
+  RC(mlp_inputs(ctx, X, n, &xb));
+  RC(ensure(ctx, ctx->tile, (size_t)n * kMlpOut * 4));
+  {
+    Prof p(ctx, "k_mlp_infer");
+    CK(launch_mlp_infer(xb, n, ctx->mlp_wb.p, (const float*)ctx->mlp_p.p, (float*)ctx->tile.p, ctx->stream));
+  }
+  CK(cudaMemcpyAsync(Y, ctx->tile.p, (size_t)n * kMlpOut * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->d2h += (size_t)n * kMlpOut * 4;
+  return SCARL_OK;
+}
+
+int scarl_pad_size_learned(scarl_ctx* ctx, int corrMod, double nu, const double corrL[3],
+                           const double xStep[3], const int Np[3], int P[3], int W[3],
+                           int* fallback) {
+  RC(begin(ctx));
+  if (!corrL || !xStep || !Np || !P) return fail(ctx, SCARL_EINVAL, "null argument");
+  int full[3];
+  RC(pad_size(SCARL_PAD_FULL, corrMod, nu, corrL, xStep, Np, 0.0, full) == SCARL_OK ? SCARL_OK : SCARL_EINVAL);
+  double ell[3];
+  bool ok = ctx->mlp_ready;
+  float X[3 * kMlpIn], Y[3 * kMlpOut];
+  for (int d = 0; d < 3; ++d) {
+    ell[d] = corrL[d] / xStep[d];
+    ok = ok && mlp_in_range(corrMod, nu, ell[d], Np[d]);
+    mlp_feat(corrMod, nu, ell[d], Np[d], X + d * kMlpIn);
+  }
+  if (ok) RC(scarl_mlp_predict(ctx, X, 3, Y));
+  int fb = ok ? 0 : 1;
+  for (int d = 0; d < 3; ++d) {
+    if (!ok) {
+      P[d] = full[d];
+      if (W) W[d] = Np[d];
+      continue;
+    }
+    const double D = ell[d] * std::exp2((double)Y[2 * d] + kLearnMargin);
+    const double need = (double)Np[d] - 1.0 + std::ceil(D);
+    int p2 = 8;
+    while ((double)p2 < need || p2 < Np[d]) p2 <<= 1;
+    if (p2 > full[d] || !std::isfinite(D)) {
+      p2 = full[d];
+      fb |= 2;
+    }
+    P[d] = p2;
+    if (W) {
+      const double w = std::ceil(ell[d] * std::exp2((double)Y[2 * d + 1] + kLearnMargin));
+      W[d] = (int)std::min<double>((double)Np[d], std::max(2.0, std::isfinite(w) ? w : (double)Np[d]));
+    }
+  }
+  if (fallback) *fallback = fb;
   return SCARL_OK;
 }
 
@@ -2000,8 +2317,11 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   if (gen == SCARL_GEN_PADDED) {
     int Pp[3];
     const double tol = o.pad_tol > 0.0 ? o.pad_tol : 1e-3;
-    if (pad_size(o.pad_policy, s->corrMod, s->nu, s->corrL, lay.xStep, lay.Np, tol, Pp) != SCARL_OK)
+    if (o.pad_policy == SCARL_PAD_LEARNED) {
+      RC(scarl_pad_size_learned(ctx, s->corrMod, s->nu, s->corrL, lay.xStep, lay.Np, Pp, nullptr, nullptr));
+    } else if (pad_size(o.pad_policy, s->corrMod, s->nu, s->corrL, lay.xStep, lay.Np, tol, Pp) != SCARL_OK) {
       return fail(ctx, SCARL_EINVAL, "invalid padding policy or tolerance");
+    }
     for (int d = 0; d < 3; ++d) P[d] = o.pad[d] > 0 ? o.pad[d] : Pp[d];
     RC(check_grid(ctx, P, lay.Np));
     for (int d = 0; d < 3; ++d)
@@ -2232,7 +2552,7 @@ int scarl_moments(scarl_ctx* ctx, const void* field, int dtype, long long xN, in
 }
 
 int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
-                   double* mean, double* var, double* cov) {
+                   const double* known_mean, double* mean, double* var, double* cov) {
   RC(begin(ctx));
   if (!field || !L || !mean || !var || !cov) return fail(ctx, SCARL_EINVAL, "null argument");
   if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
@@ -2261,7 +2581,8 @@ int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3],
   ctx->d2h += h.size() * 8;
   double s1 = 0.0;
   for (int b = 0; b < nb; ++b) s1 += h[2 * (size_t)b];
-  const double mu = s1 / (double)n;
+  const double sample_mean = s1 / (double)n;
+  const double mu = known_mean ? *known_mean : sample_mean;
   // per axis: power pass, FP64 lag sums
   const int H = maxlag + 1;
   int nblk[3];
@@ -2299,7 +2620,7 @@ int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3],
       const double pairs = (double)(L[d] - lag) * (double)(n / (size_t)L[d]);
       cov[(size_t)d * H + lag] = hs[(size_t)d * H + lag] / pairs;
     }
-  *mean = mu;
+  *mean = sample_mean;
   *var = cov[0];
   return SCARL_OK;
 }

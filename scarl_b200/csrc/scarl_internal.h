@@ -153,4 +153,29 @@ cudaError_t launch_axis_power(int dt, const void* f, const int L[3], int dir, in
 cudaError_t launch_cov_lags(const double* partial, int nblocks, int N, int maxlag,
                             const double* tw64, double* bins, double* S, cudaStream_t s);
 
+// Learned padding (mlp.cu).  One axis of one configuration: kind 1 =
+// Gaussian, 2 = Matern (nu; exponential is nu = 1/2); ell in grid points;
+// q = 4 pi^2 a^2 (Matern).  N <= 256.
+struct PadLabelIn {
+  int kind, N;
+  double ell, nu, q;
+};
+struct PadLabelOut {
+  int P, W, saturated;
+};
+cudaError_t launch_pad_labels(const PadLabelIn* in, PadLabelOut* out, int n, double tol,
+                              cudaStream_t s);
+cudaError_t launch_pad_error(const PadLabelIn* in, const int* P, double* err, int n,
+                             cudaStream_t s);
+constexpr int kMlpIn = 16, kMlpHidden = 64, kMlpOut = 2;
+constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpHidden * kMlpHidden +
+                           kMlpHidden + kMlpOut * kMlpHidden + kMlpOut;
+cudaError_t launch_mlp_train(const void* X, const float* T, int n, const void* wb, const float* p,
+                             float* grad, double* loss, cudaStream_t s);
+cudaError_t launch_mlp_infer(const void* X, int n, const void* wb, const float* p, float* Y,
+                             cudaStream_t s);
+cudaError_t launch_mlp_adam(float* p, float* g, float* m, float* v, void* wb, float lr, int t,
+                            cudaStream_t s);
+cudaError_t launch_to_bf16(const float* a, void* b, int n, cudaStream_t s);
+
 }  // namespace scarl

@@ -93,3 +93,14 @@ def test_large_field_covariance_within_monte_carlo_bounds(ctx):
         kap = _blend_kappa(int(lay["Np"][d]), int(lay["Np_ovlp"][d]), int(lay["topo"][d]), L[d], H)
         target = kap * np.exp(-np.pi * h * h / (l * l))
         assert np.max(np.abs(cov[d] - target)) < 0.03, d
+
+
+def test_axis_cov_known_mean(ctx):
+    f = _field((30, 20, 16), 9, 1.0)
+    _, _, c = S.axis_cov(ctx, f, f.shape, 6, known_mean=0.25)
+    g = f - 0.25
+    for d, n in enumerate(f.shape):
+        for h in range(7):
+            a = np.take(g, range(0, n - h), axis=d)
+            b = np.take(g, range(h, n), axis=d)
+            assert c[d, h] == pytest.approx(np.mean(a * b), rel=1e-11, abs=1e-12)

@@ -1,0 +1,90 @@
+"""Learned padding on the GPU: labels and errors against the CPU oracle, the
+MLP's gradients against the oracle's BF16 network, training, the held-out
+gain over full padding, and the Monte Carlo judge.  Tolerances: labels
+exact (or at a tie of the error with the 1 % threshold), errors rel 1e-9,
+gradients rel-L2 2e-3 per tensor (FP32 vs FP64 sums under BF16 rounding)."""
+import numpy as np
+import pytest
+
+import scarl_b200 as S
+import scarl_b200.learned as L
+from oracle import mlp as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _axes(n, seed):
+    cm, nu, N, ell = L.sample_configs(n, seed)
+    return L._axes(cm, nu, N, ell)
+
+
+def test_labels_and_errors_match_oracle(ctx):
+    cm, nu, ell, N = _axes(10, 5)
+    P, W, sat = L.labels(ctx, cm, nu, ell, N)
+    for i in range(len(cm)):
+        rP, rW, rs, err = M.labels(int(cm[i]), float(nu[i]), float(ell[i]), int(N[i]))
+        assert sat[i] == rs
+        if P[i] != rP:  # only at a tie of the error with the threshold
+            assert abs(err(min(P[i], rP)) - 0.01) < 1e-9, (i, P[i], rP)
+        assert abs(int(W[i]) - rW) <= 1, (i, W[i], rW)
+    Pq = np.maximum(N, (N * np.linspace(1.0, 3.0, len(N))).astype(np.int32))
+    e = L.pad_error(ctx, cm, nu, ell, N, Pq)
+    for i in range(0, len(cm), 3):
+        ref = M.pad_error(int(cm[i]), float(nu[i]), float(ell[i]), int(N[i]), int(Pq[i]))
+        assert e[i] == pytest.approx(ref, rel=1e-9, abs=1e-13)
+
+
+def test_gradients_match_the_oracle(ctx):
+    L.init(ctx, 11)
+    p = L.get_params(ctx).astype(np.float64)
+    cm, nu, ell, N = _axes(70, 6)  # 210 samples: three blocks, a ragged tail
+    X = L.features(cm, nu, ell, N)
+    T = np.random.default_rng(0).standard_normal((len(X), 2)).astype(np.float32)
+    g, loss = L.grad(ctx, X, T)
+    rl, rg = M.mlp_forward_backward(p, X, T)
+    assert loss == pytest.approx(rl, rel=1e-4)
+    off = np.cumsum([0, 64 * 16, 64, 64 * 64, 64, 2 * 64, 2])
+    for a, b in zip(off[:-1], off[1:]):
+        ref = rg[a:b]
+        assert np.linalg.norm(g[a:b] - ref) <= 2e-3 * np.linalg.norm(ref) + 1e-7, (a, b)
+
+
+@pytest.fixture(scope="module")
+def trained(ctx):
+    return L.fit(ctx, n_train=4096, seed=1, steps=3000, lr=3e-3)
+
+
+def test_training_and_held_out_gain_over_full_padding(ctx, trained):
+    loss = trained["loss"]
+    assert loss[-1] < 0.05 * loss[0] and loss[-1] < 0.05
+    ev = L.evaluate(ctx, n_test=512, seed=2)
+    print({k: v for k, v in ev.items() if not isinstance(v, np.ndarray)})
+    assert ev["volume_reduction"] >= 0.30          # FFT volume cut vs full padding
+    assert ev["frac_axes_within_1pct"] >= 0.99     # covariance error held
+    assert ev["max_cov_error_learned"] <= 0.02
+    # the learned policy through the generator
+    s = S.make_sample((0, 0, 0), (99, 79, 63), (6, 9, 4), (0, 0, 0), (7, 10, 5), corrMod=3)
+    a, lay = S.generate_sample(ctx, s, dtype=S.F64, pad_policy=S.PAD_LEARNED)
+    P, W, fb = L.pad_size_learned(ctx, 3, 0.5, (6, 9, 4), lay["xStep"], lay["Np"])
+    b, _ = S.generate_sample(ctx, s, dtype=S.F64, pad=P)
+    np.testing.assert_array_equal(a, b)
+    assert fb == 0 and np.all(P <= L.full_pad(lay["Np"]))
+
+
+def test_monte_carlo_judge(ctx, trained):
+    """64 realisations at the learned and at the full padding: the measured
+    covariance error of the learned grid stays within 1 % (plus 4 standard
+    errors) of the full grid's."""
+    for cm, nu, ell, N in ((3, 0.5, (14.0, 6.0, 9.0), (64, 70, 64)),
+                           (1, 0.0, (12.0, 5.0, 16.0), (64, 64, 72)),
+                           (2, 1.1, (10.0, 15.0, 4.0), (72, 64, 64))):
+        P, _, fb = L.pad_size_learned(ctx, cm, nu, ell, (1, 1, 1), N)
+        Pf = L.full_pad(N)
+        H = min(N) - 1
+        ref = np.array([M.method_cov(cm, nu, ell[d], N[d], 32 * N[d])[:H + 1] for d in range(3)])
+        ml, sl = L.judge(ctx, cm, nu, ell, N, P)
+        mf, sf = L.judge(ctx, cm, nu, ell, N, Pf)
+        el = np.max(np.abs(ml - ref))
+        ef = np.max(np.abs(mf - ref))
+        assert el <= ef + 0.01 + 4 * max(sl.max(), sf.max()), (cm, P, Pf, el, ef)
+        assert np.prod(P) <= np.prod(Pf)
