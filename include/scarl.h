@@ -51,6 +51,14 @@ extern "C" {
 /* ---- precisions ---- */
 #define SCARL_F32 4
 #define SCARL_F64 8
+/* Flag OR'ed into SCARL_F32 for the padded generator (scarl_gen_padded,
+ * scarl_generate_sample's opts.dtype): the z-axis DFT of pass 1 runs on the
+ * tensor cores as split-BF16 matrix products (head + tail of every operand,
+ * three products, FP32 accumulation), a field error near 4e-6 relative L2
+ * against FP64 (bounded by 1e-5).  Padded z lengths without a tensor-core
+ * kernel, and injected or literal spectra, run the FP32 pass instead.  No
+ * counterpart in the reference. */
+#define SCARL_SPLIT_BF16 0x100
 
 /* ---- generators for scarl_generate_sample ---- */
 #define SCARL_GEN_DCT 1      /* gen_std_gauss_FFT, SRC_F/fftw_ScaRL.f90:261 */

@@ -30,7 +30,7 @@ def _d3(v):
 
 
 def _np_dtype(dtype):
-    return np.float32 if dtype == F32 else np.float64
+    return np.float64 if (dtype & 0xFF) == F64 else np.float32
 
 
 def _ptr(a):

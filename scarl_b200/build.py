@@ -15,8 +15,8 @@ LIB = os.path.join(HERE, "libscarl_b200.so")
 OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-CUDA_SOURCES = ["gen_padded.cu", "dct_literal.cu", "post.cu", "stats.cu", "cov.cu", "mlp.cu",
-                "noalloc.cu"]
+CUDA_SOURCES = ["gen_padded.cu", "gen_tc.cu", "dct_literal.cu", "post.cu", "stats.cu", "cov.cu",
+                "mlp.cu", "noalloc.cu"]
 # gen_inst.cu once per (precision, line-length group): the generator pass
 # instantiations compile in parallel
 INSTANCES = [(dt, n) for dt in (4, 8) for n in (0, 256, 512, 1024, 2048)]

@@ -77,6 +77,7 @@ struct scarl_ctx {
   size_t budget = 0, used = 0;
   std::string err;
   Buf work, tile, stage_out, stage_in, stage_in2, tabs, dtabs, part, t1, t2, sk, pmpw;
+  Buf status;  // device word raised by kernels whose bounded waits expired
   void* pin = nullptr;
   size_t pin_n = 0;
   cudaEvent_t pin_ev = nullptr;
@@ -256,13 +257,35 @@ int out_dev(scarl_ctx* ctx, void* user, size_t bytes, void** dev, bool* host) {
   return SCARL_OK;
 }
 
+// Reads and clears the device status word (the stream must be idle).
+int check_status(scarl_ctx* ctx) {
+  if (!ctx->status.p) return SCARL_OK;
+  int st = 0;
+  CK(cudaMemcpy(&st, ctx->status.p, sizeof st, cudaMemcpyDeviceToHost));
+  if (st == 0) return SCARL_OK;
+  CK(cudaMemset(ctx->status.p, 0, sizeof st));
+  return fail(ctx, SCARL_ETIMEOUT, "a bounded tensor-core wait expired; the output is invalid");
+}
+
 int finish_out(scarl_ctx* ctx, void* user, const void* dev, size_t bytes, bool host) {
   if (host) {
     CK(cudaMemcpyAsync(user, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     ctx->d2h += bytes;
     CK(cudaStreamSynchronize(ctx->stream));
+    RC(check_status(ctx));
   }
   CK(cudaGetLastError());
+  return SCARL_OK;
+}
+
+// dtype argument of the padded generator: SCARL_F32 / SCARL_F64, optionally
+// SCARL_F32 | SCARL_SPLIT_BF16.
+int parse_dtype(scarl_ctx* ctx, int dtype, int* dt, int* split) {
+  *split = (dtype & SCARL_SPLIT_BF16) ? 1 : 0;
+  *dt = dtype & ~SCARL_SPLIT_BF16;
+  if (*dt != SCARL_F32 && *dt != SCARL_F64)
+    return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64 (SCARL_F32 | SCARL_SPLIT_BF16)");
+  if (*split && *dt != SCARL_F32) return fail(ctx, SCARL_EINVAL, "SCARL_SPLIT_BF16 applies to SCARL_F32 only");
   return SCARL_OK;
 }
 
@@ -470,7 +493,8 @@ int32_t schrage(int32_t seed) {
 
 int run_passes(scarl_ctx* ctx, int dt, const GenArgs& a) {
   {
-    Prof p(ctx, "k_gen_z");
+    const bool tc = a.split && dt == 4 && a.spec == SPEC_PHILOX && gen_z_tc_supported(a.P[2]);
+    Prof p(ctx, tc ? "k_gen_z_tc" : "k_gen_z");
     CK(launch_gen_pass(dt, 1, a, ctx->stream));
   }
   {
@@ -529,6 +553,11 @@ int gen_args(scarl_ctx* ctx, int dt, const int P[3], const int Np[3], GenArgs* a
   }
   a->Hx = P[0] / 2 + 1;
   a->Hpad = round_up(a->Hx, 16);
+  if (!ctx->status.p) {
+    RC(ensure(ctx, ctx->status, 16));
+    CK(cudaMemset(ctx->status.p, 0, 16));
+  }
+  a->status = (int*)ctx->status.p;
   const size_t wbytes = (size_t)a->Hpad * P[1] * Np[2] * 2 * dt;
   RC(ensure(ctx, ctx->work, wbytes));
   a->work = ctx->work.p;
@@ -1270,7 +1299,8 @@ int scarl_ctx_destroy(scarl_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   flush_marks(ctx);
   for (Buf* b : {&ctx->work, &ctx->tile, &ctx->stage_out, &ctx->stage_in, &ctx->stage_in2,
-                 &ctx->tabs, &ctx->dtabs, &ctx->part, &ctx->t1, &ctx->t2, &ctx->sk, &ctx->pmpw})
+                 &ctx->tabs, &ctx->dtabs, &ctx->part, &ctx->t1, &ctx->t2, &ctx->sk, &ctx->pmpw,
+                 &ctx->status})
     release(ctx, *b);
   for (auto& kv : ctx->plans) release(ctx, kv.second.tabs);
   for (auto& kv : ctx->twiddles) release(ctx, kv.second);
@@ -1305,6 +1335,7 @@ int scarl_sync(scarl_ctx* ctx) {
   RC(begin(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
+  RC(check_status(ctx));
   return SCARL_OK;
 }
 
@@ -2120,12 +2151,13 @@ int scarl_gen_std_gauss_shino_fft(scarl_ctx* ctx, double* data, const int Np[3],
   return finish_out(ctx, data, dev, n * 8, host);
 }
 
-int scarl_gen_padded(scarl_ctx* ctx, void* out, int dtype, const int Np[3], const int pad[3],
+int scarl_gen_padded(scarl_ctx* ctx, void* out, int dtype_in, const int Np[3], const int pad[3],
                      const double xStep[3], const double corrL[3], int corrMod, double nu,
                      int normalise, uint64_t seed, uint32_t stream, const void* xi) {
   RC(begin(ctx));
   if (!out || !Np || !xStep || !corrL) return fail(ctx, SCARL_EINVAL, "null argument");
-  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  int dtype, split;
+  RC(parse_dtype(ctx, dtype_in, &dtype, &split));
   if (corrMod < 1 || corrMod > 3) return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
   if (corrMod == SCARL_CM_VON_KARMAN && !(nu > 0.0)) return fail(ctx, SCARL_EINVAL, "nu must be > 0");
   int P[3];
@@ -2143,6 +2175,7 @@ int scarl_gen_padded(scarl_ctx* ctx, void* out, int dtype, const int Np[3], cons
   GenArgs a;
   RC(gen_args(ctx, dtype, P, Np, &a));
   set_plan(&a, pl);
+  a.split = split;
   a.k0 = (uint32_t)seed;
   a.k1 = (uint32_t)(seed >> 32);
   a.stream = stream;
@@ -2252,8 +2285,8 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   std::memset(&o, 0, sizeof o);
   if (o_in) o = *o_in;
   const int gen = o.generator ? o.generator : SCARL_GEN_PADDED;
-  const int dt = o.dtype ? o.dtype : SCARL_F32;
-  if (dt != SCARL_F32 && dt != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  int dt, split;
+  RC(parse_dtype(ctx, o.dtype ? o.dtype : SCARL_F32, &dt, &split));
   if (gen != SCARL_GEN_PADDED && dt != SCARL_F64)
     return fail(ctx, SCARL_EUNSUPPORTED, "the reference generators (DCT, Shino) run in FP64 only");
   const int gm = o.gen_meth ? o.gen_meth : SCARL_FFT;
@@ -2358,6 +2391,7 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
       GenArgs a;
       RC(gen_args(ctx, dt, P, lay.Np, &a));
       set_plan(&a, pl);
+      a.split = split;
       a.k0 = (uint32_t)seedStart;
       a.k1 = 0;
       a.stream = o.stream;

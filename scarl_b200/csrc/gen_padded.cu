@@ -39,6 +39,8 @@ static cudaError_t run_pass_dt(int dt, int pass, int v, const GenArgs& a, const 
 
 cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a, cudaStream_t s) {
   if (pass < 1 || pass > 3) return cudaErrorInvalidValue;
+  if (pass == 1 && a.split && dt == 4 && a.spec == SPEC_PHILOX && gen_z_tc_supported(a.P[2]))
+    return launch_gen_z_tc(a, s);
   return run_pass_dt(dt, pass, a.var[pass - 1], a, nullptr, nullptr, s);
 }
 

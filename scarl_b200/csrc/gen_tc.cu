@@ -1,0 +1,408 @@
+// gen_tc.cu -- pass 1 of the padded generator (spectrum synthesis + inverse
+// DFT along z) with the DFT on the tensor cores in split BF16: the FP32
+// output of scarl_gen_padded / scarl_generate_sample when the caller asks for
+// SCARL_F32 | SCARL_SPLIT_BF16.
+//
+// A line of N = N1 * N2 modes along z is transformed in two matrix stages
+// (the "four-step" factorisation, k = k1 + N1 k2, n = n2 + N2 n1):
+//   stage 1  Y[k1][n2] = sum_k2 x[k1 + N1 k2] e^{+2 pi i n2 k2 / N2}
+//   twiddle  Y'[k1][n2] = Y[k1][n2] e^{+2 pi i n2 k1 / N}          (FP32)
+//   stage 2  X[n2 + N2 n1] = sum_k1 Y'[k1][n2] e^{+2 pi i n1 k1 / N1}
+// Each stage is a real GEMM on interleaved re/im columns, D = A B^T with the
+// DFT matrix B = [[C, -S], [S, C]].  Every operand is split into a BF16 head
+// and a BF16 tail (h = bf16(v), t = bf16(v - h); v = h + t to 2^-17 |v|),
+// and D = Ah Bh + Ah Bt + At Bh accumulates in FP32 in tensor memory (the
+// dropped At Bt term is 2^-17 relative).  So each DFT stage carries about
+// 2^-17 relative error instead of FP32's 2^-24; the field's relative L2
+// error against FP64 stays near 4e-6 (tests bound it by 1e-5).
+//
+// Persistent CTAs of 256 threads, two per SM, walk work items of LB
+// consecutive lines (line l = kx + Hx ky, the Philox counter base of the
+// line's modes).  Per item: every thread synthesises one stage-1 row (LB N1
+// rows: line, k1) from the canonical Philox normals and amplitude tables and
+// stores it split into a K-major operand; one thread issues the stage-1
+// MMAs; each row comes back from tensor memory, is twiddled, split and
+// written into the stage-2 operand, which is MN-major with rows (line, n2)
+// so that a thread's 8 consecutive n2 form one 16-byte store; one thread
+// issues stage 2; the results pass through shared memory (z-major, padded
+// against bank conflicts) so that z < Nz leaves in 128-byte runs of
+// consecutive kx.  Every wait on the tensor core is bounded; on timeout the
+// kernel raises a status word and returns after freeing its tensor memory.
+#include <algorithm>
+
+#include "gen_kernels.cuh"
+#include "tc_sm100.cuh"
+
+namespace scarl {
+
+namespace {
+
+template <int N1_, int N2_, int LB_>
+struct TcCfg {
+  static constexpr int N1 = N1_, N2 = N2_, LB = LB_, N = N1 * N2;
+  static constexpr int THREADS = 256, CTAS_PER_SM = 2;
+  static constexpr int ROWS1 = LB * N1;  // stage-1 rows (line, k1)
+  static constexpr int ROWS2 = LB * N2;  // stage-2 rows (line, n2)
+  static constexpr int T1 = ROWS1 / 128, T2 = ROWS2 / 128;
+  static constexpr int K1 = 2 * N2, K2 = 2 * N1;  // real K (= MMA N) of each stage
+  // stage 1, K-major: 16-byte K chunks 128 B apart, 8-row groups SBO1 apart
+  static constexpr int LBO1 = 128, SBO1 = 128 * (K1 / 8), TILE1 = 16 * SBO1;
+  // stage 2 operand, MN-major: 8-row K groups LBO2 apart, 8-element M groups
+  // SBO2 apart; B2 K-major like stage 1
+  static constexpr int LBO2 = 128, SBO2 = 128 * (K2 / 8), TILE2 = 16 * SBO2;
+  static constexpr int A1B = T1 * TILE1, A2B = T2 * TILE2;
+  static constexpr int AB = A1B > A2B ? A1B : A2B;
+  static constexpr int STAGE_LD = LB + 1;  // output staging row (one z), float2 units
+  static constexpr int STAGEB = N * STAGE_LD * 8;
+  static constexpr int REGION = (2 * AB > STAGEB ? 2 * AB : STAGEB);
+  static constexpr int B1B = (K1 / 8) * SBO1, B2B = (K2 / 8) * SBO2;
+  static constexpr int TMEM_COLS = LB * N / 64;
+  static constexpr int OFF_AH = 0, OFF_AL = AB, OFF_B1H = REGION, OFF_B1L = OFF_B1H + B1B;
+  static constexpr int OFF_B2H = OFF_B1L + B1B, OFF_B2L = OFF_B2H + B2B;
+  static constexpr int OFF_ZT = OFF_B2L + B2B;   // z factor of the amplitude, N floats
+  static constexpr int OFF_TW = OFF_ZT + 4 * N;   // twiddles [n2][k1], N float2
+  static constexpr int OFF_BAR = OFF_TW + 8 * N;  // mbarrier (8 B) + tensor-memory slot (4 B)
+  static constexpr int SMEM = OFF_BAR + 16;
+  static_assert(ROWS1 == THREADS, "one stage-1 row per thread");
+  static_assert(N2 == 32, "a stage-2 row group of a line is one warp's 32 lanes");
+  static_assert(ROWS2 % 128 == 0 && T1 * K1 == TMEM_COLS && T2 * K2 == TMEM_COLS, "tiling");
+  static_assert(N1 % 8 == 0 && K1 <= 256 && K2 % 16 == 0, "radices");
+  static_assert(TMEM_COLS >= 32 && TMEM_COLS * CTAS_PER_SM <= 512 &&
+                (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory");
+  static_assert(CTAS_PER_SM * (SMEM + 1024) <= 228 * 1024, "shared memory");
+};
+
+constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s per tensor-core wait
+
+// The canonical Box-Muller pair of Normals<float> (u1 = (a + 1/2) 2^-32,
+// u2 = (b + 1/2) 2^-32, r (cos 2 pi u2, sin 2 pi u2), r = sqrt(-2 ln u1)) at
+// the split path's accuracy: r as t rsqrt(t) (0 at t = 0) and u2 from the top 23 bits of
+// b (phase error <= 2 pi 2^-24), both far below the 2^-17 of the BF16 split.
+__device__ __forceinline__ float2 split_normals(uint32_t a, uint32_t b) {
+  const float u1 = __fmaf_rn((float)a, 0x1p-32f, 0x1p-33f);
+  const float u2 = __uint_as_float(0x3F800000u | (b >> 9)) - 1.5f + 0x1p-24f;  // u2 - 1/2
+  const float t = -2.0f * __logf(u1);            // 0 when u1 rounds to 1
+  const float r = t * rsqrtf(fmaxf(t, 0x1p-100f));
+  float s, c;
+  __sincosf(6.28318530717958647692f * u2, &s, &c);
+  return make_float2(-r * c, -r * s);
+}
+
+// Byte offset of element (row, k) in a canonical K-major operand with
+// 16-byte K chunks 128 B apart and 8-row groups sbo apart (rows < 128).
+__device__ __forceinline__ uint32_t kmaj_off(int row, int k, int sbo) {
+  return (uint32_t)((row >> 3) * sbo + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// The split DFT matrix of length L as a (2L x 2L) K-major B operand:
+// row n = output (re n < L, im n >= L), column k = input (re / im).
+template <int L, int SBO>
+__device__ void fill_dft_b(unsigned char* hi, unsigned char* lo) {
+  for (int idx = threadIdx.x; idx < 4 * L * L; idx += blockDim.x) {
+    const int n = idx / (2 * L), k = idx % (2 * L);
+    const int no = n % L, ki = k % L;
+    const int m = (no * ki) % L;
+    double s, c;
+    sincospi(2.0 * (double)m / (double)L, &s, &c);
+    const bool im_out = n >= L, im_in = k >= L;
+    const double v = (im_out == im_in) ? c : (im_out ? s : -s);
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    const __nv_bfloat16 t = __double2bfloat16(v - (double)__bfloat162float(h));
+    const uint32_t off = kmaj_off(n, k, SBO);
+    *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
+    *reinterpret_cast<__nv_bfloat16*>(lo + off) = t;
+  }
+}
+
+template <int N1, int N2, int LB, int AMP>
+__global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
+  using Cfg = TcCfg<N1, N2, LB>;
+  constexpr int N = Cfg::N;
+  extern __shared__ __align__(128) unsigned char sm[];
+  unsigned char* AH = sm + Cfg::OFF_AH;
+  unsigned char* AL = sm + Cfg::OFF_AL;
+  const uint32_t sAH = tc::smem_u32(AH), sAL = tc::smem_u32(AL);
+  const uint32_t sB1H = tc::smem_u32(sm + Cfg::OFF_B1H), sB1L = tc::smem_u32(sm + Cfg::OFF_B1L);
+  const uint32_t sB2H = tc::smem_u32(sm + Cfg::OFF_B2H), sB2L = tc::smem_u32(sm + Cfg::OFF_B2L);
+  const uint32_t bar = tc::smem_u32(sm + Cfg::OFF_BAR);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + Cfg::OFF_BAR + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, q = warp & 3;
+
+  if (tid == 0) tc::mbar_init(bar, 1);
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(tslot), Cfg::TMEM_COLS);
+  fill_dft_b<N2, Cfg::SBO1>(sm + Cfg::OFF_B1H, sm + Cfg::OFF_B1L);
+  fill_dft_b<N1, Cfg::SBO2>(sm + Cfg::OFF_B2H, sm + Cfg::OFF_B2L);
+  float* zt = reinterpret_cast<float*>(sm + Cfg::OFF_ZT);
+  float2* tw2 = reinterpret_cast<float2*>(sm + Cfg::OFF_TW);
+  {
+    const float* zsrc = static_cast<const float*>(AMP == AMP_SEPARABLE ? a.az : a.qz);
+    const float2* tw = static_cast<const float2*>(a.tw_z);  // e^{2 pi i m / N}
+    for (int i = tid; i < N; i += Cfg::THREADS) {
+      zt[i] = zsrc[i];
+      tw2[i] = tw[(i / N1) * (i % N1)];  // [n2][k1] = e^{2 pi i n2 k1 / N}
+    }
+  }
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+
+  const int nlines = a.Hx * a.P[1];  // <= 1025 * 2048
+  const int nitems = (nlines + LB - 1) / LB;
+  const uint64_t mz = (uint64_t)a.Hx * (uint64_t)a.P[1];
+  const float* ax = static_cast<const float*>(a.ax);
+  const float* ay = static_cast<const float*>(a.ay);
+  const float* qx = static_cast<const float*>(a.qx);
+  const float* qy = static_cast<const float*>(a.qy);
+  float2* work = static_cast<float2*>(a.work);
+  const int Nz = a.Nout[2];
+  constexpr uint32_t ID1 = tc::idesc_bf16(128, Cfg::K1, false);
+  constexpr uint32_t ID2 = tc::idesc_bf16(128, Cfg::K2, true);  // A MN-major
+
+  // this thread's stage-1 row: (line, k1) with k1 = k1lo + 8 k1hi
+  const int R1 = tid;
+  const int s_line = (R1 >> 3) % LB, s_k1 = (R1 & 7) + 8 * (R1 / (8 * LB));
+  uint32_t phase = 0;
+  bool ok = true;
+
+  for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+    const int l0 = item * LB;
+    // ---- synthesis of stage-1 row R1 ----
+    {
+      const int l = l0 + s_line;
+      const bool valid = l < nlines;
+      const int ky = valid ? l / a.Hx : 0, kx = valid ? l - ky * a.Hx : 0;
+      float fx = 0.f, fy = 0.f;
+      if (valid) {
+        if (AMP == AMP_SEPARABLE) { fx = ax[kx] * ay[ky]; }
+        else { fx = ax[kx]; fy = 1.f + qx[kx] + qy[ky]; }
+      }
+      auto amp = [&](int kz) -> float {
+        if (AMP == AMP_SEPARABLE) return fx * zt[kz];
+        if (AMP == AMP_RECIP) return __fdividef(fx, fy + zt[kz]);
+        return fx * powf(fy + zt[kz], (float)a.expo);
+      };
+      const int tile = R1 >> 7, r = R1 & 127;
+      const uint32_t rowoff = (uint32_t)(tile * Cfg::TILE1 + (r >> 3) * Cfg::SBO1 + (r & 7) * 16);
+#pragma unroll 1
+      for (int j = 0; j < N2 / 16; ++j) {
+        float re0[8], im0[8], re1[8], im1[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int kz0 = s_k1 + N1 * (8 * j + e);
+          if (valid) {
+            const uint64_t c = (uint64_t)l + mz * (uint64_t)kz0;
+            const u32x4 o = philox4x32_10({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.k0, a.k1);
+            const float2 x0 = split_normals(o.x, o.y);
+            const float2 x1 = split_normals(o.z, o.w);
+            const float A0 = amp(kz0), A1 = amp(kz0 + N / 2);
+            re0[e] = A0 * x0.x; im0[e] = A0 * x0.y;
+            re1[e] = A1 * x1.x; im1[e] = A1 * x1.y;
+          } else {
+            re0[e] = im0[e] = re1[e] = im1[e] = 0.f;
+          }
+        }
+        // K chunks: re k2 in [8j, 8j+8) -> j, re k2 + N2/2 -> j + N2/16,
+        // im -> the same plus N2/8
+        auto put = [&](const float (&v)[8], int chunk) {
+          uint4 h, t;
+          tc::split2(v[0], v[1], h.x, t.x);
+          tc::split2(v[2], v[3], h.y, t.y);
+          tc::split2(v[4], v[5], h.z, t.z);
+          tc::split2(v[6], v[7], h.w, t.w);
+          const uint32_t off = rowoff + chunk * Cfg::LBO1;
+          *reinterpret_cast<uint4*>(AH + off) = h;
+          *reinterpret_cast<uint4*>(AL + off) = t;
+        };
+        put(re0, j);
+        put(re1, j + N2 / 16);
+        put(im0, N2 / 8 + j);
+        put(im1, N2 / 8 + N2 / 16 + j);
+      }
+    }
+    tc::fence_smem_to_async();
+    __syncthreads();
+    // ---- stage 1 on the tensor cores ----
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll 1
+      for (int t = 0; t < Cfg::T1; ++t) {
+#pragma unroll
+        for (int s = 0; s < Cfg::K1 / 16; ++s) {
+          const uint32_t ao = t * Cfg::TILE1 + s * 2 * Cfg::LBO1, bo = s * 2 * Cfg::LBO1;
+          const uint64_t ah = tc::desc(sAH + ao, Cfg::LBO1, Cfg::SBO1);
+          const uint64_t al = tc::desc(sAL + ao, Cfg::LBO1, Cfg::SBO1);
+          const uint64_t bh = tc::desc(sB1H + bo, Cfg::LBO1, Cfg::SBO1);
+          const uint64_t bl = tc::desc(sB1L + bo, Cfg::LBO1, Cfg::SBO1);
+          const uint32_t d = tmem + t * Cfg::K1;
+          tc::mma_bf16(d, ah, bh, ID1, s > 0 ? 1u : 0u);
+          tc::mma_bf16(d, ah, bl, ID1, 1u);
+          tc::mma_bf16(d, al, bh, ID1, 1u);
+        }
+      }
+      tc::commit(bar);
+    }
+    ok = warp == 0 ? tc::mbar_wait(bar, phase, kWaitNs) : true;  // one warp sleeps in the barrier
+    phase ^= 1;
+    if (!__syncthreads_and(ok)) { ok = false; break; }
+    tc::fence_after_sync();
+    // ---- stage-1 rows back, twiddled, split into the MN-major stage-2
+    //      operand: element (row n2 + N2 line, k) at
+    //      tile + (row % 128 / 8) SBO2 + (k / 8) LBO2 + (k % 8) 16 + (n2 % 8) 2,
+    //      k = k1 (re) or N1 + k1 (im) ----
+#pragma unroll 1
+    for (int t = warp >> 2; t < Cfg::T1; t += Cfg::THREADS / 128) {
+      const int R = t * 128 + q * 32 + lane;
+      const int line = (R >> 3) % LB, k1 = (R & 7) + 8 * (R / (8 * LB));
+      const float2* twk = tw2 + k1;  // e^{2 pi i n2 k1 / N} at twk[n2 N1]
+      const uint32_t row0 = (uint32_t)(N2 * line);
+      const uint32_t base = (row0 >> 7) * Cfg::TILE2 + ((row0 & 127) >> 3) * Cfg::SBO2 +
+                            (k1 >> 3) * Cfg::LBO2 + (k1 & 7) * 16;
+      constexpr uint32_t IM = (N1 / 8) * Cfg::LBO2;  // im K groups follow the re ones
+#pragma unroll
+      for (int g = 0; g < N2 / 16; ++g) {  // 16 n2 (two M groups) per tensor-memory read
+        float v[32];
+        const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + t * Cfg::K1 + g * 16;
+        tc::tmem_ld16(col, v);            // re of n2 = 16 g ..
+        tc::tmem_ld16(col + N2, v + 16);  // im
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {     // 8 n2 -> one 16-byte store per part
+          uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+          for (int e = 0; e < 8; e += 2) {
+            const int n2 = 16 * g + 8 * h + e;
+            const float2 w0 = twk[n2 * N1], w1 = twk[(n2 + 1) * N1];
+            const float xr0 = v[8 * h + e], xi0 = v[16 + 8 * h + e];
+            const float xr1 = v[8 * h + e + 1], xi1 = v[16 + 8 * h + e + 1];
+            const float yr0 = xr0 * w0.x - xi0 * w0.y, yi0 = xr0 * w0.y + xi0 * w0.x;
+            const float yr1 = xr1 * w1.x - xi1 * w1.y, yi1 = xr1 * w1.y + xi1 * w1.x;
+            tc::split2(yr0, yr1, rh[e / 2], rl[e / 2]);
+            tc::split2(yi0, yi1, ih[e / 2], il[e / 2]);
+          }
+          const uint32_t off = base + (uint32_t)(2 * g + h) * Cfg::SBO2;
+          *reinterpret_cast<uint4*>(AH + off) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+          *reinterpret_cast<uint4*>(AL + off) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+          *reinterpret_cast<uint4*>(AH + off + IM) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+          *reinterpret_cast<uint4*>(AL + off + IM) = make_uint4(il[0], il[1], il[2], il[3]);
+        }
+      }
+    }
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    // ---- stage 2 on the tensor cores ----
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll 1
+      for (int t = 0; t < Cfg::T2; ++t) {
+#pragma unroll
+        for (int s = 0; s < Cfg::K2 / 16; ++s) {
+          const uint32_t ao = t * Cfg::TILE2 + s * 2 * Cfg::LBO2, bo = s * 2 * Cfg::LBO1;
+          const uint64_t ah = tc::desc(sAH + ao, Cfg::LBO2, Cfg::SBO2);
+          const uint64_t al = tc::desc(sAL + ao, Cfg::LBO2, Cfg::SBO2);
+          const uint64_t bh = tc::desc(sB2H + bo, Cfg::LBO1, Cfg::SBO2);
+          const uint64_t bl = tc::desc(sB2L + bo, Cfg::LBO1, Cfg::SBO2);
+          const uint32_t d = tmem + t * Cfg::K2;
+          tc::mma_bf16(d, ah, bh, ID2, s > 0 ? 1u : 0u);
+          tc::mma_bf16(d, ah, bl, ID2, 1u);
+          tc::mma_bf16(d, al, bh, ID2, 1u);
+        }
+      }
+      tc::commit(bar);
+    }
+    ok = warp == 0 ? tc::mbar_wait(bar, phase, kWaitNs) : true;  // one warp sleeps in the barrier
+    phase ^= 1;
+    if (!__syncthreads_and(ok)) { ok = false; break; }
+    tc::fence_after_sync();
+    // ---- results X[n2 + N2 n1] of row (line, n2) into the z-major staging
+    //      area (the operand region, free now): stage[z][line] ----
+    float2* stage = reinterpret_cast<float2*>(sm);
+#pragma unroll 1
+    for (int t = warp >> 2; t < Cfg::T2; t += Cfg::THREADS / 128) {
+      const int line = (t * 128 + q * 32) / N2, n2 = lane;
+      float v[Cfg::K2];
+#pragma unroll
+      for (int c = 0; c < Cfg::K2 / 16; ++c)
+        tc::tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + t * Cfg::K2 + c * 16, v + c * 16);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1)
+        stage[(n2 + N2 * n1) * Cfg::STAGE_LD + line] = make_float2(v[n1], v[N1 + n1]);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    // ---- z < Nz to global memory, LB consecutive lines per z ----
+    {
+      const int line = tid % LB;
+      const int l = l0 + line;
+      const bool valid = l < nlines;
+      const int ky = valid ? l / a.Hx : 0, kx = valid ? l - ky * a.Hx : 0;
+      float2* dst = work + (size_t)ky * a.Hpad + kx;
+      const size_t zstride = (size_t)a.P[1] * a.Hpad;
+      if (valid)
+#pragma unroll 4
+        for (int z = tid / LB; z < Nz; z += Cfg::THREADS / LB)
+          dst[(size_t)z * zstride] = stage[z * Cfg::STAGE_LD + line];
+    }
+    __syncthreads();  // the staging area is the next item's operand region
+  }
+  if (!ok) {
+    // an MMA did not complete in time: report, then give it one more bounded
+    // wait before the tensor memory it writes is released
+    if (tid == 0) {
+      atomicOr(a.status, 1);
+      tc::mbar_wait(bar, phase ^ 1, kWaitNs);
+    }
+    __syncthreads();
+  }
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_free(tmem, Cfg::TMEM_COLS);
+}
+
+template <int N1, int N2, int LB, int AMP>
+cudaError_t launch_tc(const GenArgs& a, cudaStream_t s) {
+  using Cfg = TcCfg<N1, N2, LB>;
+  auto kern = k_gen_z_tc<N1, N2, LB, AMP>;
+  // per device: the shared-memory opt-in and the SM count
+  constexpr int kMaxDev = 64;
+  static int sms[kMaxDev] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  if (!sms[dev]) {
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM)) != cudaSuccess)
+      return e;
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+      return e;
+    int n = 0;
+    if ((e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    sms[dev] = n;
+  }
+  const int nitems = (a.Hx * a.P[1] + LB - 1) / LB;
+  // two resident CTAs per SM (registers, shared and tensor memory are sized for it)
+  const int grid = std::min(nitems, sms[dev] * Cfg::CTAS_PER_SM);
+  kern<<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// Line lengths with a tensor-core pass 1 (FP32 output, Philox spectrum).
+bool gen_z_tc_supported(int N) { return N == 512; }
+
+cudaError_t launch_gen_z_tc(const GenArgs& a, cudaStream_t s) {
+  if (!a.status || a.spec != SPEC_PHILOX) return cudaErrorInvalidValue;
+  switch (a.P[2]) {
+    case 512:
+      if (a.amp == AMP_SEPARABLE) return launch_tc<16, 32, 16, AMP_SEPARABLE>(a, s);
+      if (a.amp == AMP_RECIP) return launch_tc<16, 32, 16, AMP_RECIP>(a, s);
+      return launch_tc<16, 32, 16, AMP_POW>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace scarl

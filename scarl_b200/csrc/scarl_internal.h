@@ -72,6 +72,8 @@ struct GenArgs {
   double shino_f;
   Epilogue epi;
   int var[3];            // launch variant of each pass (autotuned, 0 = default)
+  int split;             // FP32: pass 1's z DFT on the tensor cores in split BF16
+  int* status;           // device word, bit 0 set when a bounded tensor-core wait expired
 };
 
 // One batched launch of a pass over several realisations that share the
@@ -92,6 +94,10 @@ cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a, cudaStream_t s);
 // and spectrum mode), v the launch variant.
 cudaError_t launch_gen_pass_batch(int dt, int pass, int v, const GenArgs& rep, const BatchMap& m,
                                   cudaStream_t s);
+// Pass 1 with the z-axis DFT as split-BF16 tensor-core matrix products
+// (gen_tc.cu): FP32, Philox spectrum, line lengths with gen_z_tc_supported.
+bool gen_z_tc_supported(int N);
+cudaError_t launch_gen_z_tc(const GenArgs& a, cudaStream_t s);
 // Blocks one realisation needs in a pass with launch variant v.
 int gen_pass_blocks(int dt, int pass, int v, const GenArgs& a);
 // Number of launch variants of a pass (valid ones depend on the line length).

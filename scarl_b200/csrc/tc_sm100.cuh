@@ -1,0 +1,148 @@
+// tc_sm100.cuh -- thin inline-PTX layer over the sm_100a tensor-core path
+// (tcgen05): tensor-memory allocation, BF16 MMAs with FP32 accumulators in
+// tensor memory, completion through an mbarrier, tensor-memory loads, and the
+// fences that order them against ordinary shared-memory stores.
+//
+// Operands live in shared memory in the canonical layouts without swizzle,
+// built from 128-byte core matrices.  K-major: a core matrix is 8 rows of 8
+// BF16 values along K; `lbo` is the byte distance between the two 16-byte K
+// chunks one MMA (K = 16) reads, `sbo` the distance between 8-row groups
+// along M (or N).  MN-major: a core matrix is 8 K rows of 8 BF16 values
+// along M; `lbo` is the distance between the two 8-row K groups one MMA
+// reads, `sbo` the distance between 8-element M groups.  D = A * B^T with A
+// (M x K) and B (N x K); for M = 128 row m of D sits in tensor-memory lane m.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace scarl {
+namespace tc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor: start address, leading / stride byte
+// offsets (16-byte units, 14 bits each), descriptor version 1 (bits 46-47),
+// base offset 0, no swizzle (bits 61-63 = 0).
+__device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A
+// and B (bits 7-9, 10-12 = 1), A MN-major if a_mn (bit 15), B K-major (bit
+// 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A * B^T, issued by one thread.
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+// Arrive on the mbarrier once every MMA this thread issued so far completes.
+__device__ __forceinline__ void commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Makes this thread's generic-proxy shared-memory stores visible to the
+// tensor core (async proxy).
+__device__ __forceinline__ void fence_smem_to_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Suspends until the phase of the given parity completes or about hint_ns
+// pass; true when it completed.
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase of the given parity to complete, for at most limit_ns
+// nanoseconds (the thread sleeps in the barrier, not in a busy loop); false
+// when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint64_t limit_ns) {
+  constexpr uint32_t kHint = 1000000u;  // 1 ms per suspension
+  if (mbar_try(mbar, parity, kHint)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try(mbar, parity, kHint))
+    if (global_ns() - t0 > limit_ns) return false;
+  return true;
+}
+
+// Tensor-memory allocation (one full warp calls; the base column address is
+// written to shared memory at slot).
+__device__ __forceinline__ void tmem_alloc(uint32_t slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t base, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(ncols)
+               : "memory");
+}
+
+// 16 consecutive 32-bit columns of the calling thread's lane (warp w reads
+// lanes 32 (w % 4) .. + 31; taddr carries the lane in bits 16-31).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Two-term BF16 split of a pair: hi = bf16(a, b), lo = bf16(residual); the
+// residual is exact in FP32, so a = hi + lo to within 2^-17 |a|.  Packed
+// with a in the low half (the lower K index in memory).
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+}  // namespace tc
+}  // namespace scarl

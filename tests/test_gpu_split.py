@@ -1,0 +1,87 @@
+"""Split-precision pass 1 (SCARL_F32 | SCARL_SPLIT_BF16): the z-axis DFT as
+BF16 head/tail tensor-core products with FP32 accumulation.  Checked against
+the FP64 oracle and the FP64 CUDA path on the same Philox normals.
+Tolerance: field rel-L2 <= 1e-5 against FP64 (the stated bound of the split
+form); the tensor-core kernel must be the one that ran."""
+import numpy as np
+import pytest
+
+import scarl_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+SPLIT = S.F32 | S.SPLIT_BF16
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    s = np.max(np.abs(b))
+    return np.linalg.norm((a - b) / s) / np.linalg.norm(b / s)
+
+
+def _ran_tc(ctx, fn):
+    ctx.profile(True)
+    ctx.profile_reset()
+    out = fn()
+    st = ctx.profile_stats()
+    ctx.profile(False)
+    return out, st
+
+
+@pytest.mark.parametrize("Np,P,dx,cl,cm,nu", [
+    ((12, 10, 300), (16, 16, 512), (1, 1, 1), (3, 3, 40), 3, 0.5),   # exponential
+    ((9, 7, 500), (16, 8, 512), (1, 1, 1), (2, 2, 30), 1, 0.5),       # Gaussian, ragged last item
+    ((20, 6, 267), (32, 16, 512), (0.5, 1, 1), (4, 3, 12), 2, 1.5),   # von Karman
+    ((5, 5, 512), (8, 8, 512), (1, 1, 1), (2, 2, 64), 3, 0.5),        # every z kept
+    ((6, 4, 1), (8, 8, 512), (1, 1, 1), (2, 2, 10), 3, 0.5),          # one z plane
+])
+def test_split_vs_oracle(ctx, oracle, Np, P, dx, cl, cm, nu):
+    ref = oracle.gen_padded(Np, P, dx, cl, cm, nu, 1, seed=77, stream=3)
+    out, st = _ran_tc(ctx, lambda: S.gen_padded(ctx, Np, dx, cl, cm, nu, pad=P, seed=77,
+                                                stream=3, dtype=SPLIT))
+    assert "k_gen_z_tc" in st and "k_gen_z" not in st
+    err = rel(out, ref)
+    print(f"split rel-L2 {err:.2e}, max {np.max(np.abs(out - ref)) / np.max(np.abs(ref)):.2e}")
+    assert err < TOL
+    out32 = S.gen_padded(ctx, Np, dx, cl, cm, nu, pad=P, seed=77, stream=3, dtype=S.F32)
+    assert rel(out32, ref) < err  # the split form is the coarser one
+
+
+def test_split_deterministic_and_seeded(ctx):
+    args = ((30, 20, 200), (1, 1, 1), (5, 5, 20), 3, 0.5)
+    a = S.gen_padded(ctx, *args, pad=(64, 32, 512), seed=4, dtype=SPLIT)
+    b = S.gen_padded(ctx, *args, pad=(64, 32, 512), seed=4, dtype=SPLIT)
+    c = S.gen_padded(ctx, *args, pad=(64, 32, 512), seed=5, dtype=SPLIT)
+    assert np.array_equal(a, b)
+    assert rel(a, c) > 0.5
+
+
+def test_split_other_lengths_use_fp32_pass(ctx, oracle):
+    Np, P = (10, 10, 100), (16, 16, 128)
+    ref = oracle.gen_padded(Np, P, (1, 1, 1), (3, 3, 10), 3, 0.5, 1, seed=2)
+    out, st = _ran_tc(ctx, lambda: S.gen_padded(ctx, Np, (1, 1, 1), (3, 3, 10), 3, pad=P, seed=2,
+                                                dtype=SPLIT))
+    assert "k_gen_z" in st and "k_gen_z_tc" not in st
+    assert rel(out, ref) < TOL
+
+
+def test_split_rejected_for_fp64(ctx):
+    with pytest.raises(S.ScarlError):
+        S.gen_padded(ctx, (8, 8, 8), (1, 1, 1), (2, 2, 2), 1, dtype=S.F64 | S.SPLIT_BF16)
+
+
+def test_split_blended_sample_vs_fp64(ctx):
+    """The headline deck (512^3 -> 513^3, exponential, l = (40, 20, 10),
+    lognormal mean 1 CV 0.3, 2x2x2 tiles, overlap 2 l) on the AUTO padded
+    grid 512^3: split FP32 against FP64 on the same normals."""
+    s = S.make_sample((0, 0, 0), (512, 512, 512), (40, 20, 10), (2, 2, 2), (41, 21, 11),
+                      corrMod=3, margiFirst=2, avg=1.0, std_dev=0.3)
+    kw = dict(nb_procs=8, topo=(2, 2, 2), pad_policy=S.PAD_AUTO)
+    f64, lay = S.generate_sample(ctx, s, dtype=S.F64, **kw)
+    (f32s, _), st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, dtype=SPLIT, **kw))
+    assert st["k_gen_z_tc"][1] == 8  # one launch per tile
+    err = rel(f32s, f64)
+    print(f"513^3 split rel-L2 {err:.2e}")
+    assert err < TOL
