@@ -2255,6 +2255,7 @@ int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* N
     }
   }
   if (changed) {
+    for (int i = 0; i < n; ++i) philox_schedule(&e->args[i]);
     const size_t bytes = (size_t)n * sizeof(GenArgs);
     void* pin;
     RC(pinned(ctx, bytes, &pin));

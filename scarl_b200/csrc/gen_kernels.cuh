@@ -123,7 +123,7 @@ __device__ __forceinline__ void gen_z_body(const GenArgs& a, int bx, int ky) {
           x1 = static_cast<const C*>(a.xi)[mrow + mz * (uint64_t)kz1];
         } else {
           const uint64_t c = mrow + mz * (uint64_t)kz0;
-          const u32x4 o = philox4x32_10({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.k0, a.k1);
+          const u32x4 o = philox4x32_10_ks({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.ks);
           x0 = Normals<T>::from(o.x, o.y);
           x1 = Normals<T>::from(o.z, o.w);
         }

@@ -37,8 +37,17 @@ static cudaError_t run_pass_dt(int dt, int pass, int v, const GenArgs& a, const 
                  : run_pass_t<float>(pass, v, a, bm, nb, s);
 }
 
-cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a, cudaStream_t s) {
+void philox_schedule(GenArgs* a) {
+  for (int r = 0; r < 10; ++r) {
+    a->ks[r] = a->k0 + (uint32_t)r * 0x9E3779B9u;
+    a->ks[10 + r] = a->k1 + (uint32_t)r * 0xBB67AE85u;
+  }
+}
+
+cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a_in, cudaStream_t s) {
   if (pass < 1 || pass > 3) return cudaErrorInvalidValue;
+  GenArgs a = a_in;
+  philox_schedule(&a);
   if (pass == 1 && a.split && dt == 4 && a.spec == SPEC_PHILOX && gen_z_tc_supported(a.P[2]))
     return launch_gen_z_tc(a, s);
   return run_pass_dt(dt, pass, a.var[pass - 1], a, nullptr, nullptr, s);

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
           const int kz0 = s_k1 + N1 * (8 * j + e);
           if (valid) {
             const uint64_t c = (uint64_t)l + mz * (uint64_t)kz0;
-            const u32x4 o = philox4x32_10({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.k0, a.k1);
+            const u32x4 o = philox4x32_10_ks({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.ks);
             const float2 x0 = split_normals(o.x, o.y);
             const float2 x1 = split_normals(o.z, o.w);
             const float A0 = amp(kz0), A1 = amp(kz0 + N / 2);

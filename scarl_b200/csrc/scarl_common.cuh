@@ -62,6 +62,26 @@ __device__ __forceinline__ u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1
   return c;
 }
 
+// The same with the round keys precomputed (ks[r] = k0 + r 0x9E3779B9,
+// ks[10 + r] = k1 + r 0xBB67AE85): kernels read them from their parameter
+// block instead of rebuilding the schedule per draw.
+__device__ __forceinline__ u32x4 philox4x32_10_ks(u32x4 c, const uint32_t* ks) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+    u32x4 n;
+    n.x = hi1 ^ c.y ^ ks[r];
+    n.y = lo1;
+    n.z = hi0 ^ c.w ^ ks[10 + r];
+    n.w = lo0;
+    c = n;
+  }
+  return c;
+}
+
 // Uniform in (0,1) from two 32-bit words: 52 random bits plus a half offset,
 // exactly representable, never 0 or 1.
 __device__ __forceinline__ double u01_d(uint32_t hi, uint32_t lo) {

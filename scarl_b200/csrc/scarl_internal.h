@@ -62,6 +62,7 @@ struct GenArgs {
   const void* qz;
   double expo;           // Matern: -(nu + 3/2) / 2
   uint32_t k0, k1, stream;
+  uint32_t ks[20];       // Philox round keys k0 + r C0 (r < 10), k1 + r C1 (philox_schedule)
   const void* xi;        // injected normal pairs (SPEC_INJECT)
   // literal Shino spectrum (FP64 tables)
   int sz[3];
@@ -86,6 +87,10 @@ struct BatchMap {
   int n;
   int total;             // start[n], the launch's grid size
 };
+
+// Fills a->ks from a->k0, a->k1 (the launchers call it; batched argument
+// blocks must have it filled before upload).
+void philox_schedule(GenArgs* a);
 
 // Launchers (return cudaSuccess or the launch error).  dt: 4 = FP32, 8 = FP64.
 // pass: 1 = synthesis + z, 2 = y, 3 = C2R x + epilogue.
