@@ -3,9 +3,13 @@
 Workload (default): a 512^3 deck (re-fitted to 513^3) with exponential
 correlation, anisotropic correlation lengths (40, 20, 10) at spacing 1,
 lognormal marginal (mean 1, CV 0.3), 2x2x2 tiles with overlap 2 l, padded
-periodic generation in FP32 with the FP64 spectral normalisation.  One step
-generates one complete field (8 tiles x 3 passes).  Synthetic: the field is
-drawn from seeded Philox normals; nothing is read from disk.
+periodic generation in FP32 with the FP64 spectral normalisation and the
+z-axis DFT of pass 1 as split-BF16 tensor-core products (SCARL_SPLIT_BF16;
+field rel-L2 against FP64 reported, gate 1e-5).  One step generates one
+complete field (8 tiles x 3 passes).  Synthetic: the field is drawn from
+seeded Philox normals; nothing is read from disk.  Beside it: the same grid
+with every DFT on the CUDA cores in FP32 (fp32_path) and the plain GPU path
+(FP32, the reference's full padding 2^ceil(log2 2 Np)).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scarl|reference]
 
@@ -141,7 +145,7 @@ def pass_bytes(lay, P, dtype_bytes=4):
             own *= Np[d] - (No[d] if pos[d] > 0 and No[d] >= 2 else 0)
         reread += Np[0] * Np[1] * Np[2] - own
     b3 = Hx * Np[1] * Np[2] * c + Np[0] * Np[1] * Np[2] * dtype_bytes + reread * dtype_bytes // nb
-    return {"k_gen_z": b1, "k_mid_y": b2, "k_c2r_x": b3}
+    return {"k_gen_z": b1, "k_gen_z_tc": b1, "k_mid_y": b2, "k_c2r_x": b3}
 
 
 def cpu_sample(lay, P, steps, warmup, stride=8):
@@ -394,8 +398,8 @@ def main():
         sample, lay = layout_of(S)
         L = [int(v) for v in lay["L"]]
         field = torch.empty(L[0] * L[1] * L[2], dtype=torch.float32, device="cuda")
-        S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=S.F32, nb_procs=8, topo=TOPO,
-                          pad_policy=S.PAD_AUTO, pad_tol=PAD_TOL, out=field)
+        S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=S.F32 | S.SPLIT_BF16,
+                          nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO, pad_tol=PAD_TOL, out=field)
         ctx.sync()
         print(json.dumps({"profile_tile": "ok", "launches": ctx.counters()["launches"]}))
         ctx.close()
@@ -415,7 +419,9 @@ def main():
 
     P_auto, P_full = pads(S, lay, S.PAD_AUTO), pads(S, lay, S.PAD_FULL)
 
-    def step(out=field, dtype=S.F32, policy=S.PAD_AUTO):
+    HEAD = S.F32 | S.SPLIT_BF16  # headline precision: split-BF16 tensor-core z stage
+
+    def step(out=field, dtype=HEAD, policy=S.PAD_AUTO):
         S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=dtype, nb_procs=8,
                           topo=TOPO, pad_policy=policy, pad_tol=PAD_TOL, autotune=True, out=out)
 
@@ -425,7 +431,8 @@ def main():
 
     for _ in range(args.warmup):
         step()
-        step(policy=S.PAD_FULL)
+        step(dtype=S.F32)
+        step(dtype=S.F32, policy=S.PAD_FULL)
     torch.cuda.synchronize()
 
     # ---- timed region: device-resident output, CUDA events on the launch stream
@@ -452,19 +459,24 @@ def main():
     ms = R.max_over_ranks(ms, dist, "cuda")
     value = world * npts / (ms * 1e-3) / 1e6
 
-    # ---- the plain path: the reference's full padding, same timing method
-    barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        step(policy=S.PAD_FULL)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms_full = e0.elapsed_time(e1) / args.steps
-    ms_full = R.max_over_ranks(ms_full, dist, "cuda")
+    def timed_steps(**kw):
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(**kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return R.max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, "cuda")
+
+    # ---- the plain GPU path: FP32 on the CUDA cores with the reference's full padding
+    ms_full = timed_steps(dtype=S.F32, policy=S.PAD_FULL)
     plain = {"value": round(world * npts / (ms_full * 1e-3) / 1e6, 2), "ms_per_step": round(ms_full, 4),
-             "padded_grid": P_full, "pad_policy": "full, 2^ceil(log2(2 Np)) (SRC_F/fftw_ScaRL.f90:194)"}
+             "padded_grid": P_full, "precision": "f32 (every DFT on the CUDA cores)",
+             "pad_policy": "full, 2^ceil(log2(2 Np)) (SRC_F/fftw_ScaRL.f90:194)"}
+    # ---- the same padded grid as the headline with every DFT in FP32
+    ms_f32 = timed_steps(dtype=S.F32)
 
     # ---- per-kernel device times (separate, profiled steps)
     ctx.profile(True)
@@ -501,25 +513,35 @@ def main():
                 "frac": round(ach / peak, 4), "traffic": traffic,
                 "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_launch": pb[dom]}
 
-    # ---- accuracy of the FP32 field against the FP64 path (same seed)
+    # ---- accuracy of the FP32 fields against the FP64 path (same seed)
     f64 = torch.empty(npts, dtype=torch.float64, device="cuda")
     step(out=f64, dtype=S.F64)
-    step()
-    torch.cuda.synchronize()
-    rel = float(torch.linalg.vector_norm(field.double() - f64) / torch.linalg.vector_norm(f64))
+
+    def rel_to_f64(dtype):
+        step(dtype=dtype)
+        torch.cuda.synchronize()
+        d = field.double() - f64
+        return (float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(f64)),
+                float(d.abs().max() / f64.abs().max()))
+
+    rel32, max32 = rel_to_f64(S.F32)
+    rel, relmax = rel_to_f64(HEAD)
     del f64
+    fp32 = {"value": round(world * npts / (ms_f32 * 1e-3) / 1e6, 2), "ms_per_step": round(ms_f32, 4),
+            "padded_grid": P_auto, "precision": "f32 (every DFT on the CUDA cores)",
+            "rel_l2_vs_fp64": rel32, "max_err_vs_fp64": max32}
 
     # ---- end to end through the C ABI with a pinned host buffer
     host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
     hnp = host.numpy()
     ctx.set_stream(0)  # library-owned stream; host calls synchronise inside
-    S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
+    S.generate_sample(ctx, sample, dtype=HEAD, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
                       pad_tol=PAD_TOL, autotune=True, out=hnp)
     c0 = ctx.counters()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        S.generate_sample(ctx, sample, dtype=S.F32, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
+        S.generate_sample(ctx, sample, dtype=HEAD, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
                           pad_tol=PAD_TOL, autotune=True, out=hnp)
     e2e_s = (time.perf_counter() - t0) / args.steps
     c1 = ctx.counters()
@@ -551,10 +573,12 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpoints/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (z DFT: bf16 head/tail products, f32 accumulation)",
                 "data": "synthetic (Philox normals, seeded per rank)",
-                "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "roofline": roof,
-                "kernels": kern, "launch_variants": tuned, "plain_path": plain,
+                "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "max_err_vs_fp64": relmax,
+                "roofline": roof, "kernels": kern, "launch_variants": tuned, "plain_path": plain,
+                "fp32_path": fp32, "speedup_vs_plain_path": round(ms_full / ms, 3),
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
                 "ensemble": ens, "large_field": large}
         print(json.dumps(line), flush=True)
