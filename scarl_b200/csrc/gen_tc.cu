@@ -37,9 +37,9 @@ namespace scarl {
 
 namespace {
 
-template <int N1_, int N2_, int LB_>
+template <int N1_, int N2_, int LB_, int NCH_>
 struct TcCfg {
-  static constexpr int N1 = N1_, N2 = N2_, LB = LB_, N = N1 * N2;
+  static constexpr int N1 = N1_, N2 = N2_, LB = LB_, N = N1 * N2, NCH = NCH_;
   static constexpr int THREADS = 256, CTAS_PER_SM = 2;
   static constexpr int ROWS1 = LB * N1;  // stage-1 rows (line, k1)
   static constexpr int ROWS2 = LB * N2;  // stage-2 rows (line, n2)
@@ -53,7 +53,7 @@ struct TcCfg {
   static constexpr int A1B = T1 * TILE1, A2B = T2 * TILE2;
   static constexpr int AB = A1B > A2B ? A1B : A2B;
   static constexpr int STAGE_LD = LB + 1;  // output staging row (one z), float2 units
-  static constexpr int STAGEB = N * STAGE_LD * 8;
+  static constexpr int STAGEB = N / NCH * STAGE_LD * 8;
   static constexpr int REGION = (2 * AB > STAGEB ? 2 * AB : STAGEB);
   static constexpr int B1B = (K1 / 8) * SBO1, B2B = (K2 / 8) * SBO2;
   static constexpr int TMEM_COLS = LB * N / 64;
@@ -64,9 +64,9 @@ struct TcCfg {
   static constexpr int OFF_BAR = OFF_TW + 8 * N;  // mbarrier (8 B) + tensor-memory slot (4 B)
   static constexpr int SMEM = OFF_BAR + 16;
   static_assert(ROWS1 == THREADS, "one stage-1 row per thread");
-  static_assert(N2 == 32, "a stage-2 row group of a line is one warp's 32 lanes");
+  static_assert((N1 / NCH) % 16 == 0, "output chunks of whole 16-column tensor-memory loads");
   static_assert(ROWS2 % 128 == 0 && T1 * K1 == TMEM_COLS && T2 * K2 == TMEM_COLS, "tiling");
-  static_assert(N1 % 8 == 0 && K1 <= 256 && K2 % 16 == 0, "radices");
+  static_assert(N1 % 8 == 0 && N2 % 16 == 0 && K1 <= 256 && K2 <= 256, "radices");
   static_assert(TMEM_COLS >= 32 && TMEM_COLS * CTAS_PER_SM <= 512 &&
                 (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory");
   static_assert(CTAS_PER_SM * (SMEM + 1024) <= 228 * 1024, "shared memory");
@@ -114,9 +114,9 @@ __device__ void fill_dft_b(unsigned char* hi, unsigned char* lo) {
   }
 }
 
-template <int N1, int N2, int LB, int AMP>
+template <int N1, int N2, int LB, int NCH, int AMP>
 __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
-  using Cfg = TcCfg<N1, N2, LB>;
+  using Cfg = TcCfg<N1, N2, LB, NCH>;
   constexpr int N = Cfg::N;
   extern __shared__ __align__(128) unsigned char sm[];
   unsigned char* AH = sm + Cfg::OFF_AH;
@@ -317,36 +317,46 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
     if (!__syncthreads_and(ok)) { ok = false; break; }
     tc::fence_after_sync();
     // ---- results X[n2 + N2 n1] of row (line, n2) into the z-major staging
-    //      area (the operand region, free now): stage[z][line] ----
+    //      area (the operand region, free now): stage[z][line], NCH
+    //      chunks of N1 / NCH consecutive n1 (z ranges of N / NCH) ----
     float2* stage = reinterpret_cast<float2*>(sm);
+    constexpr int CN1 = N1 / Cfg::NCH, CZ = N / Cfg::NCH;
 #pragma unroll 1
-    for (int t = warp >> 2; t < Cfg::T2; t += Cfg::THREADS / 128) {
-      const int line = (t * 128 + q * 32) / N2, n2 = lane;
-      float v[Cfg::K2];
+    for (int ch = 0; ch < Cfg::NCH && ch * CZ < Nz; ++ch) {
+#pragma unroll 1
+      for (int t = warp >> 2; t < Cfg::T2; t += Cfg::THREADS / 128) {
+        const int R = t * 128 + q * 32 + lane;
+        const int line = R / N2, n2 = R % N2;
+        float v[2 * CN1];
+        const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + t * Cfg::K2 + ch * CN1;
 #pragma unroll
-      for (int c = 0; c < Cfg::K2 / 16; ++c)
-        tc::tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + t * Cfg::K2 + c * 16, v + c * 16);
-      tc::tmem_wait_ld();
+        for (int c = 0; c < CN1 / 16; ++c) {
+          tc::tmem_ld16(col + c * 16, v + c * 16);             // re of n1 = ch CN1 + ..
+          tc::tmem_ld16(col + N1 + c * 16, v + CN1 + c * 16);  // im
+        }
+        tc::tmem_wait_ld();
 #pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1)
-        stage[(n2 + N2 * n1) * Cfg::STAGE_LD + line] = make_float2(v[n1], v[N1 + n1]);
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    // ---- z < Nz to global memory, LB consecutive lines per z ----
-    {
-      const int line = tid % LB;
-      const int l = l0 + line;
-      const bool valid = l < nlines;
-      const int ky = valid ? l / a.Hx : 0, kx = valid ? l - ky * a.Hx : 0;
-      float2* dst = work + (size_t)ky * a.Hpad + kx;
-      const size_t zstride = (size_t)a.P[1] * a.Hpad;
-      if (valid)
+        for (int n1 = 0; n1 < CN1; ++n1)
+          stage[(n2 + N2 * n1) * Cfg::STAGE_LD + line] = make_float2(v[n1], v[CN1 + n1]);
+      }
+      tc::fence_before_sync();
+      __syncthreads();
+      // ---- z < Nz of this chunk to global memory, LB consecutive lines per z
+      {
+        const int line = tid % LB;
+        const int l = l0 + line;
+        const bool valid = l < nlines;
+        const int ky = valid ? l / a.Hx : 0, kx = valid ? l - ky * a.Hx : 0;
+        const size_t zstride = (size_t)a.P[1] * a.Hpad;
+        float2* dst = work + (size_t)ky * a.Hpad + kx + (size_t)(ch * CZ) * zstride;
+        const int zn = min(CZ, Nz - ch * CZ);
+        if (valid)
 #pragma unroll 4
-        for (int z = tid / LB; z < Nz; z += Cfg::THREADS / LB)
-          dst[(size_t)z * zstride] = stage[z * Cfg::STAGE_LD + line];
+          for (int z = tid / LB; z < zn; z += Cfg::THREADS / LB)
+            dst[(size_t)z * zstride] = stage[z * Cfg::STAGE_LD + line];
+      }
+      __syncthreads();  // the staging area: next chunk, or the next item's operands
     }
-    __syncthreads();  // the staging area is the next item's operand region
   }
   if (!ok) {
     // an MMA did not complete in time: report, then give it one more bounded
@@ -361,10 +371,10 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
   if (warp == 0) tc::tmem_free(tmem, Cfg::TMEM_COLS);
 }
 
-template <int N1, int N2, int LB, int AMP>
+template <int N1, int N2, int LB, int NCH, int AMP>
 cudaError_t launch_tc(const GenArgs& a, cudaStream_t s) {
-  using Cfg = TcCfg<N1, N2, LB>;
-  auto kern = k_gen_z_tc<N1, N2, LB, AMP>;
+  using Cfg = TcCfg<N1, N2, LB, NCH>;
+  auto kern = k_gen_z_tc<N1, N2, LB, NCH, AMP>;
   // per device: the shared-memory opt-in and the SM count
   constexpr int kMaxDev = 64;
   static int sms[kMaxDev] = {};
@@ -389,18 +399,25 @@ cudaError_t launch_tc(const GenArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <int N1, int N2, int LB, int NCH>
+cudaError_t launch_amp(const GenArgs& a, cudaStream_t s) {
+  if (a.amp == AMP_SEPARABLE) return launch_tc<N1, N2, LB, NCH, AMP_SEPARABLE>(a, s);
+  if (a.amp == AMP_RECIP) return launch_tc<N1, N2, LB, NCH, AMP_RECIP>(a, s);
+  return launch_tc<N1, N2, LB, NCH, AMP_POW>(a, s);
+}
+
 }  // namespace
 
-// Line lengths with a tensor-core pass 1 (FP32 output, Philox spectrum).
-bool gen_z_tc_supported(int N) { return N == 512; }
+// Line lengths with a tensor-core pass 1 (FP32 output, Philox spectrum):
+// N = N1 x N2 = 16 x 16, 16 x 32, 32 x 32.
+bool gen_z_tc_supported(int N) { return N == 256 || N == 512 || N == 1024; }
 
 cudaError_t launch_gen_z_tc(const GenArgs& a, cudaStream_t s) {
   if (!a.status || a.spec != SPEC_PHILOX) return cudaErrorInvalidValue;
   switch (a.P[2]) {
-    case 512:
-      if (a.amp == AMP_SEPARABLE) return launch_tc<16, 32, 16, AMP_SEPARABLE>(a, s);
-      if (a.amp == AMP_RECIP) return launch_tc<16, 32, 16, AMP_RECIP>(a, s);
-      return launch_tc<16, 32, 16, AMP_POW>(a, s);
+    case 256: return launch_amp<16, 16, 16, 1>(a, s);
+    case 512: return launch_amp<16, 32, 16, 1>(a, s);
+    case 1024: return launch_amp<32, 32, 8, 2>(a, s);
     default: return cudaErrorInvalidValue;
   }
 }

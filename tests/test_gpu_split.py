@@ -36,6 +36,11 @@ def _ran_tc(ctx, fn):
     ((20, 6, 267), (32, 16, 512), (0.5, 1, 1), (4, 3, 12), 2, 1.5),   # von Karman
     ((5, 5, 512), (8, 8, 512), (1, 1, 1), (2, 2, 64), 3, 0.5),        # every z kept
     ((6, 4, 1), (8, 8, 512), (1, 1, 1), (2, 2, 10), 3, 0.5),          # one z plane
+    ((11, 9, 200), (32, 16, 256), (1, 1, 1), (3, 3, 20), 3, 0.5),     # N = 16 x 16
+    ((7, 5, 256), (16, 8, 256), (1, 1, 1), (2, 2, 30), 1, 0.5),       # N = 16 x 16, all z
+    ((9, 6, 600), (16, 16, 1024), (1, 1, 1), (3, 3, 60), 3, 0.5),     # N = 32 x 32, two chunks
+    ((5, 7, 1024), (8, 16, 1024), (1, 1, 1), (2, 2, 90), 2, 0.8),     # N = 32 x 32, all z
+    ((6, 5, 400), (16, 8, 1024), (1, 1, 1), (2, 2, 40), 1, 0.5),      # first chunk only
 ])
 def test_split_vs_oracle(ctx, oracle, Np, P, dx, cl, cm, nu):
     ref = oracle.gen_padded(Np, P, dx, cl, cm, nu, 1, seed=77, stream=3)
@@ -59,6 +64,7 @@ def test_split_deterministic_and_seeded(ctx):
 
 
 def test_split_other_lengths_use_fp32_pass(ctx, oracle):
+    # z lengths without a tensor-core kernel (here 128) run the FP32 pass
     Np, P = (10, 10, 100), (16, 16, 128)
     ref = oracle.gen_padded(Np, P, (1, 1, 1), (3, 3, 10), 3, 0.5, 1, seed=2)
     out, st = _ran_tc(ctx, lambda: S.gen_padded(ctx, Np, (1, 1, 1), (3, 3, 10), 3, pad=P, seed=2,
