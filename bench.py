@@ -367,6 +367,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-large-field", action="store_true")
+    ap.add_argument("--profile-stats", action="store_true",
+                    help="one 1024x1024x512 FP32 field (2 GB) and one pass of the streamed "
+                         "statistics (mean, variance, axis covariance to lag 256), no timing")
     ap.add_argument("--profile-tile", action="store_true",
                     help="generate one field once (no timing) for profiler captures; launch "
                          "variants come from SCARL_TUNE_CACHE when set")
@@ -393,6 +396,20 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+    if args.profile_stats:
+        ctx = S.Context(local)
+        s = S.make_sample((0, 0, 0), (1023, 1023, 511), (32, 32, 16), (127 / 32, 127 / 32, 0),
+                          (33, 33, 17), corrMod=1, margiFirst=1, avg=0.0, std_dev=1.0)
+        lay = S.sample_layout(s, 1, 4, (2, 2, 1))
+        L = [int(v) for v in lay["L"]]
+        field = torch.empty(L[0] * L[1] * L[2], dtype=torch.float32, device="cuda")
+        S.generate_sample(ctx, s, dtype=S.F32, nb_procs=4, topo=(2, 2, 1), pad_policy=S.PAD_AUTO,
+                          pad_tol=PAD_TOL, out=field)
+        mean, var, cov = S.axis_cov(ctx, field, L, 256)
+        ctx.sync()
+        print(json.dumps({"profile_stats": "ok", "L": L, "mean": mean, "var": var}))
+        ctx.close()
+        return
     if args.profile_tile:
         ctx = S.Context(local)
         sample, lay = layout_of(S)

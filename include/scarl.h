@@ -69,6 +69,8 @@ extern "C" {
 #define SCARL_PAD_FULL 0     /* 2^ceil(log2(2 Np)), SRC_F/fftw_ScaRL.f90:194 */
 #define SCARL_PAD_AUTO 1     /* smallest power of two with image error <= tol */
 #define SCARL_PAD_LEARNED 2  /* the context's trained predictor, full padding as fallback */
+#define SCARL_PAD_SMOOTH 3   /* as AUTO over every supported length: powers of two and
+                                3, 5, 7 x 2^a (2^a >= 16), at most 2048 */
 
 typedef struct scarl_ctx scarl_ctx;
 
@@ -116,8 +118,8 @@ typedef struct {
   int nb_procs;           /* tiles requested (mpirun -np), 0 = 1 */
   int topo_shape[3];      /* explicit topology (extra_config_ScaRL.txt); 0 = decide */
   int pad[3];             /* explicit padded grid per axis; 0 = chosen by pad_policy */
-  int pad_policy;         /* SCARL_PAD_FULL (default), SCARL_PAD_AUTO or SCARL_PAD_LEARNED */
-  double pad_tol;         /* SCARL_PAD_AUTO image tolerance, 0 = 1e-3 */
+  int pad_policy;         /* SCARL_PAD_FULL (default), _AUTO, _LEARNED or _SMOOTH */
+  double pad_tol;         /* SCARL_PAD_AUTO / _SMOOTH image tolerance, 0 = 1e-3 */
   int no_spectral_normalisation; /* 1 = raw Riemann-sum amplitudes */
   int normalize_field;    /* 1 = normalize_field (disabled in the reference) */
   uint32_t stream;        /* realisation stream (ensembles), 0 by default */

@@ -22,7 +22,7 @@ F32, F64 = 4, 8
 # flag on F32: pass 1's z DFT as split-BF16 tensor-core products
 SPLIT_BF16 = 0x100
 GEN_DCT, GEN_SHINO, GEN_PADDED = 1, 2, 3
-PAD_FULL, PAD_AUTO, PAD_LEARNED = 0, 1, 2
+PAD_FULL, PAD_AUTO, PAD_LEARNED, PAD_SMOOTH = 0, 1, 2, 3
 
 
 class Sample(C.Structure):

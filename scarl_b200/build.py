@@ -19,7 +19,10 @@ CUDA_SOURCES = ["gen_padded.cu", "gen_tc.cu", "dct_literal.cu", "post.cu", "stat
                 "mlp.cu", "noalloc.cu"]
 # gen_inst.cu once per (precision, line-length group): the generator pass
 # instantiations compile in parallel
-INSTANCES = [(dt, n) for dt in (4, 8) for n in (0, 256, 512, 1024, 2048)]
+# (0: power-of-two lengths 4..128, -1 / -2: mixed lengths 24..112 / 160..224)
+INSTANCES = [(dt, n) for dt in (4, 8)
+             for n in (0, -1, -2, 256, 320, 384, 448, 512, 640, 768, 896, 1024, 1280, 1536, 1792,
+                       2048)]
 HOST_SOURCES = ["api.cpp", "host_maps.cpp", "h5io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",

@@ -511,8 +511,10 @@ int run_passes(scarl_ctx* ctx, int dt, const GenArgs& a) {
 int check_grid(scarl_ctx* ctx, const int P[3], const int Np[3]) {
   for (int d = 0; d < 3; ++d) {
     if (Np[d] < 1) return fail(ctx, SCARL_EINVAL, "Np must be >= 1");
-    if (!pow2(P[d]) || P[d] < 8 || P[d] > 2048)
-      return fail(ctx, SCARL_EUNSUPPORTED, "padded grid must be a power of two in [8, 2048]");
+    if (!fft_length_supported(P[d]))
+      return fail(ctx, SCARL_EUNSUPPORTED,
+                  "padded grid lengths must lie in [8, 2048] and be a power of two or 3, 5 or 7 "
+                  "times a power of two >= 16");
     if (P[d] < Np[d]) return fail(ctx, SCARL_EINVAL, "padded grid smaller than the tile");
   }
   return SCARL_OK;

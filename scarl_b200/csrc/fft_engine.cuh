@@ -1,5 +1,5 @@
 // fft_engine.cuh -- batched 1D inverse DFTs (sign +, unnormalised) of
-// power-of-two length N inside one thread block.
+// length N = m 2^a (m = 1, 3, 5 or 7) inside one thread block.
 //
 // A block owns B lines of length N.  Each line is served by TPL = N/E
 // threads holding E complex values in registers.  The transform is the
@@ -10,7 +10,10 @@
 // writes x[(j/Ns) Ns R + (j mod Ns) + r Ns]; Ns grows by R every stage.
 // The first stage reads straight from the caller's loader (global memory or
 // an in-register generator) and the last stage hands each output to the
-// caller's storer, so only the middle hand-offs touch shared memory.
+// caller's storer, so only the middle hand-offs touch shared memory.  The
+// power-of-two radices come first (the first radix is even, so a first-stage
+// group holds the modes k and k + N/2 together); an odd factor m is the last
+// stage, a direct DFT in registers.
 #pragma once
 
 #include "scarl_common.cuh"
@@ -18,10 +21,14 @@
 namespace scarl {
 
 // ---------------------------------------------------------------------------
-// R-point inverse DFT in registers, R = 2..32: radix-2 decimation in
-// frequency, result left in bit-reversed order (read it through brev<R>).
+// R-point inverse DFT in registers.  R = 2..32 (power of two): radix-2
+// decimation in frequency, result left in bit-reversed order; R = 3, 5, 7:
+// direct sums over the conjugate-symmetric pairs, result in natural order.
+// operm<R>(r) is the register holding output r.
 // ---------------------------------------------------------------------------
 template <int R> __host__ __device__ constexpr int ilog2c() { return R <= 1 ? 0 : 1 + ilog2c<R / 2>(); }
+__host__ __device__ constexpr bool is_pow2c(int n) { return n >= 1 && (n & (n - 1)) == 0; }
+__host__ __device__ constexpr int odd_part(int n) { return (n > 0 && n % 2 == 0) ? odd_part(n / 2) : n; }
 
 template <int R> __host__ __device__ __forceinline__ constexpr int brev(int i) {
   int r = 0;
@@ -29,6 +36,20 @@ template <int R> __host__ __device__ __forceinline__ constexpr int brev(int i) {
     if (i & (1 << b)) r |= 1 << (ilog2c<R>() - 1 - b);
   return r;
 }
+template <int R> __host__ __device__ __forceinline__ constexpr int operm(int i) {
+  if constexpr (is_pow2c(R)) return brev<R>(i);
+  else return i;
+}
+
+// cos and sin of 2 pi j / p, j = 1 .. (p - 1) / 2, for p = 3, 5, 7.
+__device__ constexpr double kOddCos[3][3] = {
+    {-0.5000000000000000000000, 0.0, 0.0},
+    {0.3090169943749474241023, -0.8090169943749474241023, 0.0},
+    {0.6234898018587335305250, -0.2225209339563144042889, -0.9009688679024191262361}};
+__device__ constexpr double kOddSin[3][3] = {
+    {0.8660254037844386467637, 0.0, 0.0},
+    {0.9510565162951535721164, 0.5877852522924731291687, 0.0},
+    {0.7818314824680298087084, 0.9749279121818236070181, 0.4338837391175581204758}};
 
 // d * e^{+2 pi i m / 32}, m < 16, m known after unrolling.
 template <typename C> __device__ __forceinline__ C tw32(C d, int m) {
@@ -44,35 +65,87 @@ template <typename C> __device__ __forceinline__ C tw32(C d, int m) {
   return mk(d.x * c - d.y * s, d.x * s + d.y * c);
 }
 
+// X_k = sum_n v_n e^{+2 pi i n k / P}, P odd: with s_n = v_n + v_{P-n},
+// d_n = v_n - v_{P-n}, X_0 = v_0 + sum s_n and, for k = 1 .. (P-1)/2,
+// X_k = A_k + i B_k, X_{P-k} = A_k - i B_k, A_k = v_0 + sum_n s_n cos(2 pi n k / P),
+// B_k = sum_n d_n sin(2 pi n k / P).
+template <int P, typename C> __device__ __forceinline__ void dft_odd(C* v) {
+  using T = decltype(v[0].x);
+  constexpr int H = (P - 1) / 2, row = P / 2 - 1;  // table row of P = 3, 5, 7
+  C sp[H], dm[H];
+#pragma unroll
+  for (int n = 1; n <= H; ++n) {
+    sp[n - 1] = cadd(v[n], v[P - n]);
+    dm[n - 1] = csub(v[n], v[P - n]);
+  }
+  C x0 = v[0];
+#pragma unroll
+  for (int n = 0; n < H; ++n) x0 = cadd(x0, sp[n]);
+#pragma unroll
+  for (int k = 1; k <= H; ++k) {
+    C a = v[0], b = mk(T(0), T(0));
+#pragma unroll
+    for (int n = 1; n <= H; ++n) {
+      const int j = (n * k) % P;  // angle index, folded into 1 .. H with the sine's sign
+      const int jj = j <= H ? j : P - j;
+      const T c = (T)kOddCos[row][jj - 1];
+      const T sn = (j <= H) ? (T)kOddSin[row][jj - 1] : -(T)kOddSin[row][jj - 1];
+      a = mk(a.x + sp[n - 1].x * c, a.y + sp[n - 1].y * c);
+      b = mk(b.x + dm[n - 1].x * sn, b.y + dm[n - 1].y * sn);
+    }
+    v[k] = mk(a.x - b.y, a.y + b.x);
+    v[P - k] = mk(a.x + b.y, a.y - b.x);
+  }
+  v[0] = x0;
+}
+
 template <int R, typename C> __device__ __forceinline__ void dft_reg(C* v) {
+  if constexpr (!is_pow2c(R)) {
+    static_assert(R == 3 || R == 5 || R == 7, "odd radix 3, 5 or 7");
+    dft_odd<R>(v);
+  } else {
 #pragma unroll
-  for (int len = R; len >= 2; len >>= 1) {
-    const int half = len >> 1;
+    for (int len = R; len >= 2; len >>= 1) {
+      const int half = len >> 1;
 #pragma unroll
-    for (int s = 0; s < R; s += len) {
+      for (int s = 0; s < R; s += len) {
 #pragma unroll
-      for (int k = 0; k < half; ++k) {
-        const C a = v[s + k], b = v[s + k + half];
-        v[s + k] = cadd(a, b);
-        v[s + k + half] = tw32(csub(a, b), k * (32 / len));
+        for (int k = 0; k < half; ++k) {
+          const C a = v[s + k], b = v[s + k + half];
+          v[s + k] = cadd(a, b);
+          v[s + k + half] = tw32(csub(a, b), k * (32 / len));
+        }
       }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Stage plan for N = 2^n with at most E values per thread.
+// Stage plan for N = m 2^a with E values per thread: power-of-two radices of
+// at most the largest power of two dividing E, then the odd factor m as the
+// last stage (m must divide E).  At most 5 stages.
 // ---------------------------------------------------------------------------
+__host__ __device__ constexpr int pow2_of(int e) { return (e % 2 == 0) ? 2 * pow2_of(e / 2) : 1; }
+
 template <int N, int E> struct StagePlan {
-  __host__ __device__ static constexpr int radix(int s) {
-    int rem = N;
-    for (int i = 0; i < s; ++i) rem /= (rem > E ? E : rem);
-    return rem > E ? E : rem;
-  }
-  __host__ __device__ static constexpr int count() {
-    int rem = N, c = 0;
-    while (rem > 1) { rem /= (rem > E ? E : rem); ++c; }
+  static constexpr int M = odd_part(N), P2 = N / M, E2 = pow2_of(E);
+  __host__ __device__ static constexpr int p2_count() {
+    int rem = P2, c = 0;
+    while (rem > 1) { rem /= (rem > E2 ? E2 : rem); ++c; }
     return c;
+  }
+  __host__ __device__ static constexpr int radix(int s) {
+    if (M > 1 && s == p2_count()) return M;
+    int rem = P2;
+    for (int i = 0; i < s; ++i) rem /= (rem > E2 ? E2 : rem);
+    return rem > E2 ? E2 : rem;
+  }
+  __host__ __device__ static constexpr int count() { return p2_count() + (M > 1 ? 1 : 0); }
+  // a plan the engine can run: every radix divides E, 2 <= stages <= 5 (or
+  // one power-of-two stage), first radix even
+  __host__ __device__ static constexpr bool valid() {
+    return (M == 1 || M == 3 || M == 5 || M == 7) && E % M == 0 && N % E == 0 && count() <= 5 &&
+           (M == 1 || P2 >= 2) && (count() >= 2 || M == 1);
   }
   static constexpr int S = count();
 };
@@ -119,7 +192,7 @@ __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, i
     dft_reg<R>(v + q * R);
     const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) sm[sidx<O, B, LS, SK>(base + r * Ns, b)] = v[q * R + brev<R>(r)];
+    for (int r = 0; r < R; ++r) sm[sidx<O, B, LS, SK>(base + r * Ns, b)] = v[q * R + operm<R>(r)];
   }
   __syncthreads();
 }
@@ -150,7 +223,7 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
       dft_reg<R1>(v + q * R1);
       C o[R1];
 #pragma unroll
-      for (int r = 0; r < R1; ++r) o[r] = v[q * R1 + brev<R1>(r)];
+      for (int r = 0; r < R1; ++r) o[r] = v[q * R1 + operm<R1>(r)];
       store(j, o);
     }
     __syncthreads();  // keep the barrier count uniform with the multi-stage path
@@ -163,14 +236,17 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
     for (int q = 0; q < NB1; ++q) {
       const int j = t + TPL * q;
 #pragma unroll
-      for (int r = 0; r < R1; ++r) sm[sidx<O, B, LS, SK>(j * R1 + r, b)] = v[q * R1 + brev<R1>(r)];
+      for (int r = 0; r < R1; ++r) sm[sidx<O, B, LS, SK>(j * R1 + r, b)] = v[q * R1 + operm<R1>(r)];
     }
     __syncthreads();
     if constexpr (P::S >= 3)
       stockham_smem_stage<C, N, E, P::radix(1), R1, O, B, LS, SK>(sm, b, t, tw, twmul);
     if constexpr (P::S >= 4)
       stockham_smem_stage<C, N, E, P::radix(2), R1 * P::radix(1), O, B, LS, SK>(sm, b, t, tw, twmul);
-    static_assert(P::S <= 4, "line length too long for the register budget");
+    if constexpr (P::S >= 5)
+      stockham_smem_stage<C, N, E, P::radix(3), R1 * P::radix(1) * P::radix(2), O, B, LS, SK>(
+          sm, b, t, tw, twmul);
+    static_assert(P::S <= 5, "line length too long for the register budget");
     // last stage
     constexpr int RL = P::radix(P::S - 1);
     constexpr int NsL = N / RL;
@@ -195,7 +271,7 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
       // last stage: (j / NsL) == 0, output index j + r * NsL
       C o[RL];
 #pragma unroll
-      for (int r = 0; r < RL; ++r) o[r] = v[q * RL + brev<RL>(r)];
+      for (int r = 0; r < RL; ++r) o[r] = v[q * RL + operm<RL>(r)];
       store(j, o);
     }
   }

@@ -19,12 +19,31 @@ static cudaError_t run_pass_t(int pass, int v, const GenArgs& a, const BatchMap*
     case 4: return run_pass_len<T, 4>(pass, v, a, bm, nb, s);
     case 8: return run_pass_len<T, 8>(pass, v, a, bm, nb, s);
     case 16: return run_pass_len<T, 16>(pass, v, a, bm, nb, s);
+    case 24: return run_pass_len<T, 24>(pass, v, a, bm, nb, s);
     case 32: return run_pass_len<T, 32>(pass, v, a, bm, nb, s);
+    case 40: return run_pass_len<T, 40>(pass, v, a, bm, nb, s);
+    case 48: return run_pass_len<T, 48>(pass, v, a, bm, nb, s);
+    case 56: return run_pass_len<T, 56>(pass, v, a, bm, nb, s);
     case 64: return run_pass_len<T, 64>(pass, v, a, bm, nb, s);
+    case 80: return run_pass_len<T, 80>(pass, v, a, bm, nb, s);
+    case 96: return run_pass_len<T, 96>(pass, v, a, bm, nb, s);
+    case 112: return run_pass_len<T, 112>(pass, v, a, bm, nb, s);
     case 128: return run_pass_len<T, 128>(pass, v, a, bm, nb, s);
+    case 160: return run_pass_len<T, 160>(pass, v, a, bm, nb, s);
+    case 192: return run_pass_len<T, 192>(pass, v, a, bm, nb, s);
+    case 224: return run_pass_len<T, 224>(pass, v, a, bm, nb, s);
     case 256: return run_pass_len<T, 256>(pass, v, a, bm, nb, s);
+    case 320: return run_pass_len<T, 320>(pass, v, a, bm, nb, s);
+    case 384: return run_pass_len<T, 384>(pass, v, a, bm, nb, s);
+    case 448: return run_pass_len<T, 448>(pass, v, a, bm, nb, s);
     case 512: return run_pass_len<T, 512>(pass, v, a, bm, nb, s);
+    case 640: return run_pass_len<T, 640>(pass, v, a, bm, nb, s);
+    case 768: return run_pass_len<T, 768>(pass, v, a, bm, nb, s);
+    case 896: return run_pass_len<T, 896>(pass, v, a, bm, nb, s);
     case 1024: return run_pass_len<T, 1024>(pass, v, a, bm, nb, s);
+    case 1280: return run_pass_len<T, 1280>(pass, v, a, bm, nb, s);
+    case 1536: return run_pass_len<T, 1536>(pass, v, a, bm, nb, s);
+    case 1792: return run_pass_len<T, 1792>(pass, v, a, bm, nb, s);
     case 2048: return run_pass_len<T, 2048>(pass, v, a, bm, nb, s);
     default: return cudaErrorInvalidValue;
   }

@@ -300,10 +300,28 @@ double axis_correlation(int corrMod, double nu, double l, double r) {
   return std::pow(2.0, 1.0 - nu) / std::tgamma(nu) * std::pow(x, nu) * bessel_k(nu, x);
 }
 
+bool fft_length_supported(int n) {
+  if (n < 8 || n > 2048) return false;
+  int m = n;
+  while (m % 2 == 0) m /= 2;
+  if (m == 1) return true;
+  return (m == 3 || m == 5 || m == 7) && n / m >= 16;
+}
+
+// Smallest supported length >= n (power of two, or m 2^a with m = 3, 5, 7 and
+// 2^a >= 16); 0 above 2048.
+static int next_smooth(int n) {
+  for (int p = std::max(n, 8); p <= 2048; ++p)
+    if (fft_length_supported(p)) return p;
+  return 0;
+}
+
 // policy 0: the reference's 2^ceil(log2(2 Np)) (SRC_F/fftw_ScaRL.f90:194).
 // policy 1: smallest power of two P >= 8 with C((P - Np + 1) dx) <= tol along
 // each axis: the nearest periodic image of the farthest pair of tile points
 // then contributes at most tol to the covariance.
+// policy 3: the same rule over every supported length (powers of two and
+// 3, 5, 7 times a power of two >= 16, up to 2048).
 int pad_size(int policy, int corrMod, double nu, const double corrL[3], const double xStep[3],
              const int Np[3], double tol, int P[3]) {
   for (int d = 0; d < 3; ++d) {
@@ -317,6 +335,12 @@ int pad_size(int policy, int corrMod, double nu, const double corrL[3], const do
         p <<= 1;
         if (p > (1 << 24)) return SCARL_EINVAL;
       }
+    } else if (policy == 3) {
+      if (!(tol > 0.0 && tol < 1.0) || !(corrL[d] > 0.0) || !(xStep[d] > 0.0)) return SCARL_EINVAL;
+      p = next_smooth(Np[d]);
+      while (p && axis_correlation(corrMod, nu, corrL[d], (p - Np[d] + 1) * xStep[d]) > tol)
+        p = next_smooth(p + 1);
+      if (!p) return SCARL_EINVAL;  // beyond the largest supported length
     } else {
       return SCARL_EINVAL;
     }

@@ -28,6 +28,9 @@ void unity_partition_weights(const int Np[3], const int No[3], int partitionType
 int shino_sizes(const int Np[3], const double xRange[3], const double corrL[3], int sz_c[3],
                 int sz_Sk[3], double delta_k[3]);
 double axis_correlation(int corrMod, double nu, double l, double r);
+// Padded lengths the generator runs: 8..2048, a power of two or m 2^a with
+// m = 3, 5, 7 and 2^a >= 16.
+bool fft_length_supported(int n);
 int pad_size(int policy, int corrMod, double nu, const double corrL[3], const double xStep[3],
              const int Np[3], double tol, int P[3]);
 int ensemble_draw(uint64_t seed, long long first, int n, const int* choices, int nchoices,

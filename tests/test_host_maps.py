@@ -203,6 +203,30 @@ def test_pad_size_auto_is_minimal(cm, nu):
     assert list(full) == [1024, 1024, 1024]
 
 
+SMOOTH_LENGTHS = sorted({2 ** a for a in range(3, 12)} |
+                        {m * 2 ** a for m in (3, 5, 7) for a in range(4, 10) if m * 2 ** a <= 2048})
+
+
+@pytest.mark.parametrize("cm,nu", [(1, 0.5), (3, 0.5), (2, 0.8)])
+def test_pad_size_smooth_is_minimal(cm, nu):
+    """SMOOTH applies AUTO's rule over every supported length (powers of two
+    and 3, 5, 7 times 2^a >= 16, up to 2048): the chosen length passes, every
+    smaller supported length >= Np fails, and it is never above AUTO's."""
+    for Np, cl, dx in [((297, 277, 267), (40, 20, 10), (1, 1, 1)), ((50, 9, 120), (3, 7, 12), (0.5, 1, 2)),
+                       ((608, 608, 1024), (64, 64, 32), (1, 1, 1))]:
+        for tol in (1e-2, 1e-3):
+            P = S.pad_size(S.PAD_SMOOTH, cm, cl, dx, Np, nu, tol)
+            A = S.pad_size(S.PAD_AUTO, cm, cl, dx, Np, nu, tol)
+            for d in range(3):
+                assert P[d] in SMOOTH_LENGTHS and P[d] >= Np[d] and P[d] <= A[d]
+                ok = lambda p: S.axis_correlation(cm, cl[d], (p - Np[d] + 1) * dx[d], nu) <= tol
+                assert ok(P[d])
+                assert not any(ok(p) for p in SMOOTH_LENGTHS if Np[d] <= p < P[d])
+    # the headline deck: 513^3 field, exponential l = (40, 20, 10), 2x2x2 tiles
+    P = S.pad_size(S.PAD_SMOOTH, 3, (40, 20, 10), (1, 1, 1), (297, 277, 267), 0.5, 1e-3)
+    assert list(P) == [448, 384, 320]
+
+
 def test_ensemble_draw_matches_oracle(oracle):
     """Shapes and correlation lengths of ensemble realisations: library and
     oracle draw the same Philox words, bit-exact."""
