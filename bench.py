@@ -5,7 +5,9 @@ correlation, anisotropic correlation lengths (40, 20, 10) at spacing 1,
 lognormal marginal (mean 1, CV 0.3), 2x2x2 tiles with overlap 2 l, padded
 periodic generation in FP32 with the FP64 spectral normalisation and the
 z-axis DFT of pass 1 as split-BF16 tensor-core products (SCARL_SPLIT_BF16;
-field rel-L2 against FP64 reported, gate 1e-5).  One step generates one
+field rel-L2 against FP64 reported, gate 1e-5), on the SMOOTH padded grid
+(the smallest lengths 2^a or 3, 5, 7 x 2^a whose nearest periodic image adds
+at most 1e-3 to any covariance in a tile: 448 x 384 x 320).  One step generates one
 complete field (8 tiles x 3 passes).  Synthetic: the field is drawn from
 seeded Philox normals; nothing is read from disk.  Beside it: the same grid
 with every DFT on the CUDA cores in FP32 (fp32_path) and the plain GPU path
@@ -170,9 +172,10 @@ def cpu_sample(lay, P, steps, warmup, stride=8):
     mpts = (field_points / nb) / (dt * stride) / 1e6
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": round(mpts, 4), "unit": "Mpoints/s", "cores": cores, "kind": "port",
-            "sample": f"oracle (C, FP64, OpenMP) on every {stride}th line of the three passes of "
-                      f"tile 0 of {nb}; {dt:.3f} s per sample, scaled x{stride} to one tile and "
-                      f"by 1/{nb} of the {field_points}-point field"}, dt
+            "sample": f"oracle (C, FP64, OpenMP, radix-2 FFT) on every {stride}th line of the three "
+                      f"passes of tile 0 of {nb} on the power-of-two padded grid {list(P)}; "
+                      f"{dt:.3f} s per sample, scaled x{stride} to one tile and by 1/{nb} of the "
+                      f"{field_points}-point field"}, dt
 
 
 def run_reference(args, rank):
@@ -185,7 +188,7 @@ def run_reference(args, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": config_of(lay, pads(S, lay, S.PAD_AUTO)),
+            "config": config_of(lay, pads(S, lay, S.PAD_SMOOTH)),
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "Mpoints/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -194,7 +197,7 @@ def run_reference(args, rank):
 
 def bench_ensemble(S, ctx, stream, steps, warmup, rank=0, dist=None):
     """The 256-realisation ensemble of uneven grids: axes from {64, ..., 256},
-    isotropic l in [4, 32], exponential, seeds 0-255, FP32, AUTO padding.
+    isotropic l in [4, 32], exponential, seeds 0-255, FP32, SMOOTH padding.
     Batched launches replayed from a CUDA graph against the same realisations
     generated one scarl_gen_padded call at a time (same padded grids)."""
     import numpy as np
@@ -208,11 +211,12 @@ def bench_ensemble(S, ctx, stream, steps, warmup, rank=0, dist=None):
     total = int(off[-1])
     out = torch.empty(total, dtype=torch.float32, device="cuda")
     seeds = R.realisation_seeds(first, first + 256)
-    P = [[int(v) for v in S.pad_size(S.PAD_AUTO, 3, c, (1, 1, 1), n, 0.5, PAD_TOL)]
+    P = [[int(v) for v in S.pad_size(S.PAD_SMOOTH, 3, c, (1, 1, 1), n, 0.5, PAD_TOL)]
          for n, c in zip(Np, cl)]
 
     def batched():
-        S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_tol=PAD_TOL, seeds=seeds, autotune=True, out=out)
+        S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_policy=S.PAD_SMOOTH, pad_tol=PAD_TOL, seeds=seeds,
+                       autotune=True, out=out)
 
     def single():
         for i in range(256):
@@ -246,14 +250,16 @@ def bench_ensemble(S, ctx, stream, steps, warmup, rank=0, dist=None):
     host = torch.empty(total, dtype=torch.float32, pin_memory=True)
     hnp = host.numpy()
     ctx.set_stream(0)
-    S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_tol=PAD_TOL, seeds=seeds, autotune=True, out=hnp)
+    S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_policy=S.PAD_SMOOTH, pad_tol=PAD_TOL, seeds=seeds,
+                   autotune=True, out=hnp)
     c0 = ctx.counters()
     t0 = time.perf_counter()
     k = max(2, steps // 5)
     if dist is not None:
         dist.barrier()
     for _ in range(k):
-        S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_tol=PAD_TOL, seeds=seeds, autotune=True, out=hnp)
+        S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_policy=S.PAD_SMOOTH, pad_tol=PAD_TOL, seeds=seeds,
+                   autotune=True, out=hnp)
     e2e_s = R.max_over_ranks((time.perf_counter() - t0) / k, dist, "cuda")
     c1 = ctx.counters()
     ctx.set_stream(stream.cuda_stream)
@@ -262,7 +268,7 @@ def bench_ensemble(S, ctx, stream, steps, warmup, rank=0, dist=None):
     total = int(R.sum_over_ranks(total, dist, "cuda"))
     return {"workload": "256 realisations per GPU, axes uniform in {64,96,128,160,192,256}, "
                         "isotropic l uniform in [4,32], exponential, seeds 0-255 (rank k: "
-                        f"256k-256k+255), FP32, AUTO padding (image error <= {PAD_TOL:g})",
+                        f"256k-256k+255), FP32, SMOOTH padding (image error <= {PAD_TOL:g})",
             "points": total, "padded_points": pvol,
             "value": round(total / (ms_b * 1e-3) / 1e6, 2), "unit": "Mpoints/s",
             "ms_per_ensemble": round(ms_b, 3), "gpu_launches_per_ensemble": int(launches),
@@ -279,7 +285,7 @@ def bench_ensemble(S, ctx, stream, steps, warmup, rank=0, dist=None):
 
 def bench_large_field(S, ctx, stream, steps, rank=0, dist=None):
     """2048 x 2048 x 1024 FP32 field, Gaussian l = (64, 64, 32), Gaussian
-    marginal (variance 1), 4 x 4 x 1 tiles with a 128-point overlap, AUTO
+    marginal (variance 1), 4 x 4 x 1 tiles with a 128-point overlap, SMOOTH
     padding; then the streamed FP64 mean, variance and axis covariance up to
     lag 256 of the finished field."""
     import torch
@@ -292,10 +298,10 @@ def bench_large_field(S, ctx, stream, steps, rank=0, dist=None):
     L = [int(v) for v in lay["L"]]
     n = L[0] * L[1] * L[2]
     field = torch.empty(n, dtype=torch.float32, device="cuda")
-    P = [int(v) for v in S.pad_size(S.PAD_AUTO, 1, (64, 64, 32), lay["xStep"], lay["Np"], 0.5, PAD_TOL)]
+    P = [int(v) for v in S.pad_size(S.PAD_SMOOTH, 1, (64, 64, 32), lay["xStep"], lay["Np"], 0.5, PAD_TOL)]
 
     def gen():
-        S.generate_sample(ctx, s, dtype=S.F32, nb_procs=16, topo=(4, 4, 1), pad_policy=S.PAD_AUTO,
+        S.generate_sample(ctx, s, dtype=S.F32, nb_procs=16, topo=(4, 4, 1), pad_policy=S.PAD_SMOOTH,
                           pad_tol=PAD_TOL, autotune=True, out=field)
 
     gen()
@@ -337,7 +343,7 @@ def bench_large_field(S, ctx, stream, steps, rank=0, dist=None):
             if k != "k_cov_lags":
                 kern[k]["gbs"] = round(n * 4 / (tot / cnt * 1e-3) / 1e9, 1)
     return {"workload": "2048x2048x1024 FP32, Gaussian l=(64,64,32), Gaussian marginal var 1, "
-                        "4x4x1 tiles, overlap 128, AUTO padding; streamed FP64 mean, variance and "
+                        "4x4x1 tiles, overlap 128, SMOOTH padding; streamed FP64 mean, variance and "
                         "axis covariance up to lag 256",
             "points": n * world, "padded_grid": P,
             "value": round(world * n / (ms_gen * 1e-3) / 1e6, 2),
@@ -354,7 +360,8 @@ def config_of(lay, P):
                         "CV 0.3, 2x2x2 tiles, overlap 2l, padded periodic C2R FP32",
             "global_points": [int(v) for v in lay["L"]], "tile_points": [int(v) for v in lay["Np"]],
             "overlap_points": [int(v) for v in lay["Np_ovlp"]], "tiles": [int(v) for v in lay["topo"]],
-            "padded_grid": P, "pad_policy": f"auto (periodic image error <= {PAD_TOL:g})",
+            "padded_grid": P, "pad_policy": f"smooth: lengths 2^a or 3, 5, 7 x 2^a, periodic image "
+                                            f"error <= {PAD_TOL:g}",
             "l2": "working set larger than L2 (field 0.54 GB, intermediate >= 0.15 GB per tile)"}
 
 
@@ -416,7 +423,7 @@ def main():
         L = [int(v) for v in lay["L"]]
         field = torch.empty(L[0] * L[1] * L[2], dtype=torch.float32, device="cuda")
         S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=S.F32 | S.SPLIT_BF16,
-                          nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO, pad_tol=PAD_TOL, out=field)
+                          nb_procs=8, topo=TOPO, pad_policy=S.PAD_SMOOTH, pad_tol=PAD_TOL, out=field)
         ctx.sync()
         print(json.dumps({"profile_tile": "ok", "launches": ctx.counters()["launches"]}))
         ctx.close()
@@ -434,11 +441,12 @@ def main():
     npts = L[0] * L[1] * L[2]
     field = torch.empty(npts, dtype=torch.float32, device="cuda")
 
-    P_auto, P_full = pads(S, lay, S.PAD_AUTO), pads(S, lay, S.PAD_FULL)
+    P_auto, P_full = pads(S, lay, S.PAD_SMOOTH), pads(S, lay, S.PAD_FULL)
+    P_pow2 = pads(S, lay, S.PAD_AUTO)
 
     HEAD = S.F32 | S.SPLIT_BF16  # headline precision: split-BF16 tensor-core z stage
 
-    def step(out=field, dtype=HEAD, policy=S.PAD_AUTO):
+    def step(out=field, dtype=HEAD, policy=S.PAD_SMOOTH):
         S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=dtype, nb_procs=8,
                           topo=TOPO, pad_policy=policy, pad_tol=PAD_TOL, autotune=True, out=out)
 
@@ -449,6 +457,7 @@ def main():
     for _ in range(args.warmup):
         step()
         step(dtype=S.F32)
+        step(policy=S.PAD_AUTO)
         step(dtype=S.F32, policy=S.PAD_FULL)
     torch.cuda.synchronize()
 
@@ -494,6 +503,8 @@ def main():
              "pad_policy": "full, 2^ceil(log2(2 Np)) (SRC_F/fftw_ScaRL.f90:194)"}
     # ---- the same padded grid as the headline with every DFT in FP32
     ms_f32 = timed_steps(dtype=S.F32)
+    # ---- the split path on the power-of-two grid of the AUTO rule
+    ms_pow2 = timed_steps(policy=S.PAD_AUTO)
 
     # ---- per-kernel device times (separate, profiled steps)
     ctx.profile(True)
@@ -544,6 +555,8 @@ def main():
     rel32, max32 = rel_to_f64(S.F32)
     rel, relmax = rel_to_f64(HEAD)
     del f64
+    pow2 = {"value": round(world * npts / (ms_pow2 * 1e-3) / 1e6, 2), "ms_per_step": round(ms_pow2, 4),
+            "padded_grid": P_pow2, "pad_policy": "auto: smallest powers of two under the same rule"}
     fp32 = {"value": round(world * npts / (ms_f32 * 1e-3) / 1e6, 2), "ms_per_step": round(ms_f32, 4),
             "padded_grid": P_auto, "precision": "f32 (every DFT on the CUDA cores)",
             "rel_l2_vs_fp64": rel32, "max_err_vs_fp64": max32}
@@ -552,13 +565,13 @@ def main():
     host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
     hnp = host.numpy()
     ctx.set_stream(0)  # library-owned stream; host calls synchronise inside
-    S.generate_sample(ctx, sample, dtype=HEAD, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
+    S.generate_sample(ctx, sample, dtype=HEAD, nb_procs=8, topo=TOPO, pad_policy=S.PAD_SMOOTH,
                       pad_tol=PAD_TOL, autotune=True, out=hnp)
     c0 = ctx.counters()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        S.generate_sample(ctx, sample, dtype=HEAD, nb_procs=8, topo=TOPO, pad_policy=S.PAD_AUTO,
+        S.generate_sample(ctx, sample, dtype=HEAD, nb_procs=8, topo=TOPO, pad_policy=S.PAD_SMOOTH,
                           pad_tol=PAD_TOL, autotune=True, out=hnp)
     e2e_s = (time.perf_counter() - t0) / args.steps
     c1 = ctx.counters()
@@ -583,7 +596,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu, _ = cpu_sample(lay, P_auto, 1, 0)
+        cpu, _ = cpu_sample(lay, P_pow2, 1, 0)
 
     if dist is not None:
         dist.barrier()
@@ -595,7 +608,8 @@ def main():
                 "data": "synthetic (Philox normals, seeded per rank)",
                 "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "max_err_vs_fp64": relmax,
                 "roofline": roof, "kernels": kern, "launch_variants": tuned, "plain_path": plain,
-                "fp32_path": fp32, "speedup_vs_plain_path": round(ms_full / ms, 3),
+                "fp32_path": fp32, "pow2_grid_path": pow2,
+                "speedup_vs_plain_path": round(ms_full / ms, 3),
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
                 "ensemble": ens, "large_field": large}
         print(json.dumps(line), flush=True)

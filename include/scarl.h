@@ -301,7 +301,7 @@ int scarl_ensemble_draw(uint64_t seed, long long first, int n, const int* choice
  * lengths corrL[3i..], Philox key seeds[i] (NULL: i) and stream streams[i]
  * (NULL: 0).  Its field, column-major, starts at element
  * sum_{j<i} Np_j0 Np_j1 Np_j2 of out (device or host pointer).  Padded grids
- * follow pad_policy / pad_tol per realisation; margiFirst 0 leaves the
+ * follow pad_policy (SCARL_PAD_FULL, _AUTO or _SMOOTH) / pad_tol per realisation; margiFirst 0 leaves the
  * standard field, 1 / 2 apply the Gaussian / lognormal marginal of avg,
  * std_dev.  Realisations are grouped by line length in each of the three
  * passes and every group runs as one batched launch; the first call for a

@@ -2208,7 +2208,7 @@ int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* N
   if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
   if (corrMod < 1 || corrMod > 3) return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
   if (corrMod == SCARL_CM_VON_KARMAN && !(nu > 0.0)) return fail(ctx, SCARL_EINVAL, "nu must be > 0");
-  if (pad_policy != SCARL_PAD_FULL && pad_policy != SCARL_PAD_AUTO)
+  if (pad_policy != SCARL_PAD_FULL && pad_policy != SCARL_PAD_AUTO && pad_policy != SCARL_PAD_SMOOTH)
     return fail(ctx, SCARL_EINVAL, "unknown padding policy");
   if (margiFirst < 0 || margiFirst > 2) return fail(ctx, SCARL_EINVAL, "First-order marginal not detected");
   const double tol = pad_tol > 0.0 ? pad_tol : 1e-3;

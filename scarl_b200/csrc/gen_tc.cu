@@ -56,7 +56,8 @@ struct TcCfg {
   static constexpr int STAGEB = N / NCH * STAGE_LD * 8;
   static constexpr int REGION = (2 * AB > STAGEB ? 2 * AB : STAGEB);
   static constexpr int B1B = (K1 / 8) * SBO1, B2B = (K2 / 8) * SBO2;
-  static constexpr int TMEM_COLS = LB * N / 64;
+  static constexpr int TMEM_USED = LB * N / 64;  // = T1 K1 = T2 K2
+  static constexpr int TMEM_COLS = TMEM_USED <= 32 ? 32 : TMEM_USED <= 64 ? 64 : TMEM_USED <= 128 ? 128 : 256;
   static constexpr int OFF_AH = 0, OFF_AL = AB, OFF_B1H = REGION, OFF_B1L = OFF_B1H + B1B;
   static constexpr int OFF_B2H = OFF_B1L + B1B, OFF_B2L = OFF_B2H + B2B;
   static constexpr int OFF_ZT = OFF_B2L + B2B;   // z factor of the amplitude, N floats
@@ -64,11 +65,10 @@ struct TcCfg {
   static constexpr int OFF_BAR = OFF_TW + 8 * N;  // mbarrier (8 B) + tensor-memory slot (4 B)
   static constexpr int SMEM = OFF_BAR + 16;
   static_assert(ROWS1 == THREADS, "one stage-1 row per thread");
-  static_assert((N1 / NCH) % 16 == 0, "output chunks of whole 16-column tensor-memory loads");
-  static_assert(ROWS2 % 128 == 0 && T1 * K1 == TMEM_COLS && T2 * K2 == TMEM_COLS, "tiling");
-  static_assert(N1 % 8 == 0 && N2 % 16 == 0 && K1 <= 256 && K2 <= 256, "radices");
-  static_assert(TMEM_COLS >= 32 && TMEM_COLS * CTAS_PER_SM <= 512 &&
-                (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory");
+  static_assert(N1 / NCH == 4 || N1 / NCH == 8 || N1 / NCH == 16, "output chunk widths");
+  static_assert(ROWS2 % 128 == 0 && T1 * K1 == TMEM_USED && T2 * K2 == TMEM_USED, "tiling");
+  static_assert((N1 == 8 || N1 == 16 || N1 == 32) && N2 % 8 == 0 && K1 <= 256, "radices");
+  static_assert(TMEM_USED <= 256 && TMEM_COLS * CTAS_PER_SM <= 512, "tensor memory");
   static_assert(CTAS_PER_SM * (SMEM + 1024) <= 228 * 1024, "shared memory");
 };
 
@@ -95,16 +95,21 @@ __device__ __forceinline__ uint32_t kmaj_off(int row, int k, int sbo) {
 }
 
 // The split DFT matrix of length L as a (2L x 2L) K-major B operand:
-// row n = output (re n < L, im n >= L), column k = input (re / im).
-template <int L, int SBO>
+// row n = output (re n < L, im n >= L); column k = input, in natural order
+// (re k < L, im k >= L) or, with DRAW_ORDER, in the stage-1 operand's draw
+// order: k = 4 d + part with part 0 / 1 = re / im of input d, 2 / 3 = re / im
+// of input d + L / 2 (the two modes of one Philox draw).
+template <int L, int SBO, bool DRAW_ORDER>
 __device__ void fill_dft_b(unsigned char* hi, unsigned char* lo) {
   for (int idx = threadIdx.x; idx < 4 * L * L; idx += blockDim.x) {
     const int n = idx / (2 * L), k = idx % (2 * L);
-    const int no = n % L, ki = k % L;
+    const int no = n % L;
+    const int ki = DRAW_ORDER ? k / 4 + ((k & 2) ? L / 2 : 0) : k % L;
+    const bool im_in = DRAW_ORDER ? (k & 1) != 0 : k >= L;
     const int m = (no * ki) % L;
     double s, c;
     sincospi(2.0 * (double)m / (double)L, &s, &c);
-    const bool im_out = n >= L, im_in = k >= L;
+    const bool im_out = n >= L;
     const double v = (im_out == im_in) ? c : (im_out ? s : -s);
     const __nv_bfloat16 h = __double2bfloat16(v);
     const __nv_bfloat16 t = __double2bfloat16(v - (double)__bfloat162float(h));
@@ -130,8 +135,8 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
 
   if (tid == 0) tc::mbar_init(bar, 1);
   if (warp == 0) tc::tmem_alloc(tc::smem_u32(tslot), Cfg::TMEM_COLS);
-  fill_dft_b<N2, Cfg::SBO1>(sm + Cfg::OFF_B1H, sm + Cfg::OFF_B1L);
-  fill_dft_b<N1, Cfg::SBO2>(sm + Cfg::OFF_B2H, sm + Cfg::OFF_B2L);
+  fill_dft_b<N2, Cfg::SBO1, true>(sm + Cfg::OFF_B1H, sm + Cfg::OFF_B1L);
+  fill_dft_b<N1, Cfg::SBO2, false>(sm + Cfg::OFF_B2H, sm + Cfg::OFF_B2L);
   float* zt = reinterpret_cast<float*>(sm + Cfg::OFF_ZT);
   float2* tw2 = reinterpret_cast<float2*>(sm + Cfg::OFF_TW);
   {
@@ -183,42 +188,42 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
         if (AMP == AMP_RECIP) return __fdividef(fx, fy + zt[kz]);
         return fx * powf(fy + zt[kz], (float)a.expo);
       };
-      const int tile = R1 >> 7, r = R1 & 127;
-      const uint32_t rowoff = (uint32_t)(tile * Cfg::TILE1 + (r >> 3) * Cfg::SBO1 + (r & 7) * 16);
-#pragma unroll 1
-      for (int j = 0; j < N2 / 16; ++j) {
-        float re0[8], im0[8], re1[8], im1[8];
+      // K-major row R1 (tiles of 128 rows are contiguous); K in draw order:
+      // draw d (modes k2 = d and d + N2/2) fills K columns 4d .. 4d + 3, so
+      // two draws make one 16-byte chunk
+      const uint32_t rowoff = (uint32_t)((R1 >> 3) * Cfg::SBO1 + (R1 & 7) * 16);
+      auto put = [&](const float* v, int chunk) {
+        uint4 h, t;
+        tc::split2(v[0], v[1], h.x, t.x);
+        tc::split2(v[2], v[3], h.y, t.y);
+        tc::split2(v[4], v[5], h.z, t.z);
+        tc::split2(v[6], v[7], h.w, t.w);
+        const uint32_t off = rowoff + chunk * Cfg::LBO1;
+        *reinterpret_cast<uint4*>(AH + off) = h;
+        *reinterpret_cast<uint4*>(AL + off) = t;
+      };
+#pragma unroll 2
+      for (int d0 = 0; d0 < N2 / 2; d0 += 4) {  // four draws: two chunks
+        float v[16];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int kz0 = s_k1 + N1 * (8 * j + e);
+        for (int e = 0; e < 4; ++e) {
+          const int kz0 = s_k1 + N1 * (d0 + e);
           if (valid) {
             const uint64_t c = (uint64_t)l + mz * (uint64_t)kz0;
             const u32x4 o = philox4x32_10_ks({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.ks);
             const float2 x0 = split_normals(o.x, o.y);
             const float2 x1 = split_normals(o.z, o.w);
             const float A0 = amp(kz0), A1 = amp(kz0 + N / 2);
-            re0[e] = A0 * x0.x; im0[e] = A0 * x0.y;
-            re1[e] = A1 * x1.x; im1[e] = A1 * x1.y;
+            v[4 * e] = A0 * x0.x;
+            v[4 * e + 1] = A0 * x0.y;
+            v[4 * e + 2] = A1 * x1.x;
+            v[4 * e + 3] = A1 * x1.y;
           } else {
-            re0[e] = im0[e] = re1[e] = im1[e] = 0.f;
+            v[4 * e] = v[4 * e + 1] = v[4 * e + 2] = v[4 * e + 3] = 0.f;
           }
         }
-        // K chunks: re k2 in [8j, 8j+8) -> j, re k2 + N2/2 -> j + N2/16,
-        // im -> the same plus N2/8
-        auto put = [&](const float (&v)[8], int chunk) {
-          uint4 h, t;
-          tc::split2(v[0], v[1], h.x, t.x);
-          tc::split2(v[2], v[3], h.y, t.y);
-          tc::split2(v[4], v[5], h.z, t.z);
-          tc::split2(v[6], v[7], h.w, t.w);
-          const uint32_t off = rowoff + chunk * Cfg::LBO1;
-          *reinterpret_cast<uint4*>(AH + off) = h;
-          *reinterpret_cast<uint4*>(AL + off) = t;
-        };
-        put(re0, j);
-        put(re1, j + N2 / 16);
-        put(im0, N2 / 8 + j);
-        put(im1, N2 / 8 + N2 / 16 + j);
+        put(v, d0 / 2);
+        put(v + 8, d0 / 2 + 1);
       }
     }
     tc::fence_smem_to_async();
@@ -248,45 +253,38 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
     if (!__syncthreads_and(ok)) { ok = false; break; }
     tc::fence_after_sync();
     // ---- stage-1 rows back, twiddled, split into the MN-major stage-2
-    //      operand: element (row n2 + N2 line, k) at
-    //      tile + (row % 128 / 8) SBO2 + (k / 8) LBO2 + (k % 8) 16 + (n2 % 8) 2,
+    //      operand: element (row n2 + N2 line, k), rows in 8-element M groups
+    //      SBO2 apart (128-row tiles contiguous), K groups LBO2 apart,
     //      k = k1 (re) or N1 + k1 (im) ----
 #pragma unroll 1
     for (int t = warp >> 2; t < Cfg::T1; t += Cfg::THREADS / 128) {
       const int R = t * 128 + q * 32 + lane;
       const int line = (R >> 3) % LB, k1 = (R & 7) + 8 * (R / (8 * LB));
       const float2* twk = tw2 + k1;  // e^{2 pi i n2 k1 / N} at twk[n2 N1]
-      const uint32_t row0 = (uint32_t)(N2 * line);
-      const uint32_t base = (row0 >> 7) * Cfg::TILE2 + ((row0 & 127) >> 3) * Cfg::SBO2 +
-                            (k1 >> 3) * Cfg::LBO2 + (k1 & 7) * 16;
+      const uint32_t base = (uint32_t)(N2 * line / 8) * Cfg::SBO2 + (k1 >> 3) * Cfg::LBO2 + (k1 & 7) * 16;
       constexpr uint32_t IM = (N1 / 8) * Cfg::LBO2;  // im K groups follow the re ones
-#pragma unroll
-      for (int g = 0; g < N2 / 16; ++g) {  // 16 n2 (two M groups) per tensor-memory read
-        float v[32];
-        const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + t * Cfg::K1 + g * 16;
-        tc::tmem_ld16(col, v);            // re of n2 = 16 g ..
-        tc::tmem_ld16(col + N2, v + 16);  // im
+      const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + t * Cfg::K1;
+#pragma unroll 2
+      for (int g = 0; g < N2 / 8; ++g) {  // 8 n2: one M group, one 16-byte store per part
+        float v[16];
+        tc::tmem_ld<8>(col + 8 * g, v);           // re of n2 = 8 g ..
+        tc::tmem_ld<8>(col + N2 + 8 * g, v + 8);  // im
         tc::tmem_wait_ld();
+        uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {     // 8 n2 -> one 16-byte store per part
-          uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-          for (int e = 0; e < 8; e += 2) {
-            const int n2 = 16 * g + 8 * h + e;
-            const float2 w0 = twk[n2 * N1], w1 = twk[(n2 + 1) * N1];
-            const float xr0 = v[8 * h + e], xi0 = v[16 + 8 * h + e];
-            const float xr1 = v[8 * h + e + 1], xi1 = v[16 + 8 * h + e + 1];
-            const float yr0 = xr0 * w0.x - xi0 * w0.y, yi0 = xr0 * w0.y + xi0 * w0.x;
-            const float yr1 = xr1 * w1.x - xi1 * w1.y, yi1 = xr1 * w1.y + xi1 * w1.x;
-            tc::split2(yr0, yr1, rh[e / 2], rl[e / 2]);
-            tc::split2(yi0, yi1, ih[e / 2], il[e / 2]);
-          }
-          const uint32_t off = base + (uint32_t)(2 * g + h) * Cfg::SBO2;
-          *reinterpret_cast<uint4*>(AH + off) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-          *reinterpret_cast<uint4*>(AL + off) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-          *reinterpret_cast<uint4*>(AH + off + IM) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-          *reinterpret_cast<uint4*>(AL + off + IM) = make_uint4(il[0], il[1], il[2], il[3]);
+        for (int e = 0; e < 8; e += 2) {
+          const int n2 = 8 * g + e;
+          const float2 w0 = twk[n2 * N1], w1 = twk[(n2 + 1) * N1];
+          const float yr0 = v[e] * w0.x - v[8 + e] * w0.y, yi0 = v[e] * w0.y + v[8 + e] * w0.x;
+          const float yr1 = v[e + 1] * w1.x - v[9 + e] * w1.y, yi1 = v[e + 1] * w1.y + v[9 + e] * w1.x;
+          tc::split2(yr0, yr1, rh[e / 2], rl[e / 2]);
+          tc::split2(yi0, yi1, ih[e / 2], il[e / 2]);
         }
+        const uint32_t off = base + (uint32_t)g * Cfg::SBO2;
+        *reinterpret_cast<uint4*>(AH + off) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+        *reinterpret_cast<uint4*>(AL + off) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+        *reinterpret_cast<uint4*>(AH + off + IM) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+        *reinterpret_cast<uint4*>(AL + off + IM) = make_uint4(il[0], il[1], il[2], il[3]);
       }
     }
     tc::fence_smem_to_async();
@@ -329,11 +327,8 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
         const int line = R / N2, n2 = R % N2;
         float v[2 * CN1];
         const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + t * Cfg::K2 + ch * CN1;
-#pragma unroll
-        for (int c = 0; c < CN1 / 16; ++c) {
-          tc::tmem_ld16(col + c * 16, v + c * 16);             // re of n1 = ch CN1 + ..
-          tc::tmem_ld16(col + N1 + c * 16, v + CN1 + c * 16);  // im
-        }
+        tc::tmem_ld<CN1>(col, v);            // re of n1 = ch CN1 + ..
+        tc::tmem_ld<CN1>(col + N1, v + CN1);  // im
         tc::tmem_wait_ld();
 #pragma unroll
         for (int n1 = 0; n1 < CN1; ++n1)
@@ -409,13 +404,16 @@ cudaError_t launch_amp(const GenArgs& a, cudaStream_t s) {
 }  // namespace
 
 // Line lengths with a tensor-core pass 1 (FP32 output, Philox spectrum):
-// N = N1 x N2 = 16 x 16, 16 x 32, 32 x 32.
-bool gen_z_tc_supported(int N) { return N == 256 || N == 512 || N == 1024; }
+// N = N1 x N2 = 16 x 16, 8 x 40, 16 x 24, 16 x 32, 32 x 32 (the others do
+// not fit two CTAs per SM).
+bool gen_z_tc_supported(int N) { return N == 256 || N == 320 || N == 384 || N == 512 || N == 1024; }
 
 cudaError_t launch_gen_z_tc(const GenArgs& a, cudaStream_t s) {
   if (!a.status || a.spec != SPEC_PHILOX) return cudaErrorInvalidValue;
   switch (a.P[2]) {
     case 256: return launch_amp<16, 16, 16, 1>(a, s);
+    case 320: return launch_amp<8, 40, 32, 2>(a, s);
+    case 384: return launch_amp<16, 24, 16, 1>(a, s);
     case 512: return launch_amp<16, 32, 16, 1>(a, s);
     case 1024: return launch_amp<32, 32, 8, 2>(a, s);
     default: return cudaErrorInvalidValue;

@@ -41,6 +41,11 @@ def _ran_tc(ctx, fn):
     ((9, 6, 600), (16, 16, 1024), (1, 1, 1), (3, 3, 60), 3, 0.5),     # N = 32 x 32, two chunks
     ((5, 7, 1024), (8, 16, 1024), (1, 1, 1), (2, 2, 90), 2, 0.8),     # N = 32 x 32, all z
     ((6, 5, 400), (16, 8, 1024), (1, 1, 1), (2, 2, 40), 1, 0.5),      # first chunk only
+    ((10, 7, 267), (32, 16, 320), (1, 1, 1), (3, 3, 10), 3, 0.5),     # N = 8 x 40
+    ((9, 5, 320), (16, 8, 320), (1, 1, 1), (2, 2, 30), 1, 0.5),       # N = 8 x 40, all z
+    ((5, 6, 100), (8, 16, 320), (1, 1, 1), (2, 2, 15), 2, 0.8),       # first chunk only
+    ((12, 8, 300), (48, 16, 384), (1, 1, 1), (3, 3, 25), 3, 0.5),     # N = 16 x 24
+    ((6, 5, 384), (16, 8, 384), (1, 1, 1), (2, 2, 40), 1, 0.5),       # N = 16 x 24, all z
 ])
 def test_split_vs_oracle(ctx, oracle, Np, P, dx, cl, cm, nu):
     ref = oracle.gen_padded(Np, P, dx, cl, cm, nu, 1, seed=77, stream=3)
@@ -81,13 +86,15 @@ def test_split_rejected_for_fp64(ctx):
 def test_split_blended_sample_vs_fp64(ctx):
     """The headline deck (512^3 -> 513^3, exponential, l = (40, 20, 10),
     lognormal mean 1 CV 0.3, 2x2x2 tiles, overlap 2 l) on the AUTO padded
-    grid 512^3: split FP32 against FP64 on the same normals."""
+    grid 512^3 and the SMOOTH grid 448 x 384 x 320: split FP32 against FP64
+    on the same normals."""
     s = S.make_sample((0, 0, 0), (512, 512, 512), (40, 20, 10), (2, 2, 2), (41, 21, 11),
                       corrMod=3, margiFirst=2, avg=1.0, std_dev=0.3)
-    kw = dict(nb_procs=8, topo=(2, 2, 2), pad_policy=S.PAD_AUTO)
-    f64, lay = S.generate_sample(ctx, s, dtype=S.F64, **kw)
-    (f32s, _), st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, dtype=SPLIT, **kw))
-    assert st["k_gen_z_tc"][1] == 8  # one launch per tile
-    err = rel(f32s, f64)
-    print(f"513^3 split rel-L2 {err:.2e}")
-    assert err < TOL
+    for policy in (S.PAD_AUTO, S.PAD_SMOOTH):
+        kw = dict(nb_procs=8, topo=(2, 2, 2), pad_policy=policy)
+        f64, lay = S.generate_sample(ctx, s, dtype=S.F64, **kw)
+        (f32s, _), st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, dtype=SPLIT, **kw))
+        assert st["k_gen_z_tc"][1] == 8  # one launch per tile
+        err = rel(f32s, f64)
+        print(f"513^3 split rel-L2 {err:.2e} (policy {policy})")
+        assert err < TOL
