@@ -166,7 +166,8 @@ template <SmemOrder O, int B, int LS, int SK> __device__ __forceinline__ int sid
 }
 
 // One Stockham stage reading/writing shared memory (middle stages).
-// tw: e^{+2 pi i m / (N * twmul)} table, so w_{Ns R}^{q} = tw[q * (N / (Ns R)) * twmul].
+// tw: e^{+2 pi i m / (N * twmul)} table, so w_{Ns R}^{q} = tw[q * (N / (Ns R)) * twmul];
+// it may live in global or shared memory (plain loads, no read-only-cache path).
 template <typename C, int N, int E, int R, int Ns, SmemOrder O, int B, int LS, int SK>
 __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, int t,
                                                     const C* __restrict__ tw, int twmul) {
@@ -186,7 +187,7 @@ __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, i
     const int k = j % Ns;
 #pragma unroll
     for (int r = 1; r < R; ++r) {
-      const C w = __ldg(reinterpret_cast<const C*>(tw) + (size_t)(r * k) * (N / (Ns * R)) * twmul);
+      const C w = tw[(size_t)(r * k) * (N / (Ns * R)) * twmul];  // global or shared table
       v[q * R + r] = cmul(v[q * R + r], w);
     }
     dft_reg<R>(v + q * R);
@@ -264,7 +265,7 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
       const int k = j % NsL;
 #pragma unroll
       for (int r = 1; r < RL; ++r) {
-        const C w = __ldg(reinterpret_cast<const C*>(tw) + (size_t)(r * k) * twmul);
+        const C w = tw[(size_t)(r * k) * twmul];
         v[q * RL + r] = cmul(v[q * RL + r], w);
       }
       dft_reg<RL>(v + q * RL);

@@ -191,6 +191,13 @@ __device__ __forceinline__ void mid_y_body(const GenArgs& a, int bx, int z) {
 template <int N, int E> __host__ __device__ constexpr int c2r_line_stride() {
   return line_slots<N, E>() > N + 2 ? line_slots<N, E>() : N + 2;
 }
+// Shared memory of a pass-3 block: B staged lines, the twiddles
+// e^{2 pi i m / P0} (m < P0 = 2N) and the x tables of the blend (s_x and the
+// flags, Nx <= 2N entries each).
+template <typename T, int N, int E, int B> __host__ __device__ constexpr size_t c2r_smem() {
+  return (size_t)B * c2r_line_stride<N, E>() * sizeof(cplx_t<T>) + (size_t)2 * N * sizeof(cplx_t<T>) +
+         (size_t)2 * N * sizeof(T) + (size_t)2 * N;
+}
 
 template <typename T, int N, int E, int B>
 __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
@@ -199,6 +206,9 @@ __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
   constexpr int LS = c2r_line_stride<N, E>();
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
+  C* tws = sm + B * LS;                                   // 2N twiddles
+  T* sxs = reinterpret_cast<T*>(tws + 2 * N);             // s_x, x < Nx
+  uint8_t* fxs = reinterpret_cast<uint8_t*>(sxs + 2 * N);  // flags, x < Nx
   const int Nx = a.Nout[0], Ny = a.Nout[1], Nz = a.Nout[2];
   const int64_t nlines = (int64_t)Ny * Nz;
   const C* work = static_cast<const C*>(a.work);
@@ -206,7 +216,18 @@ __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
   const int64_t l = (int64_t)bx * B + b;
   const bool valid = l < nlines;
   const int y = valid ? (int)(l % Ny) : 0, z = valid ? (int)(l / Ny) : 0;
-  {  // stage the raw half-spectrum line (N + 1 values, padded to 16 bytes)
+  const bool blend = a.epi.mode != 0;
+  {  // the block's tables, then the raw half-spectrum line (N + 1 values, padded to 16 bytes)
+    const C* twx = static_cast<const C*>(a.tw_x);
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tws[i] = __ldg(twx + i);
+    if (blend) {
+      const T* sx = sw_of<T>(a.epi.ax[0]);
+      const uint8_t* fx = a.epi.ax[0].flags;
+      for (int i = threadIdx.x; i < Nx; i += blockDim.x) {
+        sxs[i] = a.epi.apply_pou ? __ldg(sx + i) : T(1);
+        fxs[i] = __ldg(fx + i);
+      }
+    }
     constexpr int CH = (N + 2) * (int)sizeof(C) / 16;
     const C* src = work + ((size_t)z * a.P[1] + (size_t)y) * a.Hpad;
     if (valid)
@@ -215,17 +236,20 @@ __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
     cp_async_wait_all();
     __syncthreads();
   }
-  const C* twx = static_cast<const C*>(a.tw_x);
   const C* line = sm + b * LS;
   auto load = each_load<C, N, E>([&](int k) -> C {
     const C xk = line[k], xn = line[N - k];
     if (k == 0) return mk(xk.x + xn.x, xk.x - xn.x);
     const C xc = cconj(xn);
     const C e = cadd(xk, xc);
-    const C o = cmul(csub(xk, xc), __ldg(twx + k));
+    const C o = cmul(csub(xk, xc), tws[k]);
     return mk(e.x - o.y, e.y + o.x);
   });
-  const LineEpilogue<T> ep(a.epi, y, z, Nx, Ny);
+  LineEpilogue<T> ep(a.epi, y, z, Nx, Ny);
+  if (blend) {  // the x tables from shared memory
+    ep.fx = fxs;
+    ep.sx = sxs;
+  }
   constexpr int RL = last_radix<N, E>();
   auto store = [&](int j, const C* o) {
     if (!valid) return;
@@ -241,7 +265,7 @@ __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
     }
     ep.template put_group<2 * RL>(xs, v, Nx);
   };
-  line_ifft<C, N, E, SmemOrder::LineFast, B, LS>(sm, b, t, twx, 2, load, store);
+  line_ifft<C, N, E, SmemOrder::LineFast, B, LS>(sm, b, t, tws, 2, load, store);
 }
 
 // ---------------------------------------------------------------------------

@@ -59,8 +59,7 @@ template <typename T, int N, int Ee, int B, bool ROW>
 __host__ __device__ constexpr bool variant_ok() {
   if (!StagePlan<N, Ee>::valid()) return false;
   constexpr int threads = B * (N / Ee);
-  constexpr size_t slots = ROW ? (size_t)c2r_line_stride<N, Ee>() : (size_t)line_slots<N, Ee>();
-  constexpr size_t smem = (size_t)B * slots * sizeof(cplx_t<T>);
+  constexpr size_t smem = ROW ? c2r_smem<T, N, Ee, B>() : (size_t)B * line_slots<N, Ee>() * sizeof(cplx_t<T>);
   return threads >= 1 && threads <= 1024 && smem <= 220 * 1024 && (N % Ee) == 0;
 }
 
@@ -131,7 +130,7 @@ inline cudaError_t run_c2r_x_v(const GenArgs& a, const BatchMap* bm, int* blocks
       return cudaSuccess;
     }
     dim3 block(B * (N / E));
-    size_t smem = (size_t)B * c2r_line_stride<N, E>() * sizeof(cplx_t<T>);
+    size_t smem = c2r_smem<T, N, E, B>();
     if (bm) return launch_k(k_c2r_x_batch<T, N, E, B>, dim3(bm->total), block, smem, s, *bm);
     return launch_k(k_c2r_x<T, N, E, B>, grid, block, smem, s, a);
   }
