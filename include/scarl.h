@@ -296,7 +296,8 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
 int scarl_ensemble_draw(uint64_t seed, long long first, int n, const int* choices, int nchoices,
                         double lmin, double lmax, int* Np, double* corrL);
 
-/* n independent padded-method realisations of uneven grids, one tile each:
+/* n independent padded-method realisations of uneven grids, one tile each
+ * (dtype SCARL_F32, SCARL_F64 or SCARL_F32 | SCARL_SPLIT_BF16):
  * realisation i has Np[3i..3i+2] points of spacing xStep[3i..], correlation
  * lengths corrL[3i..], Philox key seeds[i] (NULL: i) and stream streams[i]
  * (NULL: 0).  Its field, column-major, starts at element
@@ -304,7 +305,9 @@ int scarl_ensemble_draw(uint64_t seed, long long first, int n, const int* choice
  * follow pad_policy (SCARL_PAD_FULL, _AUTO or _SMOOTH) / pad_tol per realisation; margiFirst 0 leaves the
  * standard field, 1 / 2 apply the Gaussian / lognormal marginal of avg,
  * std_dev.  Realisations are grouped by line length in each of the three
- * passes and every group runs as one batched launch; the first call for a
+ * passes and every group runs as one batched launch (with SCARL_SPLIT_BF16
+ * the pass-1 groups whose z length has a tensor-core kernel run it,
+ * persistent over the group's realisations); the first call for a
  * list of shapes builds the plan (FP64 spectral sums, tables, workspace) and
  * captures the launches in a CUDA graph that later calls replay. */
 int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* Np,

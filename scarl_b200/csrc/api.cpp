@@ -59,6 +59,7 @@ struct EnsGroup {
 struct EnsPlan {
   std::string key;
   int dt = 4, n = 0;
+  bool split = false;  // FP32 with the split-BF16 tensor-core pass 1 where its z length has one
   std::vector<GenArgs> args;  // host copies of the device argument blocks
   std::vector<size_t> off;    // first element of each field in the output
   size_t total = 0;           // elements of all fields
@@ -275,6 +276,15 @@ int finish_out(scarl_ctx* ctx, void* user, const void* dev, size_t bytes, bool h
     RC(check_status(ctx));
   }
   CK(cudaGetLastError());
+  return SCARL_OK;
+}
+
+// The context's device status word (allocated and cleared on first use).
+int ensure_status(scarl_ctx* ctx) {
+  if (!ctx->status.p) {
+    RC(ensure(ctx, ctx->status, 16));
+    CK(cudaMemset(ctx->status.p, 0, 16));
+  }
   return SCARL_OK;
 }
 
@@ -555,10 +565,7 @@ int gen_args(scarl_ctx* ctx, int dt, const int P[3], const int Np[3], GenArgs* a
   }
   a->Hx = P[0] / 2 + 1;
   a->Hpad = round_up(a->Hx, 16);
-  if (!ctx->status.p) {
-    RC(ensure(ctx, ctx->status, 16));
-    CK(cudaMemset(ctx->status.p, 0, 16));
-  }
+  RC(ensure_status(ctx));
   a->status = (int*)ctx->status.p;
   const size_t wbytes = (size_t)a->Hpad * P[1] * Np[2] * 2 * dt;
   RC(ensure(ctx, ctx->work, wbytes));
@@ -673,10 +680,22 @@ void ens_free(scarl_ctx* ctx) {
 }
 
 // Block offsets of a group for launch variant v (host).
+// Pass-1 groups of a split-precision plan whose z length has a tensor-core kernel.
+bool ens_tc(const EnsPlan* e, const EnsGroup& g) {
+  return e->split && e->dt == 4 && g.pass == 1 && gen_z_tc_supported(g.N);
+}
+
+cudaError_t ens_launch_group(const EnsPlan* e, const EnsGroup& g, int v, const BatchMap& m,
+                             cudaStream_t s) {
+  const GenArgs& rep = e->args[g.items[0]];
+  if (ens_tc(e, g)) return launch_gen_z_tc_batch(rep, m, s);
+  return launch_gen_pass_batch(e->dt, g.pass, v, rep, m, s);
+}
+
 int ens_starts(scarl_ctx* ctx, const EnsPlan* e, const EnsGroup& g, int v, std::vector<int>* st) {
   st->assign(1, 0);
   for (int i : g.items) {
-    const int nb = gen_pass_blocks(e->dt, g.pass, v, e->args[i]);
+    const int nb = ens_tc(e, g) ? gen_z_tc_items(e->args[i]) : gen_pass_blocks(e->dt, g.pass, v, e->args[i]);
     if (nb < 0) return SCARL_EUNSUPPORTED;
     if ((long long)st->back() + nb > 2147483647LL)
       return fail(ctx, SCARL_EINVAL, "ensemble too large for one launch");
@@ -712,13 +731,16 @@ int ens_maps(scarl_ctx* ctx, EnsPlan* e) {
   return SCARL_OK;
 }
 
-int ens_build(scarl_ctx* ctx, int dt, int n, const int* Np, const double* dx, const double* cl,
-              int corrMod, double nu, int policy, double tol, const std::string& key) {
+int ens_build(scarl_ctx* ctx, int dt, int split, int n, const int* Np, const double* dx,
+              const double* cl, int corrMod, double nu, int policy, double tol,
+              const std::string& key) {
   CK(cudaStreamSynchronize(ctx->stream));
   ens_free(ctx);
+  RC(ensure_status(ctx));
   EnsPlan* e = new EnsPlan();
   ctx->ens = e;
   e->dt = dt;
+  e->split = split != 0;
   e->n = n;
   e->args.resize(n);
   e->off.resize(n);
@@ -744,6 +766,8 @@ int ens_build(scarl_ctx* ctx, int dt, int n, const int* Np, const double* dx, co
     RC(twiddles(ctx, P[1], dt, &a.tw_y));
     RC(twiddles(ctx, P[0], dt, &a.tw_x));
     set_plan(&a, pl);
+    a.split = split;
+    a.status = (int*)ctx->status.p;
     a.epi.mode = 0;
     woff[i] = wtot;
     wtot += ((size_t)a.Hpad * P[1] * np[2] * 2 * dt + 255) / 256 * 256;
@@ -795,8 +819,8 @@ const char* kBatchName[3] = {"k_gen_z_batch", "k_mid_y_batch", "k_c2r_x_batch"};
 
 int ens_launch(scarl_ctx* ctx, EnsPlan* e) {
   for (EnsGroup& g : e->groups) {
-    Prof p(ctx, kBatchName[g.pass - 1]);
-    CK(launch_gen_pass_batch(e->dt, g.pass, g.var, e->args[g.items[0]], g.m, ctx->stream));
+    Prof p(ctx, ens_tc(e, g) ? "k_gen_z_tc_batch" : kBatchName[g.pass - 1]);
+    CK(ens_launch_group(e, g, g.var, g.m, ctx->stream));
   }
   return SCARL_OK;
 }
@@ -812,7 +836,7 @@ void ens_capture(scarl_ctx* ctx, EnsPlan* e) {
   }
   bool ok = true;
   for (EnsGroup& gr : e->groups)
-    if (launch_gen_pass_batch(e->dt, gr.pass, gr.var, e->args[gr.items[0]], gr.m, ctx->stream) !=
+    if (ens_launch_group(e, gr, gr.var, gr.m, ctx->stream) !=
         cudaSuccess)
       ok = false;
   if (cudaStreamEndCapture(ctx->stream, &g) != cudaSuccess) ok = false;
@@ -835,6 +859,7 @@ int ens_tune(scarl_ctx* ctx, EnsPlan* e) {
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   for (EnsGroup& g : e->groups) {
+    if (ens_tc(e, g)) continue;  // the tensor-core pass has one launch shape
     int best = g.var;
     float best_ms = 1e30f;
     for (int v = 0; v < gen_variant_count(e->dt, g.pass); ++v) {
@@ -846,15 +871,14 @@ int ens_tune(scarl_ctx* ctx, EnsPlan* e) {
       BatchMap m = g.m;
       m.start = static_cast<const int*>(e->tmp.p);
       m.total = st.back();
-      const GenArgs& rep = e->args[g.items[0]];
-      if (launch_gen_pass_batch(e->dt, g.pass, v, rep, m, ctx->stream) != cudaSuccess) {
+      if (ens_launch_group(e, g, v, m, ctx->stream) != cudaSuccess) {
         cudaGetLastError();
         continue;
       }
       float tmin = 1e30f;
       for (int rep_i = 0; rep_i < 3; ++rep_i) {
         CK(cudaEventRecord(e0, ctx->stream));
-        CK(launch_gen_pass_batch(e->dt, g.pass, v, rep, m, ctx->stream));
+        CK(ens_launch_group(e, g, v, m, ctx->stream));
         CK(cudaEventRecord(e1, ctx->stream));
         CK(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -2197,7 +2221,7 @@ int scarl_ensemble_draw(uint64_t seed, long long first, int n, const int* choice
   return ensemble_draw(seed, first, n, choices, nchoices, lmin, lmax, Np, corrL);
 }
 
-int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* Np,
+int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype_in, int n, const int* Np,
                        const double* xStep, const double* corrL, int corrMod, double nu,
                        int pad_policy, double pad_tol, const uint64_t* seeds,
                        const uint32_t* streams, int margiFirst, double avg, double std_dev,
@@ -2205,7 +2229,8 @@ int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* N
   RC(begin(ctx));
   if (!out || !Np || !xStep || !corrL) return fail(ctx, SCARL_EINVAL, "null argument");
   if (n < 1 || n > 65536) return fail(ctx, SCARL_EINVAL, "ensemble size must be in [1, 65536]");
-  if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
+  int dtype, split;
+  RC(parse_dtype(ctx, dtype_in, &dtype, &split));
   if (corrMod < 1 || corrMod > 3) return fail(ctx, SCARL_EINVAL, "ERROR: Correlation model not implemented");
   if (corrMod == SCARL_CM_VON_KARMAN && !(nu > 0.0)) return fail(ctx, SCARL_EINVAL, "nu must be > 0");
   if (pad_policy != SCARL_PAD_FULL && pad_policy != SCARL_PAD_AUTO && pad_policy != SCARL_PAD_SMOOTH)
@@ -2215,7 +2240,7 @@ int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* N
   std::string key;
   {
     char b[160];
-    std::snprintf(b, sizeof b, "%d|%d|%a|%d|%a|%d", dtype, corrMod, nu, pad_policy, tol, n);
+    std::snprintf(b, sizeof b, "%d|%d|%a|%d|%a|%d", dtype_in, corrMod, nu, pad_policy, tol, n);
     key = b;
     key.reserve(key.size() + (size_t)n * 96);
     for (int i = 0; i < n; ++i) {
@@ -2231,7 +2256,7 @@ int scarl_gen_ensemble(scarl_ctx* ctx, void* out, int dtype, int n, const int* N
     }
   }
   if (!ctx->ens || ctx->ens->key != key)
-    RC(ens_build(ctx, dtype, n, Np, xStep, corrL, corrMod, nu, pad_policy, tol, key));
+    RC(ens_build(ctx, dtype, split, n, Np, xStep, corrL, corrMod, nu, pad_policy, tol, key));
   EnsPlan* e = ctx->ens;
   void* dev;
   bool host;

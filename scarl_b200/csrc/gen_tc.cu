@@ -119,11 +119,19 @@ __device__ void fill_dft_b(unsigned char* hi, unsigned char* lo) {
   }
 }
 
-template <int N1, int N2, int LB, int NCH, int AMP>
-__global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
+// One CTA's walk over work items.  Single tile: items of a0's grid.  Batch
+// (several realisations sharing the z length): the flat item index is mapped
+// to (realisation, local item) through the group's offset table, and the
+// realisation's argument block and amplitude table are reloaded into shared
+// memory when it changes.
+template <int N1, int N2, int LB, int NCH, int AMP, bool BATCH>
+__device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* __restrict__ bargs,
+                                              const int* __restrict__ bitems,
+                                              const int* __restrict__ bstart, int bn, int btotal) {
   using Cfg = TcCfg<N1, N2, LB, NCH>;
   constexpr int N = Cfg::N;
   extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ GenArgs sa;  // batch: the current realisation's arguments
   unsigned char* AH = sm + Cfg::OFF_AH;
   unsigned char* AL = sm + Cfg::OFF_AL;
   const uint32_t sAH = tc::smem_u32(AH), sAL = tc::smem_u32(AL);
@@ -139,13 +147,14 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
   fill_dft_b<N1, Cfg::SBO2, false>(sm + Cfg::OFF_B2H, sm + Cfg::OFF_B2L);
   float* zt = reinterpret_cast<float*>(sm + Cfg::OFF_ZT);
   float2* tw2 = reinterpret_cast<float2*>(sm + Cfg::OFF_TW);
+  auto load_zt = [&](const GenArgs& g) {
+    const float* zsrc = static_cast<const float*>(AMP == AMP_SEPARABLE ? g.az : g.qz);
+    for (int i = tid; i < N; i += Cfg::THREADS) zt[i] = zsrc[i];
+  };
   {
-    const float* zsrc = static_cast<const float*>(AMP == AMP_SEPARABLE ? a.az : a.qz);
-    const float2* tw = static_cast<const float2*>(a.tw_z);  // e^{2 pi i m / N}
-    for (int i = tid; i < N; i += Cfg::THREADS) {
-      zt[i] = zsrc[i];
-      tw2[i] = tw[(i / N1) * (i % N1)];  // [n2][k1] = e^{2 pi i n2 k1 / N}
-    }
+    const float2* tw = static_cast<const float2*>(a0.tw_z);  // e^{2 pi i m / N}
+    for (int i = tid; i < N; i += Cfg::THREADS) tw2[i] = tw[(i / N1) * (i % N1)];  // [n2][k1]
+    if (!BATCH) load_zt(a0);
   }
   tc::fence_smem_to_async();
   tc::fence_before_sync();
@@ -153,15 +162,6 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
   tc::fence_after_sync();
   const uint32_t tmem = *tslot;
 
-  const int nlines = a.Hx * a.P[1];  // <= 1025 * 2048
-  const int nitems = (nlines + LB - 1) / LB;
-  const uint64_t mz = (uint64_t)a.Hx * (uint64_t)a.P[1];
-  const float* ax = static_cast<const float*>(a.ax);
-  const float* ay = static_cast<const float*>(a.ay);
-  const float* qx = static_cast<const float*>(a.qx);
-  const float* qy = static_cast<const float*>(a.qy);
-  float2* work = static_cast<float2*>(a.work);
-  const int Nz = a.Nout[2];
   constexpr uint32_t ID1 = tc::idesc_bf16(128, Cfg::K1, false);
   constexpr uint32_t ID2 = tc::idesc_bf16(128, Cfg::K2, true);  // A MN-major
 
@@ -170,8 +170,40 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
   const int s_line = (R1 >> 3) % LB, s_k1 = (R1 & 7) + 8 * (R1 / (8 * LB));
   uint32_t phase = 0;
   bool ok = true;
+  const int nitems0 = BATCH ? btotal : (a0.Hx * a0.P[1] + LB - 1) / LB;
+  int cur = -1;
 
-  for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+  for (int gitem = blockIdx.x; gitem < nitems0 && ok; gitem += gridDim.x) {
+    int item = gitem;
+    if constexpr (BATCH) {
+      int lo = 0, hi = bn;  // bstart[lo] <= gitem < bstart[hi]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(bstart + mid) <= gitem) lo = mid;
+        else hi = mid;
+      }
+      item = gitem - __ldg(bstart + lo);
+      const int r = __ldg(bitems + lo);
+      if (r != cur) {  // uniform over the CTA: every thread walks the same items
+        __syncthreads();
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(bargs + r);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+        for (int i = tid; i < (int)(sizeof(GenArgs) / 4); i += Cfg::THREADS) dst[i] = __ldg(src + i);
+        __syncthreads();
+        load_zt(sa);
+        __syncthreads();
+        cur = r;
+      }
+    }
+    const GenArgs& a = BATCH ? sa : a0;
+    const int nlines = a.Hx * a.P[1];  // <= 1025 * 2048
+    const uint64_t mz = (uint64_t)a.Hx * (uint64_t)a.P[1];
+    const float* ax = static_cast<const float*>(a.ax);
+    const float* ay = static_cast<const float*>(a.ay);
+    const float* qx = static_cast<const float*>(a.qx);
+    const float* qy = static_cast<const float*>(a.qy);
+    float2* work = static_cast<float2*>(a.work);
+    const int Nz = a.Nout[2];
     const int l0 = item * LB;
     // ---- synthesis of stage-1 row R1 ----
     {
@@ -357,7 +389,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
     // an MMA did not complete in time: report, then give it one more bounded
     // wait before the tensor memory it writes is released
     if (tid == 0) {
-      atomicOr(a.status, 1);
+      atomicOr(a0.status, 1);  // the context's status word, shared by every member of a batch
       tc::mbar_wait(bar, phase ^ 1, kWaitNs);
     }
     __syncthreads();
@@ -367,18 +399,25 @@ __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
 }
 
 template <int N1, int N2, int LB, int NCH, int AMP>
-cudaError_t launch_tc(const GenArgs& a, cudaStream_t s) {
-  using Cfg = TcCfg<N1, N2, LB, NCH>;
-  auto kern = k_gen_z_tc<N1, N2, LB, NCH, AMP>;
-  // per device: the shared-memory opt-in and the SM count
-  constexpr int kMaxDev = 64;
-  static int sms[kMaxDev] = {};
+__global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
+  gen_z_tc_body<N1, N2, LB, NCH, AMP, false>(a, nullptr, nullptr, nullptr, 0, 0);
+}
+template <int N1, int N2, int LB, int NCH, int AMP>
+__global__ void __launch_bounds__(256, 2) k_gen_z_tc_batch(const GenArgs rep, const BatchMap m) {
+  gen_z_tc_body<N1, N2, LB, NCH, AMP, true>(rep, m.args, m.items, m.start, m.n, m.total);
+}
+
+// One-time per device and kernel: the shared-memory opt-in; returns the SM
+// count.  sms is the caller's per-kernel cache (one per instantiation).
+constexpr int kMaxDev = 64;
+template <class K>
+cudaError_t tc_prepare(K kern, int smem, int (&sms)[kMaxDev], int* sms_out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
   if (!sms[dev]) {
-    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
       return e;
     if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
@@ -387,18 +426,49 @@ cudaError_t launch_tc(const GenArgs& a, cudaStream_t s) {
     if ((e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     sms[dev] = n;
   }
-  const int nitems = (a.Hx * a.P[1] + LB - 1) / LB;
+  *sms_out = sms[dev];
+  return cudaSuccess;
+}
+
+// bm == nullptr: one tile; else the batched kernel over bm->total items.
+template <int N1, int N2, int LB, int NCH, int AMP>
+cudaError_t launch_tc(const GenArgs& a, const BatchMap* bm, cudaStream_t s) {
+  using Cfg = TcCfg<N1, N2, LB, NCH>;
+  int sms = 0;
+  cudaError_t e;
   // two resident CTAs per SM (registers, shared and tensor memory are sized for it)
-  const int grid = std::min(nitems, sms[dev] * Cfg::CTAS_PER_SM);
-  kern<<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(a);
+  if (bm) {
+    static int cache[kMaxDev] = {};
+    auto kern = k_gen_z_tc_batch<N1, N2, LB, NCH, AMP>;
+    if ((e = tc_prepare(kern, Cfg::SMEM, cache, &sms)) != cudaSuccess) return e;
+    kern<<<std::min(bm->total, sms * Cfg::CTAS_PER_SM), Cfg::THREADS, Cfg::SMEM, s>>>(a, *bm);
+  } else {
+    static int cache[kMaxDev] = {};
+    auto kern = k_gen_z_tc<N1, N2, LB, NCH, AMP>;
+    if ((e = tc_prepare(kern, Cfg::SMEM, cache, &sms)) != cudaSuccess) return e;
+    const int nitems = (a.Hx * a.P[1] + LB - 1) / LB;
+    kern<<<std::min(nitems, sms * Cfg::CTAS_PER_SM), Cfg::THREADS, Cfg::SMEM, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
 template <int N1, int N2, int LB, int NCH>
-cudaError_t launch_amp(const GenArgs& a, cudaStream_t s) {
-  if (a.amp == AMP_SEPARABLE) return launch_tc<N1, N2, LB, NCH, AMP_SEPARABLE>(a, s);
-  if (a.amp == AMP_RECIP) return launch_tc<N1, N2, LB, NCH, AMP_RECIP>(a, s);
-  return launch_tc<N1, N2, LB, NCH, AMP_POW>(a, s);
+cudaError_t launch_amp(const GenArgs& a, const BatchMap* bm, cudaStream_t s) {
+  if (a.amp == AMP_SEPARABLE) return launch_tc<N1, N2, LB, NCH, AMP_SEPARABLE>(a, bm, s);
+  if (a.amp == AMP_RECIP) return launch_tc<N1, N2, LB, NCH, AMP_RECIP>(a, bm, s);
+  return launch_tc<N1, N2, LB, NCH, AMP_POW>(a, bm, s);
+}
+
+cudaError_t launch_any(const GenArgs& a, const BatchMap* bm, cudaStream_t s) {
+  if (!a.status || a.spec != SPEC_PHILOX) return cudaErrorInvalidValue;
+  switch (a.P[2]) {
+    case 256: return launch_amp<16, 16, 16, 1>(a, bm, s);
+    case 320: return launch_amp<8, 40, 32, 2>(a, bm, s);
+    case 384: return launch_amp<16, 24, 16, 1>(a, bm, s);
+    case 512: return launch_amp<16, 32, 16, 1>(a, bm, s);
+    case 1024: return launch_amp<32, 32, 8, 2>(a, bm, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace
@@ -408,16 +478,18 @@ cudaError_t launch_amp(const GenArgs& a, cudaStream_t s) {
 // not fit two CTAs per SM).
 bool gen_z_tc_supported(int N) { return N == 256 || N == 320 || N == 384 || N == 512 || N == 1024; }
 
-cudaError_t launch_gen_z_tc(const GenArgs& a, cudaStream_t s) {
-  if (!a.status || a.spec != SPEC_PHILOX) return cudaErrorInvalidValue;
-  switch (a.P[2]) {
-    case 256: return launch_amp<16, 16, 16, 1>(a, s);
-    case 320: return launch_amp<8, 40, 32, 2>(a, s);
-    case 384: return launch_amp<16, 24, 16, 1>(a, s);
-    case 512: return launch_amp<16, 32, 16, 1>(a, s);
-    case 1024: return launch_amp<32, 32, 8, 2>(a, s);
-    default: return cudaErrorInvalidValue;
-  }
+// Work items (256 / N1 lines each) of one realisation.
+int gen_z_tc_items(const GenArgs& a) {
+  if (!gen_z_tc_supported(a.P[2])) return -1;
+  const int lb = a.P[2] == 320 ? 32 : (a.P[2] == 1024 ? 8 : 16);
+  return (a.Hx * a.P[1] + lb - 1) / lb;
+}
+
+cudaError_t launch_gen_z_tc(const GenArgs& a, cudaStream_t s) { return launch_any(a, nullptr, s); }
+
+cudaError_t launch_gen_z_tc_batch(const GenArgs& rep, const BatchMap& m, cudaStream_t s) {
+  if (m.n < 1 || m.total < 1) return cudaErrorInvalidValue;
+  return launch_any(rep, &m, s);
 }
 
 }  // namespace scarl

@@ -103,6 +103,10 @@ cudaError_t launch_gen_pass_batch(int dt, int pass, int v, const GenArgs& rep, c
 // (gen_tc.cu): FP32, Philox spectrum, line lengths with gen_z_tc_supported.
 bool gen_z_tc_supported(int N);
 cudaError_t launch_gen_z_tc(const GenArgs& a, cudaStream_t s);
+// Batched form over realisations sharing the z length (m.start: offsets in
+// work items, gen_z_tc_items per realisation; rep: any member).
+int gen_z_tc_items(const GenArgs& a);
+cudaError_t launch_gen_z_tc_batch(const GenArgs& rep, const BatchMap& m, cudaStream_t s);
 // Blocks one realisation needs in a pass with launch variant v.
 int gen_pass_blocks(int dt, int pass, int v, const GenArgs& a);
 // Number of launch variants of a pass (valid ones depend on the line length).
