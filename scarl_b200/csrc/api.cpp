@@ -2622,10 +2622,16 @@ int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3],
   int Nc[3];
   for (int d = 0; d < 3; ++d) {
     if (L[d] < 1 || maxlag >= L[d]) return fail(ctx, SCARL_EINVAL, "maxlag must be below every extent");
-    int M = 8;
-    while (M < L[d] + maxlag) M <<= 1;
-    if (M > 4096) return fail(ctx, SCARL_EUNSUPPORTED, "L[d] + maxlag must be <= 4096");
-    Nc[d] = M / 2;
+    // smallest padded line M = 2 N >= L + maxlag with a covariance kernel for N
+    static const int kCovN[] = {4, 8, 16, 32, 64, 128, 256, 320, 384, 512, 640, 768, 1024, 1280,
+                                1536, 2048};
+    Nc[d] = 0;
+    for (int c : kCovN)
+      if (2 * c >= L[d] + maxlag) {
+        Nc[d] = c;
+        break;
+      }
+    if (!Nc[d]) return fail(ctx, SCARL_EUNSUPPORTED, "L[d] + maxlag must be <= 4096");
   }
   const size_t n = (size_t)L[0] * L[1] * L[2];
   const void* dev;

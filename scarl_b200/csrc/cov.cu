@@ -7,7 +7,8 @@
 // against.)
 //
 // Each line of L_d values, centred by the global mean, is zero-padded to
-// M = 2N >= L_d + H points and transformed as one complex DFT of length N
+// M = 2N >= L_d + H points (N a power of two or 320, 384, 640, 768, 1280,
+// 1536, whichever is smallest) and transformed as one complex DFT of length N
 // (even samples real, odd samples imaginary, then the even/odd split).  The
 // power |Y_k|^2, k = 0..N, is summed over all lines of the block in the
 // working precision and added to per-thread FP64 accumulators; one pass reads
@@ -24,9 +25,10 @@ namespace scarl {
 
 namespace {
 
-// values per thread: 16 complex in FP32, 8 in FP64
+// values per thread: 16 complex in FP32, 8 in FP64 (mixed lengths m 2^a:
+// m times a power of two, eff_E)
 template <typename T, int N> __host__ __device__ constexpr int cov_E() {
-  return N < (sizeof(T) == 4 ? 16 : 8) ? N : (sizeof(T) == 4 ? 16 : 8);
+  return eff_E<N, (sizeof(T) == 4 ? 16 : 8)>();
 }
 // lines per block, for 512-thread blocks at most: ROW (x lines, lanes along
 // a line) up to 32 lines, column layouts (lanes across lines) up to 16
@@ -38,11 +40,13 @@ template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_B()
 template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_threads() {
   return cov_B<T, N, ROW>() * (N / cov_E<T, N>());
 }
-// resident blocks asked of the compiler: 1024 threads per SM, at most 32 blocks
+// resident blocks asked of the compiler: 1024 threads per SM (512 for FP64 and
+// for mixed lengths, whose E holds an odd factor), at most 32 blocks
 template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_minb() {
-  return (1024 / cov_threads<T, N, ROW>()) > 32 ? 32 : 1024 / cov_threads<T, N, ROW>();
+  constexpr int per_sm = (sizeof(T) == 8 || odd_part(N) > 1) ? 512 : 1024;
+  return (per_sm / cov_threads<T, N, ROW>()) > 32 ? 32
+         : (per_sm / cov_threads<T, N, ROW>()) < 1 ? 1 : per_sm / cov_threads<T, N, ROW>();
 }
-
 struct CovGeom {
   const void* f;
   int n;          // points per line (L_d)
@@ -168,6 +172,12 @@ cudaError_t run_power_n(int N, CovGeom g, int want_blocks, int* blocks, cudaStre
     case 512: return run_power<T, 512, ROW>(g, want_blocks, blocks, s);
     case 1024: return run_power<T, 1024, ROW>(g, want_blocks, blocks, s);
     case 2048: return run_power<T, 2048, ROW>(g, want_blocks, blocks, s);
+    case 320: return run_power<T, 320, ROW>(g, want_blocks, blocks, s);
+    case 384: return run_power<T, 384, ROW>(g, want_blocks, blocks, s);
+    case 640: return run_power<T, 640, ROW>(g, want_blocks, blocks, s);
+    case 768: return run_power<T, 768, ROW>(g, want_blocks, blocks, s);
+    case 1280: return run_power<T, 1280, ROW>(g, want_blocks, blocks, s);
+    case 1536: return run_power<T, 1536, ROW>(g, want_blocks, blocks, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -150,6 +150,27 @@ template <int N, int E> struct StagePlan {
   static constexpr int S = count();
 };
 
+// Power-of-two stages of a 2^a length with radices of at most e2.
+__host__ __device__ constexpr int p2_stages(int p2, int e2) {
+  return p2 > 1 ? 1 + p2_stages(p2 / (p2 > e2 ? e2 : p2), e2) : 0;
+}
+__host__ __device__ constexpr int grow_e2(int p2, int e2) {
+  return (e2 < p2 && p2_stages(p2, e2) + 1 > 5) ? grow_e2(p2, 2 * e2) : e2;
+}
+// Values per thread of a launch variant: E itself for power-of-two lengths;
+// for N = m 2^a (m odd) m e2 with e2 >= E / 4 the smallest power of two whose
+// plan (power-of-two stages, then the radix-m stage) has at most 5 stages.
+template <int N, int E> __host__ __device__ constexpr int eff_E() {
+  constexpr int m = odd_part(N);
+  if constexpr (m == 1) {
+    return E < N ? E : N;
+  } else {
+    constexpr int p2 = N / m;
+    constexpr int e0 = (E / 4 < 2 ? 2 : E / 4) > p2 ? p2 : (E / 4 < 2 ? 2 : E / 4);
+    return m * grow_e2(p2, e0);
+  }
+}
+
 // Shared-memory addressing of line element n of line b, skewed by one slot
 // per SK elements (SK = first radix) so the first stage's stride-SK writes
 // fall in distinct banks:
