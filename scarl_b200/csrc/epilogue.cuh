@@ -71,9 +71,7 @@ struct LineEpilogue {
     return v;
   }
   // K outputs at once: every read of an earlier tile's partial sum is issued
-  // before any write.  Blend mode is written without data-dependent branches
-  // (predicated loads, selects and stores), so lanes whose points fall in
-  // different regions of the tile do not diverge.
+  // before any write.
   template <int K>
   __device__ __forceinline__ void put_group(const int* xs, const T* v, int Nx) const {
     if (mode == 0) {
@@ -82,28 +80,20 @@ struct LineEpilogue {
         if (xs[i] < Nx) out[base + xs[i]] = marg(v[i]);
       return;
     }
-    uint32_t f[K];
-    T old[K], s[K];
+    uint8_t f[K];
+    T old[K];
 #pragma unroll
     for (int i = 0; i < K; ++i) {
-      const bool in = xs[i] < Nx;
-      const int xi = in ? xs[i] : 0;
-      f[i] = in ? (uint32_t)(fyz & fx[xi]) : 0u;
-      s[i] = pou ? syz * sx[xi] : T(1);
-      old[i] = T(0);
-      if ((f[i] & 3u) == 1u) old[i] = out[base + xi];  // contributes, not the first tile
+      f[i] = xs[i] < Nx ? (uint8_t)(fyz & fx[xs[i]]) : (uint8_t)0;
+      old[i] = ((f[i] & 3) == 1) ? out[base + xs[i]] : T(0);
     }
 #pragma unroll
     for (int i = 0; i < K; ++i) {
-      const T w = old[i] + v[i] * s[i];
-      T o = w;  // the last contributor applies the marginal (FP32: computed, then selected)
-      if constexpr (sizeof(T) == 4) {
-        const T m = marg(w);
-        o = (f[i] & 4u) ? m : w;
-      } else {
-        if (f[i] & 4u) o = marg(w);
-      }
-      if (f[i] & 1u) out[base + xs[i]] = o;
+      if (!(f[i] & 1)) continue;
+      T w = pou ? v[i] * (syz * sx[xs[i]]) : v[i];
+      if (!(f[i] & 2)) w = old[i] + w;
+      if (f[i] & 4) w = marg(w);
+      out[base + xs[i]] = w;
     }
   }
   __device__ __forceinline__ void put(int x, T v) const {
