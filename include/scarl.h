@@ -150,6 +150,13 @@ int scarl_autotune(scarl_ctx* ctx, int dtype, int corrMod, double nu, const int 
                    const char* cache_path);
 int scarl_tune_get(scarl_ctx* ctx, int dtype, int pass, int N, int* variant);
 int scarl_tune_set(scarl_ctx* ctx, int dtype, int pass, int N, int variant);
+/* Test hook of the tensor-core pass's bounded waits (no counterpart in the
+ * reference): while enabled, SCARL_SPLIT_BF16 tiles issue no matrix product,
+ * so every CTA's wait on the tensor core runs out after 20 ms; the kernel
+ * raises the context's status word, frees its tensor memory and returns, and
+ * the call (or the next scarl_sync) returns SCARL_ETIMEOUT.  The context stays
+ * usable. */
+int scarl_tc_wait_test(scarl_ctx* ctx, int enable);
 /* Kernels launched and bytes copied host->device / device->host by this
  * context since its creation. */
 int scarl_counters(scarl_ctx* ctx, long long* launches, unsigned long long* h2d_bytes,

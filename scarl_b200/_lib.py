@@ -64,6 +64,7 @@ SIGNATURES = {
     "scarl_last_error": (C.c_char_p, [_vp]),
     "scarl_ctx_set_stream": (C.c_int, [_vp, _vp]),
     "scarl_sync": (C.c_int, [_vp]),
+    "scarl_tc_wait_test": (C.c_int, [_vp, C.c_int]),
     "scarl_counters": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong),
                                  C.POINTER(C.c_ulonglong)]),
     "scarl_autotune": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, _ip, _ip, _dp, _dp,

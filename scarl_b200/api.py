@@ -73,6 +73,10 @@ class Context:
     def sync(self):
         _check(lib().scarl_sync(self.handle), self)
 
+    def tc_wait_test(self, enable=True):
+        """Test hook: the tensor-core pass's waits run out (SCARL_ETIMEOUT)."""
+        _check(lib().scarl_tc_wait_test(self.handle, int(bool(enable))), self)
+
     def profile(self, enable=True):
         _check(lib().scarl_profile(self.handle, int(enable)), self)
 

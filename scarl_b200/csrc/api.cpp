@@ -79,6 +79,7 @@ struct scarl_ctx {
   std::string err;
   Buf work, tile, stage_out, stage_in, stage_in2, tabs, dtabs, part, t1, t2, sk, pmpw;
   Buf status;  // device word raised by kernels whose bounded waits expired
+  int wait_test = 0;  // test hook of the bounded tensor-core waits
   void* pin = nullptr;
   size_t pin_n = 0;
   cudaEvent_t pin_ev = nullptr;
@@ -567,6 +568,7 @@ int gen_args(scarl_ctx* ctx, int dt, const int P[3], const int Np[3], GenArgs* a
   a->Hpad = round_up(a->Hx, 16);
   RC(ensure_status(ctx));
   a->status = (int*)ctx->status.p;
+  a->wait_test = ctx->wait_test;
   const size_t wbytes = (size_t)a->Hpad * P[1] * Np[2] * 2 * dt;
   RC(ensure(ctx, ctx->work, wbytes));
   a->work = ctx->work.p;
@@ -1362,6 +1364,12 @@ int scarl_sync(scarl_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
   RC(check_status(ctx));
+  return SCARL_OK;
+}
+
+int scarl_tc_wait_test(scarl_ctx* ctx, int enable) {
+  if (!ctx) return SCARL_EINVAL;
+  ctx->wait_test = enable ? 1 : 0;
   return SCARL_OK;
 }
 

@@ -170,6 +170,10 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
   const int s_line = (R1 >> 3) % LB, s_k1 = (R1 & 7) + 8 * (R1 / (8 * LB));
   uint32_t phase = 0;
   bool ok = true;
+  // test hook: no stage-1 MMA is issued, so the first wait runs out (after
+  // 20 ms) and the bounded-wait path below reports it
+  const bool wait_test = a0.wait_test != 0;
+  const uint64_t wait_ns = wait_test ? 20000000ull : kWaitNs;
   const int nitems0 = BATCH ? btotal : (a0.Hx * a0.P[1] + LB - 1) / LB;
   int cur = -1;
 
@@ -261,7 +265,7 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
     tc::fence_smem_to_async();
     __syncthreads();
     // ---- stage 1 on the tensor cores ----
-    if (tid == 0) {
+    if (tid == 0 && !wait_test) {
       tc::fence_after_sync();
 #pragma unroll 1
       for (int t = 0; t < Cfg::T1; ++t) {
@@ -280,7 +284,7 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
       }
       tc::commit(bar);
     }
-    ok = warp == 0 ? tc::mbar_wait(bar, phase, kWaitNs) : true;  // one warp sleeps in the barrier
+    ok = warp == 0 ? tc::mbar_wait(bar, phase, wait_ns) : true;  // one warp sleeps in the barrier
     phase ^= 1;
     if (!__syncthreads_and(ok)) { ok = false; break; }
     tc::fence_after_sync();
@@ -342,7 +346,7 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
       }
       tc::commit(bar);
     }
-    ok = warp == 0 ? tc::mbar_wait(bar, phase, kWaitNs) : true;  // one warp sleeps in the barrier
+    ok = warp == 0 ? tc::mbar_wait(bar, phase, wait_ns) : true;  // one warp sleeps in the barrier
     phase ^= 1;
     if (!__syncthreads_and(ok)) { ok = false; break; }
     tc::fence_after_sync();
@@ -390,7 +394,7 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
     // wait before the tensor memory it writes is released
     if (tid == 0) {
       atomicOr(a0.status, 1);  // the context's status word, shared by every member of a batch
-      tc::mbar_wait(bar, phase ^ 1, kWaitNs);
+      tc::mbar_wait(bar, phase ^ 1, wait_ns);
     }
     __syncthreads();
   }

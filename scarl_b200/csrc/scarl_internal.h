@@ -75,6 +75,7 @@ struct GenArgs {
   int var[3];            // launch variant of each pass (autotuned, 0 = default)
   int split;             // FP32: pass 1's z DFT on the tensor cores in split BF16
   int* status;           // device word, bit 0 set when a bounded tensor-core wait expired
+  int wait_test;         // test hook: the tensor-core pass issues no MMA and waits 20 ms
 };
 
 // One batched launch of a pass over several realisations that share the

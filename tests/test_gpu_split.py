@@ -98,3 +98,22 @@ def test_split_blended_sample_vs_fp64(ctx):
         err = rel(f32s, f64)
         print(f"513^3 split rel-L2 {err:.2e} (policy {policy})")
         assert err < TOL
+
+
+def test_split_bounded_wait_reports_timeout(ctx, oracle):
+    """With the test hook no matrix product is issued: every CTA's bounded wait
+    on the tensor core runs out, the call returns SCARL_ETIMEOUT, and the
+    context generates correctly afterwards."""
+    from scarl_b200 import _lib
+    Np, P, cl = (12, 10, 300), (16, 16, 512), (3, 3, 40)
+    ctx.tc_wait_test(True)
+    try:
+        with pytest.raises(S.ScarlError) as e:
+            S.gen_padded(ctx, Np, (1, 1, 1), cl, 3, pad=P, seed=77, stream=3, dtype=SPLIT)
+        assert e.value.code == _lib.ETIMEOUT
+    finally:
+        ctx.tc_wait_test(False)
+    ref = oracle.gen_padded(Np, P, (1, 1, 1), cl, 3, 0.5, 1, seed=77, stream=3)
+    out = S.gen_padded(ctx, Np, (1, 1, 1), cl, 3, pad=P, seed=77, stream=3, dtype=SPLIT)
+    assert rel(out, ref) < TOL
+    ctx.sync()
