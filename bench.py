@@ -373,6 +373,28 @@ def config_of(lay, P):
             "l2": "working set larger than L2 (field 0.54 GB, intermediate >= 0.15 GB per tile)"}
 
 
+def bench_learned(S, ctx):
+    """The learned padding predictor: trained on the GPU (4096 generated
+    configurations, 3000 Adam steps), then judged on 512 held-out
+    configurations against full padding: FFT volume cut and the covariance
+    error at the predicted padding (target: cut >= 30 % at <= 1 % error)."""
+    import scarl_b200.learned as LRN
+    t0 = time.perf_counter()
+    fit = LRN.fit(ctx, n_train=4096, seed=1, steps=3000, lr=3e-3)
+    t1 = time.perf_counter()
+    ev = LRN.evaluate(ctx, n_test=512, seed=2)
+    t2 = time.perf_counter()
+    return {"train_configs": 4096, "train_axes": fit["axes"], "steps": 3000,
+            "loss_first": round(float(fit["loss"][0]), 5), "loss_last": round(float(fit["loss"][-1]), 5),
+            "s_train_incl_labels": round(t1 - t0, 2), "s_evaluate": round(t2 - t1, 2),
+            "held_out_configs": ev["configs"],
+            "fft_volume_cut_vs_full": round(ev["volume_reduction"], 4),
+            "frac_axes_within_1pct": round(ev["frac_axes_within_1pct"], 4),
+            "max_cov_error_learned": round(ev["max_cov_error_learned"], 5),
+            "max_cov_error_full": round(ev["max_cov_error_full"], 5),
+            "fallbacks": ev["fallbacks"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -382,6 +404,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-large-field", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--profile-stats", action="store_true",
                     help="one 1024x1024x512 FP32 field (2 GB) and one pass of the streamed "
                          "statistics (mean, variance, axis covariance to lag 256), no timing")
@@ -602,6 +625,10 @@ def main():
     if not args.no_large_field:
         large = bench_large_field(S, ctx, stream, 3, rank, dist)
 
+    learned = None
+    if rank == 0 and not args.no_learned:
+        learned = bench_learned(S, ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = cpu_sample(lay, P_pow2, 1, 0)
@@ -619,7 +646,7 @@ def main():
                 "fp32_path": fp32, "pow2_grid_path": pow2,
                 "speedup_vs_plain_path": round(ms_full / ms, 3),
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-                "ensemble": ens, "large_field": large}
+                "ensemble": ens, "large_field": large, "learned_padding": learned}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

@@ -40,10 +40,10 @@ template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_B()
 template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_threads() {
   return cov_B<T, N, ROW>() * (N / cov_E<T, N>());
 }
-// resident blocks asked of the compiler: 1024 threads per SM (512 for FP64 and
-// for mixed lengths, whose E holds an odd factor), at most 32 blocks
+// resident blocks asked of the compiler: 512 threads per SM (128 registers a
+// thread: room for the FP32 prefetch of the next lines), at most 32 blocks
 template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_minb() {
-  constexpr int per_sm = (sizeof(T) == 8 || odd_part(N) > 1) ? 512 : 1024;
+  constexpr int per_sm = 512;
   return (per_sm / cov_threads<T, N, ROW>()) > 32 ? 32
          : (per_sm / cov_threads<T, N, ROW>()) < 1 ? 1 : per_sm / cov_threads<T, N, ROW>();
 }
@@ -81,7 +81,15 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
   for (int q = 0; q < QB; ++q) acc[q] = 0.0;
   const int64_t ngroups = (g.nlines + B - 1) / B;
   const T mu = (T)g.mu;
-  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+  // First-stage inputs of this thread for the lines of group grp, centred and
+  // zero-padded: dst[q R1 + r] = (x[2k], x[2k + 1]), k = t + TPL q + r N / R1.
+  // In FP32 the next group's inputs are fetched into registers before the
+  // current group's transform, so their global-memory latency overlaps it
+  // (FP64, and lines of more than 20 values a thread or one thread a line,
+  // have no registers to spare for it).
+  constexpr bool PF = sizeof(T) == 4 && E <= 20 && TPL > 1;
+  constexpr int R1 = StagePlan<N, E>::radix(0);
+  auto fetch = [&](int64_t grp, C* dst) {
     const int64_t l = grp * B + b;
     const bool valid = l < g.nlines;
     const int64_t base = valid ? (l % g.na) * g.sa + (l / g.na) * g.sb : 0;
@@ -89,13 +97,38 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
       if (!valid || i >= g.n) return T(0);
       return __ldg(f + base + (int64_t)i * g.st) - mu;
     };
-    auto load = each_load<C, N, E>([&](int k) -> C { return mk(val(2 * k), val(2 * k + 1)); });
+#pragma unroll
+    for (int q = 0; q < E / R1; ++q)
+#pragma unroll
+      for (int r = 0; r < R1; ++r) {
+        const int k = t + TPL * q + r * (N / R1);
+        dst[q * R1 + r] = mk(val(2 * k), val(2 * k + 1));
+      }
+  };
+  C nxt[PF ? E : 1];
+  if constexpr (PF) fetch(blockIdx.x, nxt);
+  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    C cur[E];
+    if constexpr (PF) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) cur[i] = nxt[i];
+      if (grp + gridDim.x < ngroups) fetch(grp + gridDim.x, nxt);
+    } else {
+      fetch(grp, cur);
+    }
+    auto load = [&](int j, C* v) {
+      const int q = (j - t) / TPL;
+#pragma unroll
+      for (int r = 0; r < R1; ++r) v[r] = cur[q * R1 + r];
+    };
     constexpr int RL = last_radix<N, E>();
-    // outputs go straight to shared memory (line b at b * N), after every
-    // thread has left the transform's shared-memory reads
+    // outputs go straight to shared memory (line b at b (N + 1): the odd
+    // stride spreads the lines of a column layout, whose lanes store the same
+    // j of different lines, over the banks), after every thread has left the
+    // transform's shared-memory reads
     auto store = [&](int j, const C* o) {
 #pragma unroll
-      for (int r = 0; r < RL; ++r) sm[b * N + j + r * (N / RL)] = o[r];
+      for (int r = 0; r < RL; ++r) sm[b * (N + 1) + j + r * (N / RL)] = o[r];
     };
     line_ifft<C, N, E, O, B, LS, true>(sm, b, t, tw, 2, load, store);
     __syncthreads();
@@ -106,8 +139,8 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
       const C w = __ldg(tw + k);
       T s = T(0);
       for (int bb = 0; bb < B; ++bb) {
-        const C zk = sm[bb * N + (k == N ? 0 : k)];
-        const C zc = cconj(sm[bb * N + (k == 0 || k == N ? 0 : N - k)]);
+        const C zk = sm[bb * (N + 1) + (k == N ? 0 : k)];
+        const C zc = cconj(sm[bb * (N + 1) + (k == 0 || k == N ? 0 : N - k)]);
         const C e = mk((zk.x + zc.x) * T(0.5), (zk.y + zc.y) * T(0.5));
         // (zk - zc) / (2i)
         const C od = mk((zk.y - zc.y) * T(0.5), -(zk.x - zc.x) * T(0.5));
@@ -129,7 +162,7 @@ template <typename T, int N, bool ROW> size_t cov_smem() {
   constexpr int E = cov_E<T, N>();
   constexpr int B = cov_B<T, N, ROW>();
   const size_t fft = (size_t)B * line_slots<N, E>() * sizeof(cplx_t<T>);
-  const size_t pw = (size_t)B * N * sizeof(cplx_t<T>);
+  const size_t pw = (size_t)B * (N + 1) * sizeof(cplx_t<T>);
   return fft > pw ? fft : pw;
 }
 

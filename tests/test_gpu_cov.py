@@ -27,8 +27,8 @@ def _field(shape, seed, shift=0.0):
     ((9, 200, 12), 8, 0.0),
     ((16, 16, 300), 15, 1.0),
     ((257, 31, 17), 16, 0.0),
-    ((600, 7, 9), 30, 0.5),     # x line padded to M = 640 (N = 320 = 5 x 64)
-    ((9, 700, 8), 60, 0.0),     # y line padded to M = 768 (N = 384 = 3 x 128)
+    ((600, 40, 35), 30, 0.5),   # x line padded to M = 640 (N = 320 = 5 x 64)
+    ((64, 700, 62), 60, 0.0),   # y line padded to M = 768 (N = 384 = 3 x 128)
 ])
 def test_axis_cov_vs_oracle(ctx, oracle, shape, maxlag, shift):
     f = _field(shape, sum(shape), shift)
