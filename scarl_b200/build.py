@@ -58,6 +58,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 return LIB
     os.makedirs(OBJ, exist_ok=True)
     nvcc = _nvcc()
+    hdr = hashlib.sha256()
+    for d in (CSRC, INCLUDE):
+        for f in sorted(os.listdir(d)):
+            if f.endswith((".h", ".cuh", ".hpp")):
+                with open(os.path.join(d, f), "rb") as fh:
+                    hdr.update(f.encode() + fh.read())
+
+    def job_digest(cmd, src):
+        # an object is rebuilt when its command, its source or any header changes
+        h = hashlib.sha256(hdr.digest())
+        h.update(" ".join(cmd).encode())
+        with open(src, "rb") as fh:
+            h.update(fh.read())
+        return h.hexdigest()
+
     jobs = []  # (label, command, object)
     for dt, n in INSTANCES:
         obj = os.path.join(OBJ, f"gen_inst_{dt}_{n}.o")
@@ -72,19 +87,33 @@ def build(force: bool = False, verbose: bool = False) -> str:
         else:
             cmd[1:1] = ["-x", "cu"] + ARCH
         jobs.append((src, cmd, obj))
-    # longest jobs first, at most one per core
-    pending = list(jobs)
+    # longest jobs first, at most one per core; up-to-date objects are kept
+    pending = []
+    for label, cmd, obj in jobs:
+        src = cmd[cmd.index("-c") + 1]
+        dg = job_digest(cmd, src)
+        st = obj + ".stamp"
+        if not force and os.path.exists(obj) and os.path.exists(st):
+            with open(st) as fh:
+                if fh.read().strip() == dg:
+                    continue
+        if os.path.exists(st):
+            os.remove(st)
+        pending.append((label, cmd, obj, st, dg))
     running, failed = [], []
     width = max(1, os.cpu_count() or 1)
     while pending or running:
         while pending and len(running) < width:
-            label, cmd, _ = pending.pop(0)
+            label, cmd, _, st, dg = pending.pop(0)
             if verbose:
                 print(" ".join(cmd))
-            running.append((label, subprocess.Popen(cmd)))
-        label, p = running.pop(0)
+            running.append((label, subprocess.Popen(cmd), st, dg))
+        label, p, st, dg = running.pop(0)
         if p.wait() != 0:
             failed.append(label)
+        else:
+            with open(st, "w") as fh:
+                fh.write(dg)
     if failed:
         raise RuntimeError("nvcc failed for " + ", ".join(failed))
     objs = [j[2] for j in jobs]

@@ -83,6 +83,10 @@ struct scarl_ctx {
   void* pin = nullptr;
   size_t pin_n = 0;
   cudaEvent_t pin_ev = nullptr;
+  // device -> pinned host copies of finished z slabs, overlapped with the
+  // generation of the remaining tiles
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> slab_ev;
   std::map<std::string, PaddedPlan> plans;
   std::map<long long, Buf> twiddles;
   std::map<int, Buf> dct_tabs;
@@ -163,6 +167,16 @@ bool is_device_ptr(const void* p) {
     return false;
   }
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+bool is_pinned_host(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
 }
 
 // Pinned host staging for small tables; waits for the previous upload.
@@ -277,6 +291,65 @@ int finish_out(scarl_ctx* ctx, void* user, const void* dev, size_t bytes, bool h
     RC(check_status(ctx));
   }
   CK(cudaGetLastError());
+  return SCARL_OK;
+}
+
+// Output copied back in boxes while later tiles are generated.  Tiles run
+// x fastest, then y, then z; with ystart(ty) = (Np_y - Np_ovlp_y) ty
+// (ystart(0) = 0, ystart(Ty) = L_y) and zstart likewise, the box
+// [ystart(ty), ystart(ty + 1)) x [zstart(tz), zstart(tz + 1)) (all x) is only
+// covered by tile rows (ty, tz), (ty - 1, tz), (ty, tz - 1) and
+// (ty - 1, tz - 1), so it is final once row (ty, tz) is blended.  Its
+// device -> host copy (one strided 2D copy: a run of whole y rows per z
+// plane) runs on a second stream that waits for the row.
+struct SlabCopier {
+  scarl_ctx* ctx = nullptr;
+  char* user = nullptr;
+  const char* dev = nullptr;
+  size_t row = 0;    // bytes of one x row
+  size_t plane = 0;  // bytes of one z plane
+  int nev = 0;
+  bool on = false;
+};
+
+int slab_begin(scarl_ctx* ctx, SlabCopier& c, void* user, const void* dev, size_t row, int Ly) {
+  c.ctx = ctx;
+  c.user = static_cast<char*>(user);
+  c.dev = static_cast<const char*>(dev);
+  c.row = row;
+  c.plane = row * (size_t)Ly;
+  c.on = true;
+  if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  return SCARL_OK;
+}
+
+// Rows [y0, y1) of planes [z0, z1) are final once the work queued so far on
+// the context's stream completes.
+int slab_copy(SlabCopier& c, int y0, int y1, int z0, int z1) {
+  scarl_ctx* ctx = c.ctx;
+  if (!c.on || y1 <= y0 || z1 <= z0) return SCARL_OK;
+  if ((int)ctx->slab_ev.size() <= c.nev) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->slab_ev.push_back(e);
+  }
+  cudaEvent_t e = ctx->slab_ev[c.nev++];
+  CK(cudaEventRecord(e, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->copy_stream, e, 0));
+  const size_t o = (size_t)z0 * c.plane + (size_t)y0 * c.row, w = (size_t)(y1 - y0) * c.row;
+  CK(cudaMemcpy2DAsync(c.user + o, c.plane, c.dev + o, c.plane, w, (size_t)(z1 - z0),
+                       cudaMemcpyDeviceToHost, ctx->copy_stream));
+  ctx->d2h += w * (size_t)(z1 - z0);
+  return SCARL_OK;
+}
+
+// Waits for every queued copy (also on error paths: the copies write the
+// caller's memory).
+int slab_end(SlabCopier& c) {
+  scarl_ctx* ctx = c.ctx;
+  if (!c.on) return SCARL_OK;
+  c.on = false;
+  CK(cudaStreamSynchronize(ctx->copy_stream));
   return SCARL_OK;
 }
 
@@ -1338,6 +1411,11 @@ int scarl_ctx_destroy(scarl_ctx* ctx) {
   for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
   if (ctx->pin_ev) cudaEventDestroy(ctx->pin_ev);
   if (ctx->pin) cudaFreeHost(ctx->pin);
+  for (cudaEvent_t e : ctx->slab_ev) cudaEventDestroy(e);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return SCARL_OK;
@@ -2414,37 +2492,62 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   const void* phi_all = nullptr;
   if (gen == SCARL_GEN_DCT && o.phiK)
     RC(in_dev(ctx, ctx->stage_in, o.phiK, nk * lay.nb_tiles * 8, &phi_all));
-  for (int r = 0; r < lay.nb_tiles; ++r) {
-    scarl_tile t;
-    tile_geometry(&lay, s->xMinGlob, r, &t);
-    const int32_t seedStart = (int32_t)((uint32_t)s->seedBase + 1u + (uint32_t)r);
-    Epilogue e = epi;
-    for (int d = 0; d < 3; ++d) {
-      e.off[d] = t.pos_0[d] - 1;
-      e.ax[d] = axes[(size_t)r * 3 + d];
+  // pinned host output over several rows of tiles: finished boxes stream
+  // back while the later rows are generated
+  SlabCopier slabs;
+  const bool stream_out = host && !o.normalize_field && lay.topo_shape[1] * lay.topo_shape[2] > 1 &&
+                          is_pinned_host(global);
+  if (stream_out) RC(slab_begin(ctx, slabs, global, dev, (size_t)lay.L[0] * dt, lay.L[1]));
+  auto row_start = [&](int d, int tp) {  // first plane (d = 1: y, 2: z) of the box of tile row tp
+    return tp >= lay.topo_shape[d] ? lay.L[d] : std::min(lay.L[d], (lay.Np[d] - lay.Np_ovlp[d]) * tp);
+  };
+  const int rc_tiles = [&]() -> int {
+    for (int r = 0; r < lay.nb_tiles; ++r) {
+      scarl_tile t;
+      tile_geometry(&lay, s->xMinGlob, r, &t);
+      const int32_t seedStart = (int32_t)((uint32_t)s->seedBase + 1u + (uint32_t)r);
+      Epilogue e = epi;
+      for (int d = 0; d < 3; ++d) {
+        e.off[d] = t.pos_0[d] - 1;
+        e.ax[d] = axes[(size_t)r * 3 + d];
+      }
+      if (gen == SCARL_GEN_PADDED) {
+        GenArgs a;
+        RC(gen_args(ctx, dt, P, lay.Np, &a));
+        set_plan(&a, pl);
+        a.split = split;
+        a.k0 = (uint32_t)seedStart;
+        a.k1 = 0;
+        a.stream = o.stream;
+        a.epi = e;
+        RC(run_passes(ctx, dt, a));
+      } else if (gen == SCARL_GEN_SHINO) {
+        GenArgs a;
+        RC(shino_args(ctx, lay.Np, t.xRange, s->corrL, seedStart, &a));
+        a.epi = e;
+        RC(run_passes(ctx, 8, a));
+      } else {
+        const double* phi = phi_all ? (const double*)phi_all + nk * r : nullptr;
+        RC(dct_tile(ctx, (double*)ctx->tile.p, lay.Np, t.xRange, s->corrL, phi, nullptr, (uint32_t)seedStart,
+                    gm == SCARL_FFT_MPI));
+        Prof p(ctx, "k_blend_tile");
+        CK(launch_blend_tile(8, ctx->tile.p, lay.Np, e, ctx->stream));
+      }
+      if (stream_out && t.topo_pos[0] == lay.topo_shape[0] - 1) {
+        const int ty = t.topo_pos[1], tz = t.topo_pos[2];
+        RC(slab_copy(slabs, row_start(1, ty), row_start(1, ty + 1), row_start(2, tz), row_start(2, tz + 1)));
+      }
     }
-    if (gen == SCARL_GEN_PADDED) {
-      GenArgs a;
-      RC(gen_args(ctx, dt, P, lay.Np, &a));
-      set_plan(&a, pl);
-      a.split = split;
-      a.k0 = (uint32_t)seedStart;
-      a.k1 = 0;
-      a.stream = o.stream;
-      a.epi = e;
-      RC(run_passes(ctx, dt, a));
-    } else if (gen == SCARL_GEN_SHINO) {
-      GenArgs a;
-      RC(shino_args(ctx, lay.Np, t.xRange, s->corrL, seedStart, &a));
-      a.epi = e;
-      RC(run_passes(ctx, 8, a));
-    } else {
-      const double* phi = phi_all ? (const double*)phi_all + nk * r : nullptr;
-      RC(dct_tile(ctx, (double*)ctx->tile.p, lay.Np, t.xRange, s->corrL, phi, nullptr, (uint32_t)seedStart,
-                  gm == SCARL_FFT_MPI));
-      Prof p(ctx, "k_blend_tile");
-      CK(launch_blend_tile(8, ctx->tile.p, lay.Np, e, ctx->stream));
-    }
+    return SCARL_OK;
+  }();
+  const int rc_slabs = slab_end(slabs);
+  RC(rc_tiles);
+  RC(rc_slabs);
+  if (stream_out) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    RC(check_status(ctx));
+    CK(cudaGetLastError());
+    return SCARL_OK;
   }
   if (o.normalize_field) {
     double avg, sd;
