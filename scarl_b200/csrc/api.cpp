@@ -390,7 +390,6 @@ int in_dev(scarl_ctx* ctx, Buf& buf, const void* user, size_t bytes, const void*
   return SCARL_OK;
 }
 
-bool pow2(int n) { return n >= 2 && (n & (n - 1)) == 0; }
 int default_pad(int Np) {
   int p = 1;
   while (p < 2 * Np) p <<= 1;

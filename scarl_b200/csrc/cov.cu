@@ -30,12 +30,15 @@ namespace {
 template <typename T, int N> __host__ __device__ constexpr int cov_E() {
   return eff_E<N, (sizeof(T) == 4 ? 16 : 8)>();
 }
-// lines per block, for 512-thread blocks at most: ROW (x lines, lanes along
-// a line) up to 32 lines, column layouts (lanes across lines) up to 16
+// lines per block, for blocks of at most 256 threads in FP32 (two blocks per
+// SM, whose barriers fall at different times) and 512 in FP64: ROW (x lines,
+// lanes along a line) up to 32 lines, column layouts (lanes across lines) up
+// to 16
 template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_B() {
   constexpr int tpl = N / cov_E<T, N>();
   constexpr int cap = ROW ? 32 : 16;
-  return (512 / tpl) < 1 ? 1 : ((512 / tpl) > cap ? cap : 512 / tpl);
+  constexpr int nt = sizeof(T) == 4 ? 256 : 512;
+  return (nt / tpl) < 1 ? 1 : ((nt / tpl) > cap ? cap : nt / tpl);
 }
 template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_threads() {
   return cov_B<T, N, ROW>() * (N / cov_E<T, N>());
@@ -46,6 +49,13 @@ template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_min
   constexpr int per_sm = 512;
   return (per_sm / cov_threads<T, N, ROW>()) > 32 ? 32
          : (per_sm / cov_threads<T, N, ROW>()) < 1 ? 1 : per_sm / cov_threads<T, N, ROW>();
+}
+// complex slots of a block's line region: the transform's scratch, then the
+// power rows (B lines N + 1 apart); FP32 twiddles follow it
+template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_rows() {
+  constexpr int fft = cov_B<T, N, ROW>() * line_slots<N, cov_E<T, N>()>();
+  constexpr int pw = cov_B<T, N, ROW>() * (N + 1);
+  return fft > pw ? fft : pw;
 }
 struct CovGeom {
   const void* f;
@@ -75,7 +85,15 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
   const int b = ROW ? (int)threadIdx.x / TPL : (int)threadIdx.x % B;
   const int t = ROW ? (int)threadIdx.x % TPL : (int)threadIdx.x / B;
   const T* f = static_cast<const T*>(g.f);
+  // FP32: the 2N twiddles e^{2 pi i m / M} in shared memory (once per block)
+  constexpr bool TWS = sizeof(T) == 4;
   const C* tw = static_cast<const C*>(g.tw);
+  if constexpr (TWS) {
+    C* tws = sm + cov_rows<T, N, ROW>();
+    for (int i = (int)threadIdx.x; i < 2 * N; i += (int)blockDim.x) tws[i] = __ldg(tw + i);
+    __syncthreads();
+    tw = tws;
+  }
   double acc[QB];
 #pragma unroll
   for (int q = 0; q < QB; ++q) acc[q] = 0.0;
@@ -136,7 +154,7 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
     for (int q = 0; q < QB; ++q) {
       const int k = (int)threadIdx.x + NT * q;
       if (k > N) break;
-      const C w = __ldg(tw + k);
+      const C w = tw[k];
       T s = T(0);
       for (int bb = 0; bb < B; ++bb) {
         const C zk = sm[bb * (N + 1) + (k == N ? 0 : k)];
@@ -159,11 +177,7 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
 }
 
 template <typename T, int N, bool ROW> size_t cov_smem() {
-  constexpr int E = cov_E<T, N>();
-  constexpr int B = cov_B<T, N, ROW>();
-  const size_t fft = (size_t)B * line_slots<N, E>() * sizeof(cplx_t<T>);
-  const size_t pw = (size_t)B * (N + 1) * sizeof(cplx_t<T>);
-  return fft > pw ? fft : pw;
+  return ((size_t)cov_rows<T, N, ROW>() + (sizeof(T) == 4 ? 2 * N : 0)) * sizeof(cplx_t<T>);
 }
 
 template <typename T, int N, bool ROW>
