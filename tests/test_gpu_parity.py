@@ -164,22 +164,23 @@ def test_generate_sample_vs_oracle(ctx, oracle, case, generator):
         assert rel(out32, ref) < TOL32
 
 
-@pytest.mark.parametrize("topo,generator,dtype", [
-    ((2, 2, 2), S.GEN_PADDED, S.F32),
-    ((2, 1, 3), S.GEN_PADDED, S.F64),
-    ((1, 2, 4), S.GEN_PADDED, S.F32 | S.SPLIT_BF16),
-    ((2, 1, 2), S.GEN_DCT, S.F64),
-    ((2, 3, 1), S.GEN_PADDED, S.F32),
-    ((1, 1, 1), S.GEN_PADDED, S.F32),
+@pytest.mark.parametrize("topo,generator,dtype,ov", [
+    ((2, 2, 2), S.GEN_PADDED, S.F32, (1, 1, 1.5)),
+    ((2, 1, 3), S.GEN_PADDED, S.F64, (1, 1, 1.5)),
+    ((1, 2, 4), S.GEN_PADDED, S.F32 | S.SPLIT_BF16, (1, 1, 1.5)),
+    ((2, 1, 2), S.GEN_DCT, S.F64, (1, 1, 1.5)),
+    ((2, 3, 1), S.GEN_PADDED, S.F32, (1, 1, 1.5)),
+    ((1, 1, 1), S.GEN_PADDED, S.F32, (1, 1, 1.5)),
+    ((1, 3, 2), S.GEN_PADDED, S.F32, (0, 0, 0)),      # overlap 0: neighbours share one plane
 ])
-def test_generate_sample_pinned_host_output(ctx, topo, generator, dtype):
+def test_generate_sample_pinned_host_output(ctx, topo, generator, dtype, ov):
     """Into pinned host memory the field comes back box by box (the y rows
     and z planes a row of tiles finishes) while later tile rows are
     generated: bit-identical to the device output and to a pageable host
     output, every byte copied once."""
     import torch
     cm = 3 if generator == S.GEN_PADDED else 1
-    s = S.make_sample((0, 0, 0), (60, 50, 90), (4, 5, 6), (1, 1, 1.5), (5, 5, 5), cm, 2, 1.0, 0.3, 9)
+    s = S.make_sample((0, 0, 0), (60, 50, 90), (4, 5, 6), ov, (5, 5, 5), cm, 2, 1.0, 0.3, 9)
     nb = topo[0] * topo[1] * topo[2]
     kw = dict(generator=generator, dtype=dtype, nb_procs=nb, topo=topo)
     ref, lay = S.generate_sample(ctx, s, **kw)  # pageable host memory
