@@ -9,11 +9,15 @@
 #include <array>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/scarl.h"
@@ -69,6 +73,70 @@ struct EnsPlan {
   cudaGraphExec_t exec = nullptr;
 };
 
+// A few host threads that copy a staged chunk into the caller's pageable
+// memory in parallel (memory bandwidth and first-touch page faults of a fresh
+// destination are shared among them).  run(f) calls f(p) for every part p <
+// parts(), part 0 on the calling thread, and returns when all are done.
+class HostPool {
+ public:
+  explicit HostPool(int workers) {
+    for (int i = 0; i < workers; ++i) th_.emplace_back([this, i] { loop(i + 1); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (std::thread& t : th_) t.join();
+  }
+  int parts() const { return (int)th_.size() + 1; }
+  void run(const std::function<void(int)>& f) {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      f_ = &f;
+      pending_ = (int)th_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    f(0);
+    std::unique_lock<std::mutex> l(m_);
+    done_.wait(l, [&] { return pending_ == 0; });
+    f_ = nullptr;
+  }
+
+ private:
+  void loop(int p) {
+    long seen = 0;
+    for (;;) {
+      const std::function<void(int)>* f;
+      {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+        f = f_;
+      }
+      (*f)(p);
+      std::lock_guard<std::mutex> g(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)>* f_ = nullptr;
+  int pending_ = 0;
+  long gen_ = 0;
+  bool stop_ = false;
+};
+
+// pageable host output: chunks of kRingChunk bytes through kRingSlots pinned
+// slots, for outputs of at least kRingMin bytes
+constexpr int kRingSlots = 4;
+constexpr size_t kRingChunk = (size_t)32 << 20;
+constexpr size_t kRingMin = (size_t)8 << 20;
+
 }  // namespace
 
 struct scarl_ctx {
@@ -87,6 +155,10 @@ struct scarl_ctx {
   // generation of the remaining tiles
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> slab_ev;
+  // pinned ring and copy threads of pageable host outputs
+  char* ring = nullptr;
+  cudaEvent_t ring_ev[kRingSlots] = {};
+  HostPool* hpool = nullptr;
   std::map<std::string, PaddedPlan> plans;
   std::map<long long, Buf> twiddles;
   std::map<int, Buf> dct_tabs;
@@ -283,10 +355,55 @@ int check_status(scarl_ctx* ctx) {
   return fail(ctx, SCARL_ETIMEOUT, "a bounded tensor-core wait expired; the output is invalid");
 }
 
+// Device -> pageable host copy through the pinned ring: the DMA fills the
+// next slots while the host threads move a finished slot into the caller's
+// memory (a direct copy into pageable memory runs at a fraction of the link
+// rate, and into a fresh allocation it also takes every page fault on one
+// thread).
+int copy_out_ring(scarl_ctx* ctx, void* user, const void* dev, size_t bytes) {
+  if (!ctx->ring) CK(cudaMallocHost((void**)&ctx->ring, kRingSlots * kRingChunk));
+  for (cudaEvent_t& e : ctx->ring_ev)
+    if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (!ctx->hpool) {
+    const unsigned hc = std::thread::hardware_concurrency();
+    ctx->hpool = new HostPool((int)std::min(7u, hc > 1 ? hc - 1 : 1u));
+  }
+  char* dst = static_cast<char*>(user);
+  const char* src = static_cast<const char*>(dev);
+  const size_t nch = (bytes + kRingChunk - 1) / kRingChunk;
+  auto enqueue = [&](size_t i) -> int {
+    const int slot = (int)(i % kRingSlots);
+    const size_t off = i * kRingChunk, len = std::min(kRingChunk, bytes - off);
+    CK(cudaMemcpyAsync(ctx->ring + slot * kRingChunk, src + off, len, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaEventRecord(ctx->ring_ev[slot], ctx->stream));
+    return SCARL_OK;
+  };
+  for (size_t i = 0; i < std::min(nch, (size_t)kRingSlots); ++i) RC(enqueue(i));
+  for (size_t i = 0; i < nch; ++i) {
+    const int slot = (int)(i % kRingSlots);
+    const size_t off = i * kRingChunk, len = std::min(kRingChunk, bytes - off);
+    CK(cudaEventSynchronize(ctx->ring_ev[slot]));
+    const char* from = ctx->ring + slot * kRingChunk;
+    const int np = ctx->hpool->parts();
+    const size_t part = ((len + np - 1) / np + 63) / 64 * 64;
+    ctx->hpool->run([&](int p) {
+      const size_t a = std::min(len, (size_t)p * part), b = std::min(len, a + part);
+      if (b > a) std::memcpy(dst + off + a, from + a, b - a);
+    });
+    if (i + kRingSlots < nch) RC(enqueue(i + kRingSlots));
+  }
+  ctx->d2h += bytes;
+  return SCARL_OK;
+}
+
 int finish_out(scarl_ctx* ctx, void* user, const void* dev, size_t bytes, bool host) {
   if (host) {
-    CK(cudaMemcpyAsync(user, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    ctx->d2h += bytes;
+    if (bytes >= kRingMin && !is_pinned_host(user)) {
+      RC(copy_out_ring(ctx, user, dev, bytes));
+    } else {
+      CK(cudaMemcpyAsync(user, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      ctx->d2h += bytes;
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     RC(check_status(ctx));
   }
@@ -1411,6 +1528,10 @@ int scarl_ctx_destroy(scarl_ctx* ctx) {
   if (ctx->pin_ev) cudaEventDestroy(ctx->pin_ev);
   if (ctx->pin) cudaFreeHost(ctx->pin);
   for (cudaEvent_t e : ctx->slab_ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->ring_ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->ring) cudaFreeHost(ctx->ring);
+  delete ctx->hpool;
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamDestroy(ctx->copy_stream);

@@ -188,6 +188,7 @@ def test_generate_sample_pinned_host_output(ctx, topo, generator, dtype, ov):
     tdt = torch.float64 if ref.dtype == np.float64 else torch.float32
     dev = torch.empty(int(np.prod(L)), dtype=tdt, device="cuda")
     S.generate_sample(ctx, s, out=dev, **kw)
+    ctx.sync()
     pin = torch.empty(int(np.prod(L)), dtype=tdt, pin_memory=True)
     hp = pin.numpy().reshape(L, order="F")
     for _ in range(2):
@@ -198,6 +199,40 @@ def test_generate_sample_pinned_host_output(ctx, topo, generator, dtype, ov):
         assert c1["d2h_bytes"] - c0["d2h_bytes"] == ref.nbytes
         np.testing.assert_array_equal(hp, ref)
     np.testing.assert_array_equal(dev.cpu().numpy().reshape(L, order="F"), ref)
+
+
+@pytest.mark.parametrize("dtype", [S.F32, S.F64])
+def test_large_pageable_host_output(ctx, dtype):
+    """Outputs of 8 MB and more into pageable host memory pass through the
+    context's pinned ring in 32 MB chunks (here several, the last one
+    ragged), copied out by host threads: bit-identical to the device output,
+    into fresh and into reused arrays."""
+    import torch
+    s = S.make_sample((0, 0, 0), (300, 300, 200), (6, 8, 5), (1, 1, 1), (9, 9, 9), 3, 2, 1.0, 0.3, 4)
+    kw = dict(dtype=dtype, nb_procs=4, topo=(2, 2, 1))
+    a, lay = S.generate_sample(ctx, s, **kw)  # fresh pageable array
+    L = tuple(int(v) for v in lay["L"])
+    assert a.nbytes > 2 * 32 * 2**20 and a.nbytes % (32 * 2**20) != 0
+    tdt = torch.float64 if a.dtype == np.float64 else torch.float32
+    dev = torch.empty(int(np.prod(L)), dtype=tdt, device="cuda")
+    S.generate_sample(ctx, s, out=dev, **kw)
+    ctx.sync()  # device outputs return once the work is queued
+    ref = dev.cpu().numpy().reshape(L, order="F")
+    np.testing.assert_array_equal(a, ref)
+    b = np.full(L, np.nan, dtype=a.dtype, order="F")
+    for _ in range(2):
+        c0 = ctx.counters()
+        S.generate_sample(ctx, s, out=b, **kw)
+        assert ctx.counters()["d2h_bytes"] - c0["d2h_bytes"] == b.nbytes
+        np.testing.assert_array_equal(b, ref)
+    # the single-tile generator through the same path
+    g = S.gen_padded(ctx, (260, 250, 130), (1, 1, 1), (5, 5, 5), 3, pad=(512, 512, 256), seed=3,
+                     dtype=dtype)
+    gd = torch.empty(260 * 250 * 130, dtype=tdt, device="cuda")
+    S.gen_padded(ctx, (260, 250, 130), (1, 1, 1), (5, 5, 5), 3, pad=(512, 512, 256), seed=3,
+                 dtype=dtype, out=gd)
+    ctx.sync()
+    np.testing.assert_array_equal(g, gd.cpu().numpy().reshape(g.shape, order="F"))
 
 
 def test_generate_sample_normalize_field(ctx, oracle):
