@@ -359,47 +359,95 @@ int check_status(scarl_ctx* ctx) {
 // next slots while the host threads move a finished slot into the caller's
 // memory (a direct copy into pageable memory runs at a fraction of the link
 // rate, and into a fresh allocation it also takes every page fault on one
-// thread).
-int copy_out_ring(scarl_ctx* ctx, void* user, const void* dev, size_t bytes) {
+// thread).  A piece is h runs of w <= kRingChunk bytes, `pitch` apart, from
+// byte offset off of both the device and the host buffer; its copy waits for
+// the event `after` when one is given.
+struct RingPiece {
+  size_t off, w, h;
+  cudaEvent_t after;
+};
+
+int ring_copy(scarl_ctx* ctx, void* user, const void* dev, size_t pitch, const std::vector<RingPiece>& pieces,
+              cudaStream_t s) {
   if (!ctx->ring) CK(cudaMallocHost((void**)&ctx->ring, kRingSlots * kRingChunk));
   for (cudaEvent_t& e : ctx->ring_ev)
     if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   if (!ctx->hpool) {
+    // SCARL_HOST_COPY_THREADS (copy threads including the caller), else up
+    // to 12 of the host's hardware threads
     const unsigned hc = std::thread::hardware_concurrency();
-    ctx->hpool = new HostPool((int)std::min(7u, hc > 1 ? hc - 1 : 1u));
+    int n = (int)std::min(12u, std::max(hc, 1u));
+    if (const char* v = std::getenv("SCARL_HOST_COPY_THREADS")) n = std::max(1, std::min(64, std::atoi(v)));
+    ctx->hpool = new HostPool(n - 1);
   }
   char* dst = static_cast<char*>(user);
   const char* src = static_cast<const char*>(dev);
-  const size_t nch = (bytes + kRingChunk - 1) / kRingChunk;
+  const size_t np = pieces.size();
   auto enqueue = [&](size_t i) -> int {
-    const int slot = (int)(i % kRingSlots);
-    const size_t off = i * kRingChunk, len = std::min(kRingChunk, bytes - off);
-    CK(cudaMemcpyAsync(ctx->ring + slot * kRingChunk, src + off, len, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaEventRecord(ctx->ring_ev[slot], ctx->stream));
+    const RingPiece& q = pieces[i];
+    char* slot = ctx->ring + (i % kRingSlots) * kRingChunk;
+    if (q.after) CK(cudaStreamWaitEvent(s, q.after, 0));
+    if (q.h == 1) CK(cudaMemcpyAsync(slot, src + q.off, q.w, cudaMemcpyDeviceToHost, s));
+    else CK(cudaMemcpy2DAsync(slot, q.w, src + q.off, pitch, q.w, q.h, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(ctx->ring_ev[i % kRingSlots], s));
     return SCARL_OK;
   };
-  for (size_t i = 0; i < std::min(nch, (size_t)kRingSlots); ++i) RC(enqueue(i));
-  for (size_t i = 0; i < nch; ++i) {
-    const int slot = (int)(i % kRingSlots);
-    const size_t off = i * kRingChunk, len = std::min(kRingChunk, bytes - off);
-    CK(cudaEventSynchronize(ctx->ring_ev[slot]));
-    const char* from = ctx->ring + slot * kRingChunk;
-    const int np = ctx->hpool->parts();
-    const size_t part = ((len + np - 1) / np + 63) / 64 * 64;
+  for (size_t i = 0; i < std::min(np, (size_t)kRingSlots); ++i) RC(enqueue(i));
+  size_t total = 0;
+  for (size_t i = 0; i < np; ++i) {
+    const RingPiece& q = pieces[i];
+    CK(cudaEventSynchronize(ctx->ring_ev[i % kRingSlots]));
+    const char* from = ctx->ring + (i % kRingSlots) * kRingChunk;
+    const size_t len = q.w * q.h;
+    const int parts = ctx->hpool->parts();
+    const size_t part = ((len + parts - 1) / parts + 63) / 64 * 64;
     ctx->hpool->run([&](int p) {
-      const size_t a = std::min(len, (size_t)p * part), b = std::min(len, a + part);
-      if (b > a) std::memcpy(dst + off + a, from + a, b - a);
+      // packed bytes [a, b) of the slot, run by run
+      size_t a = std::min(len, (size_t)p * part);
+      const size_t b = std::min(len, a + part);
+      while (a < b) {
+        const size_t r = a / q.w, x = a % q.w, n = std::min(b - a, q.w - x);
+        std::memcpy(dst + q.off + r * pitch + x, from + a, n);
+        a += n;
+      }
     });
-    if (i + kRingSlots < nch) RC(enqueue(i + kRingSlots));
+    total += len;
+    if (i + kRingSlots < np) RC(enqueue(i + kRingSlots));
   }
-  ctx->d2h += bytes;
+  ctx->d2h += total;
   return SCARL_OK;
+}
+
+// Contiguous bytes as ring pieces of at most one slot each.
+std::vector<RingPiece> ring_contiguous(size_t bytes) {
+  std::vector<RingPiece> v;
+  for (size_t off = 0; off < bytes; off += kRingChunk) v.push_back({off, std::min(kRingChunk, bytes - off), 1, nullptr});
+  return v;
+}
+
+// Rows [y0, y1) of planes [z0, z1) (x rows of `row` bytes, planes of `plane`
+// bytes) as ring pieces that wait for event e: whole row runs of several
+// planes per piece, or parts of one plane's run when a run exceeds a slot.
+void ring_box(std::vector<RingPiece>& v, size_t row, size_t plane, int y0, int y1, int z0, int z1,
+              cudaEvent_t e) {
+  if (y1 <= y0 || z1 <= z0) return;
+  const size_t w = (size_t)(y1 - y0) * row;
+  if (w <= kRingChunk) {
+    const int per = (int)std::max<size_t>(1, kRingChunk / w);
+    for (int z = z0; z < z1; z += per)
+      v.push_back({(size_t)z * plane + (size_t)y0 * row, w, (size_t)std::min(per, z1 - z), e});
+  } else {
+    const int per = (int)std::max<size_t>(1, kRingChunk / row);
+    for (int z = z0; z < z1; ++z)
+      for (int y = y0; y < y1; y += per)
+        v.push_back({(size_t)z * plane + (size_t)y * row, (size_t)std::min(per, y1 - y) * row, 1, e});
+  }
 }
 
 int finish_out(scarl_ctx* ctx, void* user, const void* dev, size_t bytes, bool host) {
   if (host) {
     if (bytes >= kRingMin && !is_pinned_host(user)) {
-      RC(copy_out_ring(ctx, user, dev, bytes));
+      RC(ring_copy(ctx, user, dev, 0, ring_contiguous(bytes), ctx->stream));
     } else {
       CK(cudaMemcpyAsync(user, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
       ctx->d2h += bytes;
@@ -2618,6 +2666,14 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   const bool stream_out = host && !o.normalize_field && lay.topo_shape[1] * lay.topo_shape[2] > 1 &&
                           is_pinned_host(global);
   if (stream_out) RC(slab_begin(ctx, slabs, global, dev, (size_t)lay.L[0] * dt, lay.L[1]));
+  // pageable host output of kRingMin bytes and more over several rows of
+  // tiles: the same boxes pass through the pinned ring, starting while the
+  // later rows are generated
+  const size_t row_b = (size_t)lay.L[0] * dt, plane_b = row_b * lay.L[1];
+  const bool ring_out = host && !stream_out && !o.normalize_field &&
+                        lay.topo_shape[1] * lay.topo_shape[2] > 1 && ng * dt >= kRingMin && row_b <= kRingChunk;
+  std::vector<RingPiece> ring_pieces;
+  size_t ring_nev = 0;
   auto row_start = [&](int d, int tp) {  // first plane (d = 1: y, 2: z) of the box of tile row tp
     return tp >= lay.topo_shape[d] ? lay.L[d] : std::min(lay.L[d], (lay.Np[d] - lay.Np_ovlp[d]) * tp);
   };
@@ -2653,9 +2709,21 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
         Prof p(ctx, "k_blend_tile");
         CK(launch_blend_tile(8, ctx->tile.p, lay.Np, e, ctx->stream));
       }
-      if (stream_out && t.topo_pos[0] == lay.topo_shape[0] - 1) {
+      if ((stream_out || ring_out) && t.topo_pos[0] == lay.topo_shape[0] - 1) {
         const int ty = t.topo_pos[1], tz = t.topo_pos[2];
-        RC(slab_copy(slabs, row_start(1, ty), row_start(1, ty + 1), row_start(2, tz), row_start(2, tz + 1)));
+        if (stream_out) {
+          RC(slab_copy(slabs, row_start(1, ty), row_start(1, ty + 1), row_start(2, tz), row_start(2, tz + 1)));
+        } else {
+          if (ctx->slab_ev.size() <= ring_nev) {
+            cudaEvent_t ev;
+            CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            ctx->slab_ev.push_back(ev);
+          }
+          cudaEvent_t ev = ctx->slab_ev[ring_nev++];
+          CK(cudaEventRecord(ev, ctx->stream));
+          ring_box(ring_pieces, row_b, plane_b, row_start(1, ty), row_start(1, ty + 1), row_start(2, tz),
+                   row_start(2, tz + 1), ev);
+        }
       }
     }
     return SCARL_OK;
@@ -2663,6 +2731,16 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   const int rc_slabs = slab_end(slabs);
   RC(rc_tiles);
   RC(rc_slabs);
+  if (ring_out) {
+    if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    const int rc_ring = ring_copy(ctx, global, dev, plane_b, ring_pieces, ctx->copy_stream);
+    CK(cudaStreamSynchronize(ctx->copy_stream));
+    RC(rc_ring);
+    CK(cudaStreamSynchronize(ctx->stream));
+    RC(check_status(ctx));
+    CK(cudaGetLastError());
+    return SCARL_OK;
+  }
   if (stream_out) {
     CK(cudaStreamSynchronize(ctx->stream));
     RC(check_status(ctx));

@@ -201,15 +201,16 @@ def test_generate_sample_pinned_host_output(ctx, topo, generator, dtype, ov):
     np.testing.assert_array_equal(dev.cpu().numpy().reshape(L, order="F"), ref)
 
 
-@pytest.mark.parametrize("dtype", [S.F32, S.F64])
-def test_large_pageable_host_output(ctx, dtype):
+@pytest.mark.parametrize("dtype,topo", [(S.F32, (2, 2, 1)), (S.F64, (2, 2, 1)), (S.F32, (1, 2, 3))])
+def test_large_pageable_host_output(ctx, dtype, topo):
     """Outputs of 8 MB and more into pageable host memory pass through the
-    context's pinned ring in 32 MB chunks (here several, the last one
-    ragged), copied out by host threads: bit-identical to the device output,
-    into fresh and into reused arrays."""
+    context's pinned ring in pieces of at most 32 MB (the boxes that each row
+    of tiles finishes, copied while later rows generate; for a single tile,
+    32 MB chunks with a ragged last one), moved out by host threads:
+    bit-identical to the device output, into fresh and into reused arrays."""
     import torch
     s = S.make_sample((0, 0, 0), (300, 300, 200), (6, 8, 5), (1, 1, 1), (9, 9, 9), 3, 2, 1.0, 0.3, 4)
-    kw = dict(dtype=dtype, nb_procs=4, topo=(2, 2, 1))
+    kw = dict(dtype=dtype, nb_procs=topo[0] * topo[1] * topo[2], topo=topo)
     a, lay = S.generate_sample(ctx, s, **kw)  # fresh pageable array
     L = tuple(int(v) for v in lay["L"])
     assert a.nbytes > 2 * 32 * 2**20 and a.nbytes % (32 * 2**20) != 0
