@@ -367,8 +367,9 @@ struct RingPiece {
   cudaEvent_t after;
 };
 
-int ring_copy(scarl_ctx* ctx, void* user, const void* dev, size_t pitch, const std::vector<RingPiece>& pieces,
-              cudaStream_t s) {
+// The ring's slots, their events (the last DMA into or out of each slot) and
+// the host copy threads, created on first use.
+int ring_init(scarl_ctx* ctx) {
   if (!ctx->ring) CK(cudaMallocHost((void**)&ctx->ring, kRingSlots * kRingChunk));
   for (cudaEvent_t& e : ctx->ring_ev)
     if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -380,12 +381,29 @@ int ring_copy(scarl_ctx* ctx, void* user, const void* dev, size_t pitch, const s
     if (const char* v = std::getenv("SCARL_HOST_COPY_THREADS")) n = std::max(1, std::min(64, std::atoi(v)));
     ctx->hpool = new HostPool(n - 1);
   }
+  return SCARL_OK;
+}
+
+// dst[a, b) = src[a, b) for the part of [0, len) that pool part p owns.
+void pool_memcpy(HostPool* pool, char* dst, const char* src, size_t len) {
+  const int parts = pool->parts();
+  const size_t part = ((len + parts - 1) / parts + 63) / 64 * 64;
+  pool->run([&](int p) {
+    const size_t a = std::min(len, (size_t)p * part), b = std::min(len, a + part);
+    if (b > a) std::memcpy(dst + a, src + a, b - a);
+  });
+}
+
+int ring_copy(scarl_ctx* ctx, void* user, const void* dev, size_t pitch, const std::vector<RingPiece>& pieces,
+              cudaStream_t s) {
+  RC(ring_init(ctx));
   char* dst = static_cast<char*>(user);
   const char* src = static_cast<const char*>(dev);
   const size_t np = pieces.size();
   auto enqueue = [&](size_t i) -> int {
     const RingPiece& q = pieces[i];
     char* slot = ctx->ring + (i % kRingSlots) * kRingChunk;
+    CK(cudaStreamWaitEvent(s, ctx->ring_ev[i % kRingSlots], 0));  // an earlier upload may still read it
     if (q.after) CK(cudaStreamWaitEvent(s, q.after, 0));
     if (q.h == 1) CK(cudaMemcpyAsync(slot, src + q.off, q.w, cudaMemcpyDeviceToHost, s));
     else CK(cudaMemcpy2DAsync(slot, q.w, src + q.off, pitch, q.w, q.h, cudaMemcpyDeviceToHost, s));
@@ -415,6 +433,31 @@ int ring_copy(scarl_ctx* ctx, void* user, const void* dev, size_t pitch, const s
     if (i + kRingSlots < np) RC(enqueue(i + kRingSlots));
   }
   ctx->d2h += total;
+  return SCARL_OK;
+}
+
+// Host -> device copy of a caller's buffer on the context's stream.  Pageable
+// buffers of kRingMin bytes and more go through the pinned ring: host threads
+// fill a slot while the DMA empties the previous ones.
+int copy_in(scarl_ctx* ctx, void* dst, const void* user, size_t bytes) {
+  if (bytes < kRingMin || is_pinned_host(user)) {
+    CK(cudaMemcpyAsync(dst, user, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h2d += bytes;
+    return SCARL_OK;
+  }
+  RC(ring_init(ctx));
+  const char* src = static_cast<const char*>(user);
+  char* d = static_cast<char*>(dst);
+  for (size_t off = 0, i = 0; off < bytes; off += kRingChunk, ++i) {
+    const int slot = (int)(i % kRingSlots);
+    const size_t len = std::min(kRingChunk, bytes - off);
+    char* sl = ctx->ring + slot * kRingChunk;
+    CK(cudaEventSynchronize(ctx->ring_ev[slot]));  // the slot's last DMA is done
+    pool_memcpy(ctx->hpool, sl, src + off, len);
+    CK(cudaMemcpyAsync(d + off, sl, len, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaEventRecord(ctx->ring_ev[slot], ctx->stream));
+  }
+  ctx->h2d += bytes;
   return SCARL_OK;
 }
 
@@ -549,8 +592,7 @@ int in_dev(scarl_ctx* ctx, Buf& buf, const void* user, size_t bytes, const void*
     return SCARL_OK;
   }
   RC(ensure(ctx, buf, bytes));
-  CK(cudaMemcpyAsync(buf.p, user, bytes, cudaMemcpyHostToDevice, ctx->stream));
-  ctx->h2d += bytes;
+  RC(copy_in(ctx, buf.p, user, bytes));
   *dev = buf.p;
   return SCARL_OK;
 }
@@ -2768,8 +2810,7 @@ int scarl_apply_unity_partition(scarl_ctx* ctx, double* field, const int Np[3],
   if (host) {
     RC(ensure(ctx, ctx->stage_out, n * 8));
     dev = ctx->stage_out.p;
-    CK(cudaMemcpyAsync(dev, field, n * 8, cudaMemcpyHostToDevice, ctx->stream));
-    ctx->h2d += n * 8;
+    RC(copy_in(ctx, dev, field, n * 8));
   } else {
     dev = field;
   }
@@ -2810,7 +2851,7 @@ int scarl_add_overlap(scarl_ctx* ctx, double* tiles, const int Np[3], const int 
   if (host) {
     RC(ensure(ctx, ctx->stage_out, n * 8));
     dev = ctx->stage_out.p;
-    CK(cudaMemcpyAsync(dev, tiles, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    RC(copy_in(ctx, dev, tiles, n * 8));
   } else {
     dev = tiles;
   }
@@ -2834,7 +2875,7 @@ int scarl_multivariate_transformation(scarl_ctx* ctx, void* field, int dtype, lo
   if (host) {
     RC(ensure(ctx, ctx->stage_out, (size_t)n * dtype));
     dev = ctx->stage_out.p;
-    CK(cudaMemcpyAsync(dev, field, (size_t)n * dtype, cudaMemcpyHostToDevice, ctx->stream));
+    RC(copy_in(ctx, dev, field, (size_t)n * dtype));
   } else {
     dev = field;
   }
@@ -2876,7 +2917,7 @@ int scarl_normalize_field(scarl_ctx* ctx, void* field, int dtype, long long n, d
   if (host) {
     RC(ensure(ctx, ctx->stage_out, (size_t)n * dtype));
     dev = ctx->stage_out.p;
-    CK(cudaMemcpyAsync(dev, field, (size_t)n * dtype, cudaMemcpyHostToDevice, ctx->stream));
+    RC(copy_in(ctx, dev, field, (size_t)n * dtype));
   } else {
     dev = field;
   }

@@ -106,3 +106,23 @@ def test_axis_cov_known_mean(ctx):
             a = np.take(g, range(0, n - h), axis=d)
             b = np.take(g, range(h, n), axis=d)
             assert c[d, h] == pytest.approx(np.mean(a * b), rel=1e-11, abs=1e-12)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_large_pageable_host_input(ctx, dtype):
+    """A pageable host field of 8 MB and more is uploaded through the
+    context's pinned ring (32 MB chunks, the last one ragged): the statistics
+    equal those of the same field passed as a device tensor, bit for bit, and
+    every byte is uploaded once."""
+    import torch
+    shape = (250, 260, 270)
+    f = np.asfortranarray(np.random.default_rng(5).standard_normal(shape).astype(dtype))
+    assert f.nbytes > 2 * 32 * 2**20 and f.nbytes % (32 * 2**20) != 0
+    c0 = ctx.counters()
+    m, v, c = S.axis_cov(ctx, f, shape, 40)
+    assert ctx.counters()["h2d_bytes"] - c0["h2d_bytes"] == f.nbytes
+    d = torch.from_numpy(f.reshape(-1, order="F").copy()).cuda()
+    md, vd, cd = S.axis_cov(ctx, d, shape, 40)
+    assert m == md and v == vd
+    np.testing.assert_array_equal(c, cd)
+    assert abs(m) < 1e-3 and abs(v - 1) < 1e-2
