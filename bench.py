@@ -585,7 +585,13 @@ def main():
 
     rel32, max32 = rel_to_f64(S.F32)
     rel, relmax = rel_to_f64(HEAD)
+    # ---- the reference's precision: every DFT and sum in FP64, same grid
+    for _ in range(args.warmup):
+        step(out=f64, dtype=S.F64)
+    ms_f64 = timed_steps(out=f64, dtype=S.F64)
     del f64
+    fp64 = {"value": round(world * npts / (ms_f64 * 1e-3) / 1e6, 2), "ms_per_step": round(ms_f64, 4),
+            "padded_grid": P_auto, "precision": "f64 (every DFT and sum in FP64, as the reference)"}
     pow2 = {"value": round(world * npts / (ms_pow2 * 1e-3) / 1e6, 2), "ms_per_step": round(ms_pow2, 4),
             "padded_grid": P_pow2, "pad_policy": "auto: smallest powers of two under the same rule"}
     fp32 = {"value": round(world * npts / (ms_f32 * 1e-3) / 1e6, 2), "ms_per_step": round(ms_f32, 4),
@@ -643,7 +649,7 @@ def main():
                 "data": "synthetic (Philox normals, seeded per rank)",
                 "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "max_err_vs_fp64": relmax,
                 "roofline": roof, "kernels": kern, "launch_variants": tuned, "plain_path": plain,
-                "fp32_path": fp32, "pow2_grid_path": pow2,
+                "fp32_path": fp32, "fp64_path": fp64, "pow2_grid_path": pow2,
                 "speedup_vs_plain_path": round(ms_full / ms, 3),
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
                 "ensemble": ens, "large_field": large, "learned_padding": learned}

@@ -1862,9 +1862,7 @@ int scarl_stat_file(scarl_ctx* ctx, const char* res_path, const char* dset_name,
                       dt == SCARL_F32 ? h32.data() : nullptr, &err))
     return fail(ctx, SCARL_EIO, err);
   RC(ensure(ctx, ctx->tile, n * dt));
-  CK(cudaMemcpyAsync(ctx->tile.p, dt == SCARL_F64 ? (const void*)h64.data() : (const void*)h32.data(),
-                     n * dt, cudaMemcpyHostToDevice, ctx->stream));
-  ctx->h2d += n * dt;
+  RC(copy_in(ctx, ctx->tile.p, dt == SCARL_F64 ? (const void*)h64.data() : (const void*)h32.data(), n * dt));
   double evA = 0.0, evS = 0.0;
   RC(scarl_moments(ctx, ctx->tile.p, dt, (long long)n, 1, &evA, &evS, globalAvg, globalStdDev));
   std::vector<h5::Attr> stats;
