@@ -71,6 +71,13 @@ class Clocks:
                 ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
                  "-lms", "50", "-f", self.path],
                 stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            # sampling is live before the timed region starts (nvidia-smi takes
+            # a while to write its first line)
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
