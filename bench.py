@@ -20,6 +20,7 @@ not shard across GPUs), weak scaling.  --impl reference times the CPU
 restatement of the same path on the host cores (tile sample).
 """
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -52,16 +53,21 @@ def load_peaks():
 
 
 class Clocks:
-    """nvidia-smi samples (50 ms) while the timed region runs."""
+    """nvidia-smi samples (50 ms); the record keeps those taken between
+    begin() and stop() (the timed region), by their timestamps."""
 
     FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,timestamp")
 
     def __init__(self, bus_id):
         self.bus = (bus_id or "").lower()
         self.proc = None
         self.path = None
+        self.t_begin = None
+
+    def begin(self):
+        self.t_begin = time.time()
 
     def start(self):
         try:
@@ -84,6 +90,8 @@ class Clocks:
     def stop(self):
         if not self.proc:
             return None
+        t_end = time.time()
+        time.sleep(0.12)  # the sample after the region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -94,7 +102,7 @@ class Clocks:
             with open(self.path) as fh:
                 for line in fh:
                     f = [x.strip() for x in line.split(",")]
-                    if len(f) < 10:
+                    if len(f) < 11:
                         continue
                     if self.bus and self.bus[-12:] not in f[1].lower():
                         continue
@@ -104,6 +112,17 @@ class Clocks:
             return None
         if not rows:
             return None
+
+        def stamp(x):
+            try:
+                return datetime.datetime.strptime(x, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                return None
+        if self.t_begin is not None:
+            inside = [r for r in rows if stamp(r[10]) is not None
+                      and self.t_begin <= stamp(r[10]) <= t_end + 0.06]
+            rows = inside or [r for r in rows if stamp(r[10]) is not None
+                              and stamp(r[10]) >= self.t_begin][:1] or rows[-1:]
 
         def num(x):
             try:
@@ -511,6 +530,7 @@ def main():
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    clk.begin()
     e0.record(stream)
     for _ in range(args.steps):
         step()
