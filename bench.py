@@ -573,14 +573,20 @@ def main():
     torch.cuda.synchronize()
     stats = ctx.profile_stats()
     ctx.profile(False)
-    pb = pass_bytes(lay, P_auto)
+    pb_tile = pass_bytes(lay, P_auto)
+    # passes 1 and 2 run batched over a field's tiles (one launch covers
+    # several tiles), pass 3 once per tile: bytes per launch = bytes per tile
+    # x tiles per launch
+    ntiles = int(lay["nb_tiles"])
+    tpl = {k: max(1, round(ntiles * nprof / n)) for k, (tot, n) in stats.items() if n}
+    pb = {k: b * tpl.get(k, 1) for k, b in pb_tile.items()}
     peak, peak_kind = load_peaks()
     kern = {}
     for k, (tot, n) in stats.items():
         avg = tot / max(n, 1)
         b = pb.get(k)
-        kern[k] = {"launches": n, "avg_ms": round(avg, 4), "share": None,
-                   "gbs": round(b / (avg * 1e-3) / 1e9, 1) if b else None}
+        kern[k] = {"launches": n, "tiles_per_launch": tpl.get(k, 1), "avg_ms": round(avg, 4),
+                   "share": None, "gbs": round(b / (avg * 1e-3) / 1e9, 1) if b else None}
     tot_all = sum(v[0] for v in stats.values()) or 1.0
     for k, (tot, n) in stats.items():
         kern[k]["share"] = round(tot / tot_all, 4)
@@ -589,7 +595,9 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if dom and os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(dom)
+            traffic = json.load(open(tpath)).get(dom)  # one tile's launch
+            if traffic is not None:
+                traffic = traffic * tpl.get(dom, 1)
         except Exception:
             traffic = None
     roof = None

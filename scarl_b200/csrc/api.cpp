@@ -155,6 +155,7 @@ struct scarl_ctx {
   // generation of the remaining tiles
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> slab_ev;
+  Buf targs;  // argument blocks and block maps of the tiles batched in passes 1-2
   // pinned ring and copy threads of pageable host outputs
   char* ring = nullptr;
   cudaEvent_t ring_ev[kRingSlots] = {};
@@ -794,6 +795,48 @@ int run_passes(scarl_ctx* ctx, int dt, const GenArgs& a) {
   {
     Prof p(ctx, "k_c2r_x");
     CK(launch_gen_pass(dt, 3, a, ctx->stream));
+  }
+  return SCARL_OK;
+}
+
+// Passes 1 and 2 of k tiles of one sample (same padded grid and tile shape,
+// one work buffer each) as one batched launch per pass: a pass over one tile
+// ends with a partial last wave (the persistent tensor-core pass 1 of the
+// 513^3 headline: 2700 items on 296 CTAs), over k tiles the waves pack.
+// Each tile computes exactly what its single launch computes.  grp[j] must
+// have its Philox schedule filled.
+int run_passes12_batched(scarl_ctx* ctx, int dt, const GenArgs* grp, int k) {
+  const GenArgs& a0 = grp[0];
+  const bool tc = a0.split && dt == 4 && a0.spec == SPEC_PHILOX && gen_z_tc_supported(a0.P[2]);
+  const int nb1 = tc ? gen_z_tc_items(a0) : gen_pass_blocks(dt, 1, a0.var[0], a0);
+  const int nb2 = gen_pass_blocks(dt, 2, a0.var[1], a0);
+  if (nb1 < 1 || nb2 < 1) return fail(ctx, SCARL_EUNSUPPORTED, "no batched launch for this grid");
+  if ((long long)nb1 * k > 2147483647LL || (long long)nb2 * k > 2147483647LL)
+    return fail(ctx, SCARL_EINVAL, "too many blocks for one batched launch");
+  // [k GenArgs][k items][k + 1 pass-1 offsets][k + 1 pass-2 offsets]
+  const size_t ab = (size_t)k * sizeof(GenArgs), bytes = ab + (size_t)(3 * k + 2) * sizeof(int);
+  RC(ensure(ctx, ctx->targs, bytes));
+  void* pin;
+  RC(pinned(ctx, bytes, &pin));
+  std::memcpy(pin, grp, ab);
+  int* h = reinterpret_cast<int*>(static_cast<char*>(pin) + ab);
+  for (int j = 0; j < k; ++j) h[j] = j;
+  for (int j = 0; j <= k; ++j) {
+    h[k + j] = j * nb1;
+    h[2 * k + 1 + j] = j * nb2;
+  }
+  RC(upload_pinned(ctx, ctx->targs.p, bytes));
+  const GenArgs* dargs = static_cast<const GenArgs*>(ctx->targs.p);
+  const int* di = reinterpret_cast<const int*>(static_cast<const char*>(ctx->targs.p) + ab);
+  const BatchMap m1{dargs, di, di + k, k, k * nb1};
+  const BatchMap m2{dargs, di, di + 2 * k + 1, k, k * nb2};
+  {
+    Prof p(ctx, tc ? "k_gen_z_tc" : "k_gen_z");
+    CK(tc ? launch_gen_z_tc_batch(a0, m1, ctx->stream) : launch_gen_pass_batch(dt, 1, a0.var[0], a0, m1, ctx->stream));
+  }
+  {
+    Prof p(ctx, "k_mid_y");
+    CK(launch_gen_pass_batch(dt, 2, a0.var[1], a0, m2, ctx->stream));
   }
   return SCARL_OK;
 }
@@ -1605,7 +1648,7 @@ int scarl_ctx_destroy(scarl_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   flush_marks(ctx);
-  for (Buf* b : {&ctx->work, &ctx->tile, &ctx->stage_out, &ctx->stage_in, &ctx->stage_in2,
+  for (Buf* b : {&ctx->work, &ctx->targs, &ctx->tile, &ctx->stage_out, &ctx->stage_in, &ctx->stage_in2,
                  &ctx->tabs, &ctx->dtabs, &ctx->part, &ctx->t1, &ctx->t2, &ctx->sk, &ctx->pmpw,
                  &ctx->status})
     release(ctx, *b);
@@ -2717,6 +2760,33 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   auto row_start = [&](int d, int tp) {  // first plane (d = 1: y, 2: z) of the box of tile row tp
     return tp >= lay.topo_shape[d] ? lay.L[d] : std::min(lay.L[d], (lay.Np[d] - lay.Np_ovlp[d]) * tp);
   };
+  // padded tiles: passes 1-2 batched over groups of up to kb tiles, one work
+  // buffer each (at most kBatchWork bytes of them); pass 3 per tile, in order
+  constexpr size_t kBatchWork = (size_t)4 << 30;
+  int kb = 1;
+  size_t wtile = 0;
+  if (gen == SCARL_GEN_PADDED && lay.nb_tiles > 1) {
+    wtile = (size_t)round_up(P[0] / 2 + 1, 16) * P[1] * lay.Np[2] * 2 * dt;
+    kb = (int)std::min<size_t>((size_t)lay.nb_tiles, std::max<size_t>(1, kBatchWork / wtile));
+    if (kb > 1 && ensure(ctx, ctx->work, wtile * kb) != SCARL_OK) kb = 1;  // budget: one tile at a time
+  }
+  std::vector<GenArgs> grp;
+  auto padded_args = [&](int r, GenArgs* a) -> int {
+    scarl_tile t;
+    tile_geometry(&lay, s->xMinGlob, r, &t);
+    RC(gen_args(ctx, dt, P, lay.Np, a));
+    set_plan(a, pl);
+    a->split = split;
+    a->k0 = (uint32_t)s->seedBase + 1u + (uint32_t)r;
+    a->k1 = 0;
+    a->stream = o.stream;
+    a->epi = epi;
+    for (int d = 0; d < 3; ++d) {
+      a->epi.off[d] = t.pos_0[d] - 1;
+      a->epi.ax[d] = axes[(size_t)r * 3 + d];
+    }
+    return SCARL_OK;
+  };
   const int rc_tiles = [&]() -> int {
     for (int r = 0; r < lay.nb_tiles; ++r) {
       scarl_tile t;
@@ -2727,15 +2797,22 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
         e.off[d] = t.pos_0[d] - 1;
         e.ax[d] = axes[(size_t)r * 3 + d];
       }
-      if (gen == SCARL_GEN_PADDED) {
+      if (gen == SCARL_GEN_PADDED && kb > 1) {
+        if (r % kb == 0) {
+          const int k = std::min(kb, lay.nb_tiles - r);
+          grp.resize(k);
+          for (int j = 0; j < k; ++j) {
+            RC(padded_args(r + j, &grp[j]));
+            grp[j].work = static_cast<char*>(ctx->work.p) + wtile * j;
+            philox_schedule(&grp[j]);
+          }
+          RC(run_passes12_batched(ctx, dt, grp.data(), k));
+        }
+        Prof p(ctx, "k_c2r_x");
+        CK(launch_gen_pass(dt, 3, grp[r % kb], ctx->stream));
+      } else if (gen == SCARL_GEN_PADDED) {
         GenArgs a;
-        RC(gen_args(ctx, dt, P, lay.Np, &a));
-        set_plan(&a, pl);
-        a.split = split;
-        a.k0 = (uint32_t)seedStart;
-        a.k1 = 0;
-        a.stream = o.stream;
-        a.epi = e;
+        RC(padded_args(r, &a));
         RC(run_passes(ctx, dt, a));
       } else if (gen == SCARL_GEN_SHINO) {
         GenArgs a;
