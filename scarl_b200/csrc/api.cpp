@@ -2760,14 +2760,20 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   auto row_start = [&](int d, int tp) {  // first plane (d = 1: y, 2: z) of the box of tile row tp
     return tp >= lay.topo_shape[d] ? lay.L[d] : std::min(lay.L[d], (lay.Np[d] - lay.Np_ovlp[d]) * tp);
   };
-  // padded tiles: passes 1-2 batched over groups of up to kb tiles, one work
-  // buffer each (at most kBatchWork bytes of them); pass 3 per tile, in order
+  // padded tiles whose pass 1 runs on the tensor cores (a persistent kernel,
+  // whose per-tile launches end with a partial wave): passes 1-2 batched over
+  // groups of up to kb tiles, one work buffer each (at most kBatchWork bytes
+  // of them); pass 3 per tile, in order.  The CUDA-core passes gain nothing
+  // from batching (measured: the FP32 pass 1 is slower batched) and run per tile.
   constexpr size_t kBatchWork = (size_t)4 << 30;
   int kb = 1;
   size_t wtile = 0;
-  if (gen == SCARL_GEN_PADDED && lay.nb_tiles > 1) {
+  if (gen == SCARL_GEN_PADDED && lay.nb_tiles > 1 && split && dt == 4 && gen_z_tc_supported(P[2])) {
     wtile = (size_t)round_up(P[0] / 2 + 1, 16) * P[1] * lay.Np[2] * 2 * dt;
     kb = (int)std::min<size_t>((size_t)lay.nb_tiles, std::max<size_t>(1, kBatchWork / wtile));
+    // an output streamed to the host takes one row of tiles per group, so
+    // that the first boxes are final (and copied) early
+    if (stream_out || ring_out) kb = std::min(kb, lay.topo_shape[0]);
     if (kb > 1 && ensure(ctx, ctx->work, wtile * kb) != SCARL_OK) kb = 1;  // budget: one tile at a time
   }
   std::vector<GenArgs> grp;

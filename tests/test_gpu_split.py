@@ -94,29 +94,39 @@ def test_split_blended_sample_vs_fp64(ctx):
         kw = dict(nb_procs=8, topo=(2, 2, 2), pad_policy=policy)
         f64, lay = S.generate_sample(ctx, s, dtype=S.F64, **kw)
         (f32s, _), st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, dtype=SPLIT, **kw))
-        assert st["k_gen_z_tc"][1] == 1  # one batched launch over the 8 tiles
+        assert st["k_gen_z_tc"][1] == 4  # host output: one batched launch per row of 2 tiles
         err = rel(f32s, f64)
         print(f"513^3 split rel-L2 {err:.2e} (policy {policy})")
         assert err < TOL
 
 
-@pytest.mark.parametrize("dtype,k1", [(SPLIT, "k_gen_z_tc"), (S.F32, "k_gen_z")])
-def test_batched_tiles_equal_per_tile_launches(ctx, dtype, k1):
-    """Passes 1 and 2 of a sample's tiles run as one batched launch each; a
-    context whose memory budget holds one tile's work buffer only runs them
-    per tile.  The two fields are bit-identical (513^3 headline deck)."""
+def test_batched_tiles_equal_per_tile_launches(ctx):
+    """With the tensor-core pass 1 and the field in device memory, passes 1
+    and 2 of a sample's 8 tiles run as one batched launch each; a context
+    whose memory budget holds one tile's work buffer only runs them per tile;
+    a host output takes one row of tiles per launch.  All three fields are
+    bit-identical (513^3 headline deck)."""
+    import torch
     s = S.make_sample((0, 0, 0), (512, 512, 512), (40, 20, 10), (2, 2, 2), (41, 21, 11),
                       corrMod=3, margiFirst=2, avg=1.0, std_dev=0.3)
-    kw = dict(dtype=dtype, nb_procs=8, topo=(2, 2, 2), pad_policy=S.PAD_SMOOTH)
-    (a, _), st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, **kw))
-    assert st[k1][1] == 1 and st["k_mid_y"][1] == 1 and st["k_c2r_x"][1] == 8
-    small = S.Context(0, budget_bytes=1 << 30)  # staging + one 185 MB work buffer fit, eight do not
+    kw = dict(dtype=SPLIT, nb_procs=8, topo=(2, 2, 2), pad_policy=S.PAD_SMOOTH)
+    n = 513 ** 3
+    a = torch.empty(n, dtype=torch.float32, device="cuda")
+    _, st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, out=a, **kw))
+    ctx.sync()
+    assert st["k_gen_z_tc"][1] == 1 and st["k_mid_y"][1] == 1 and st["k_c2r_x"][1] == 8
+    b = torch.empty(n, dtype=torch.float32, device="cuda")
+    small = S.Context(0, budget_bytes=1 << 30)  # one 185 MB work buffer fits, eight do not
     try:
-        (b, _), st1 = _ran_tc(small, lambda: S.generate_sample(small, s, **kw))
+        _, st1 = _ran_tc(small, lambda: S.generate_sample(small, s, out=b, **kw))
+        small.sync()
     finally:
         small.close()
-    assert st1[k1][1] == 8 and st1["k_mid_y"][1] == 8
-    np.testing.assert_array_equal(a, b)
+    assert st1["k_gen_z_tc"][1] == 8 and st1["k_mid_y"][1] == 8
+    assert torch.equal(a, b)
+    (h, _), st2 = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, **kw))
+    assert st2["k_gen_z_tc"][1] == 4
+    np.testing.assert_array_equal(h.reshape(-1, order="F"), a.cpu().numpy())
 
 
 def test_split_bounded_wait_reports_timeout(ctx, oracle):
@@ -136,3 +146,10 @@ def test_split_bounded_wait_reports_timeout(ctx, oracle):
     out = S.gen_padded(ctx, Np, (1, 1, 1), cl, 3, pad=P, seed=77, stream=3, dtype=SPLIT)
     assert rel(out, ref) < TOL
     ctx.sync()
+
+
+def test_fp32_tiles_run_per_tile(ctx):
+    """The CUDA-core FP32 passes run per tile (batching measured slower)."""
+    s = S.make_sample((0, 0, 0), (120, 100, 90), (8, 6, 5), (1, 1, 1), (5, 5, 5), corrMod=3)
+    (_, _), st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, dtype=S.F32, nb_procs=8, topo=(2, 2, 2)))
+    assert st["k_gen_z"][1] == 8 and st["k_mid_y"][1] == 8 and st["k_c2r_x"][1] == 8
