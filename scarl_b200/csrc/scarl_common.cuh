@@ -68,15 +68,14 @@ __device__ __forceinline__ u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1
 __device__ __forceinline__ u32x4 philox4x32_10_ks(u32x4 c, const uint32_t* ks) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
-    const uint32_t lo0 = 0xD2511F53u * c.x;
-    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
-    const uint32_t lo1 = 0xCD9E8D57u * c.z;
-    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+    // each 32 x 32 -> 64-bit product as one wide multiply (both halves)
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
     u32x4 n;
-    n.x = hi1 ^ c.y ^ ks[r];
-    n.y = lo1;
-    n.z = hi0 ^ c.w ^ ks[10 + r];
-    n.w = lo0;
+    n.x = (uint32_t)(p1 >> 32) ^ c.y ^ ks[r];
+    n.y = (uint32_t)p1;
+    n.z = (uint32_t)(p0 >> 32) ^ c.w ^ ks[10 + r];
+    n.w = (uint32_t)p0;
     c = n;
   }
   return c;
