@@ -148,6 +148,31 @@ def test_split_bounded_wait_reports_timeout(ctx, oracle):
     ctx.sync()
 
 
+def test_batched_tiles_ragged_groups(ctx):
+    """Tiles of 555 MB work buffers (991^3 field, 2x2x2 tiles on the 512^3 grid):
+    the 4 GB batching cap takes them in groups of 7 and 1; the field equals
+    per-tile launches bit for bit."""
+    import torch
+    s = S.make_sample((0, 0, 0), (990, 990, 990), (4, 4, 4), (1, 1, 1), (5, 5, 5), corrMod=3)
+    kw = dict(dtype=SPLIT, nb_procs=8, topo=(2, 2, 2), pad_policy=S.PAD_SMOOTH)
+    n = 991 ** 3
+    a = torch.empty(n, dtype=torch.float32, device="cuda")
+    _, st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, out=a, **kw))
+    ctx.sync()
+    assert st["k_gen_z_tc"][1] == 2 and st["k_mid_y"][1] == 2 and st["k_c2r_x"][1] == 8
+    b = torch.empty(n, dtype=torch.float32, device="cuda")
+    small = S.Context(0, budget_bytes=1 << 30)
+    try:
+        _, st1 = _ran_tc(small, lambda: S.generate_sample(small, s, out=b, **kw))
+        small.sync()
+    finally:
+        small.close()
+    assert st1["k_gen_z_tc"][1] == 8
+    assert torch.equal(a, b)
+    del a, b
+    torch.cuda.empty_cache()
+
+
 def test_fp32_tiles_run_per_tile(ctx):
     """The CUDA-core FP32 passes run per tile (batching measured slower)."""
     s = S.make_sample((0, 0, 0), (120, 100, 90), (8, 6, 5), (1, 1, 1), (5, 5, 5), corrMod=3)
