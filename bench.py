@@ -52,6 +52,34 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def load_bf16_peak():
+    """Dense BF16 peak (TFLOP/s) for a kernel timed in isolation: the measured
+    burst figure, else 1590 (an earlier measurement on this hardware)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+# tensor-core pass 1 configurations by z length: (N1, N2, lines per work item)
+TC_CFG = {256: (16, 16, 16), 320: (8, 40, 32), 384: (16, 24, 16), 512: (16, 32, 16), 1024: (32, 32, 8)}
+
+
+def tc_flops_per_tile(P):
+    """BF16 MMA flops of one tile's tensor-core pass 1 (2 M N K per product,
+    three split products per stage): stage 1 has LB N1 rows and K = N =
+    2 N2, stage 2 LB N2 rows and K = N = 2 N1; every work item of LB lines
+    runs both stages."""
+    if P[2] not in TC_CFG:
+        return None
+    n1, n2, lb = TC_CFG[P[2]]
+    items = -(-((P[0] // 2 + 1) * P[1]) // lb)
+    per_item = 3 * 2 * (lb * n1) * (2 * n2) ** 2 + 3 * 2 * (lb * n2) * (2 * n1) ** 2
+    return items * per_item
+
+
 class Clocks:
     """nvidia-smi samples (50 ms); the record keeps those taken between
     begin() and stop() (the timed region), by their timestamps."""
@@ -607,6 +635,18 @@ def main():
                 "frac": round(ach / peak, 4), "traffic": traffic,
                 "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_launch": pb[dom]}
 
+    # ---- the tensor-core stages of pass 1: MMA throughput of the same launches
+    tensor = None
+    ftile = tc_flops_per_tile(P_auto)
+    if ftile and "k_gen_z_tc" in stats:
+        tot, n = stats["k_gen_z_tc"]
+        tflops = ftile * tpl.get("k_gen_z_tc", 1) / (tot / n * 1e-3) / 1e12
+        tpeak, tkind = load_bf16_peak()
+        tensor = {"kernel": "k_gen_z_tc", "flops_per_tile": ftile, "achieved_tflops": round(tflops, 1),
+                  "peak_tflops": tpeak, "peak_source": f"{tkind} bf16_tflops",
+                  "frac": round(tflops / tpeak, 4),
+                  "note": "split BF16: three MMAs per DFT stage (head x head, head x tail, tail x head)"}
+
     # ---- accuracy of the FP32 fields against the FP64 path (same seed)
     f64 = torch.empty(npts, dtype=torch.float64, device="cuda")
     step(out=f64, dtype=S.F64)
@@ -683,7 +723,7 @@ def main():
                 "dtype": "f32 (z DFT: bf16 head/tail products, f32 accumulation)",
                 "data": "synthetic (Philox normals, seeded per rank)",
                 "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "max_err_vs_fp64": relmax,
-                "roofline": roof, "kernels": kern, "launch_variants": tuned, "plain_path": plain,
+                "roofline": roof, "tensor_stages": tensor, "kernels": kern, "launch_variants": tuned, "plain_path": plain,
                 "fp32_path": fp32, "fp64_path": fp64, "pow2_grid_path": pow2,
                 "speedup_vs_plain_path": round(ms_full / ms, 3),
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
