@@ -339,6 +339,7 @@ void so_tile_geometry(const int Np[3], const int Np_ovlp[3], const int topo_pos[
 void so_unity_partition_weights(const int Np[3], const int Np_ovlp[3], int partitionType,
                                 const int topo_pos[3], const int topo_shape[3], double* w) {
   const int64_t n = (int64_t)Np[0] * Np[1] * Np[2];
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) w[i] = 1.0;
   for (int jj = 1; jj <= 2; ++jj) {
     for (int ii = 0; ii < 3; ++ii) {
@@ -353,16 +354,17 @@ void so_unity_partition_weights(const int Np[3], const int Np_ovlp[3], int parti
       if (partitionType == 1)
         for (int kk = 0; kk < no; ++kk) pat[kk] = (1.0 + cos(SO_PI_REF * pat[kk])) / 2.0;
       int D = (jj == 1) ? 0 : Np[ii] - no;
-      for (int t = 0; t < no; ++t) {
-        int plane = D + t;
-        for (int k = 0; k < Np[2]; ++k)
-          for (int j = 0; j < Np[1]; ++j)
-            for (int i = 0; i < Np[0]; ++i) {
-              int c[3] = {i, j, k};
-              if (c[ii] != plane) continue;
-              w[i + (int64_t)Np[0] * (j + (int64_t)Np[1] * k)] *= pat[t];
-            }
-      }
+      /* every point of plane D + t (index ii) takes factor pat[t]; a point
+       * lies in one plane per (jj, ii), so the product order per point is
+       * the reference's */
+#pragma omp parallel for schedule(static)
+      for (int k = 0; k < Np[2]; ++k)
+        for (int j = 0; j < Np[1]; ++j)
+          for (int i = 0; i < Np[0]; ++i) {
+            const int c = ii == 0 ? i : (ii == 1 ? j : k);
+            if (c < D || c >= D + no) continue;
+            w[i + (int64_t)Np[0] * (j + (int64_t)Np[1] * k)] *= pat[c - D];
+          }
       free(pat);
     }
   }
@@ -374,6 +376,7 @@ void so_apply_unity_partition(const int Np[3], const int Np_ovlp[3], int partiti
   const int64_t n = (int64_t)Np[0] * Np[1] * Np[2];
   double* w = (double*)malloc(sizeof(double) * n);
   so_unity_partition_weights(Np, Np_ovlp, partitionType, topo_pos, topo_shape, w);
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) f[i] = f[i] * sqrt(w[i]);
   free(w);
 }
@@ -429,6 +432,7 @@ void so_add_overlap(double* const* RF, const int Np[3], const int Np_ovlp[3],
         }
   }
   for (int r = 0; r < nb; ++r) {
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; ++i) RF[r][i] = RF[r][i] + acc[r][i];
     free(acc[r]);
   }
@@ -516,6 +520,7 @@ void so_assemble_global(double* const* RF, const int Np[3], const int Np_ovlp[3]
     so_get_topo_pos(r, topo_shape, pos);
     int o[3];
     for (int d = 0; d < 3; ++d) o[d] = (Np[d] - Np_ovlp[d]) * pos[d];
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < Np[2]; ++k)
       for (int j = 0; j < Np[1]; ++j)
         for (int i = 0; i < Np[0]; ++i)
@@ -531,7 +536,8 @@ void so_assemble_global(double* const* RF, const int Np[3], const int Np_ovlp[3]
 typedef struct {
   int n;
   int pow2;
-  zc* tw;      /* e^{-2 pi i k / n}, k < n (pow2) */
+  int nf, fac[32]; /* mixed radix: radices 4, 2, 3, 5, 7 whose product is n (nf > 0) */
+  zc* tw;      /* e^{-2 pi i k / n}, k < n (pow2 and mixed radix) */
   int* rev;
   int m;       /* Bluestein convolution length */
   zc* chirp;   /* e^{-i pi k^2 / n} */
@@ -562,6 +568,57 @@ static void so_fft_pow2(const so_plan* p, zc* x) {
 
 static so_plan* so_plan_get(int n);
 
+/* n as a product of the radices 4, 2, 3, 5, 7 (fours first); 0 when n has
+ * another prime factor. */
+static int so_factor(int n, int fac[32], int* nf) {
+  int k = 0;
+  const int rad[5] = {4, 2, 3, 5, 7};
+  for (int i = 0; i < 5 && n > 1; ++i)
+    while (n % rad[i] == 0 && k < 32) { fac[k++] = rad[i]; n /= rad[i]; }
+  *nf = n == 1 ? k : 0;
+  return n == 1;
+}
+
+/* Unnormalised forward DFT by Stockham autosort over the plan's radices
+ * (Govindaraju et al., SC08): stage s with span Ns reads x[j + q n / R],
+ * twiddles by e^{-2 pi i q (j mod Ns) / (Ns R)}, takes a length-R DFT and
+ * writes y[(j / Ns) Ns R + (j mod Ns) + u Ns]. */
+static void so_fft_mixed(const so_plan* p, zc* x) {
+  const int n = p->n;
+  zc* buf = (zc*)malloc(sizeof(zc) * n);
+  zc* a = x;
+  zc* b = buf;
+  int Ns = 1;
+  for (int s = 0; s < p->nf; ++s) {
+    const int R = p->fac[s], stride = n / R, tstep = n / (Ns * R);
+    for (int j = 0; j < stride; ++j) {
+      zc v[8], y[8];
+      const int k = j % Ns;
+      for (int q = 0; q < R; ++q) v[q] = a[j + q * stride] * p->tw[q * k * tstep];
+      if (R == 2) {
+        y[0] = v[0] + v[1];
+        y[1] = v[0] - v[1];
+      } else if (R == 4) {
+        const zc t0 = v[0] + v[2], t1 = v[0] - v[2], t2 = v[1] + v[3], d = v[1] - v[3];
+        const zc t3 = cimag(d) - I * creal(d); /* -i (v1 - v3) */
+        y[0] = t0 + t2; y[2] = t0 - t2; y[1] = t1 + t3; y[3] = t1 - t3;
+      } else {
+        for (int u = 0; u < R; ++u) {
+          zc acc = v[0];
+          for (int q = 1; q < R; ++q) acc += v[q] * p->tw[((u * q) % R) * stride];
+          y[u] = acc;
+        }
+      }
+      const int d = (j / Ns) * Ns * R + k;
+      for (int u = 0; u < R; ++u) b[d + u * Ns] = y[u];
+    }
+    zc* t = a; a = b; b = t;
+    Ns *= R;
+  }
+  if (a != x) memcpy(x, a, sizeof(zc) * n);
+  free(buf);
+}
+
 static so_plan* so_plan_make(int n) {
   so_plan* p = (so_plan*)calloc(1, sizeof(so_plan));
   p->n = n;
@@ -579,6 +636,12 @@ static so_plan* so_plan_make(int n) {
       int r = 0;
       for (int b = 0; b < lg; ++b) if (i & (1 << b)) r |= 1 << (lg - 1 - b);
       p->rev[i] = r;
+    }
+  } else if (so_factor(n, p->fac, &p->nf)) {
+    p->tw = (zc*)malloc(sizeof(zc) * n);
+    for (int k = 0; k < n; ++k) {
+      double a = -2.0 * M_PI * (double)k / (double)n;
+      p->tw[k] = cos(a) + I * sin(a);
     }
   } else {
     int m = 1;
@@ -624,6 +687,7 @@ static void so_fft_fwd(zc* x, int n) {
   if (n <= 1) return;
   so_plan* p = so_plan_get(n);
   if (p->pow2) { so_fft_pow2(p, x); return; }
+  if (p->nf) { so_fft_mixed(p, x); return; }
   /* Bluestein: X_k = c_k * sum_j (x_j c_j) conj(c_{k-j}) */
   int m = p->m;
   so_plan* pm = so_plan_get(m);
@@ -953,19 +1017,41 @@ void so_gen_std_gauss_shino_fft(double* out, const int Np[3], const double xRang
  *   1 Gaussian:     C(r) = exp(-pi sum (r_d/l_d)^2)
  *   3 exponential:  C(r) = exp(-|r/a|), a = l/2
  *   2 von Karman:   Matern(nu) with a = l Gamma(nu) / (2 sqrt(pi) Gamma(nu+1/2)) */
-double so_spectrum(int corrMod, double nu, const double corrL[3], const double f[3]) {
-  if (corrMod == 1) {
+/* The model constants of so_spectrum, prepared once per grid; so_spec_eval
+ * forms each product in the order so_spectrum always has, so its values are
+ * those of so_spectrum bit for bit. */
+typedef struct {
+  int corrMod;
+  double corrL[3], t[3], c, p;
+} so_spec;
+
+static void so_spec_prep(so_spec* s, int corrMod, double nu, const double corrL[3]) {
+  s->corrMod = corrMod;
+  for (int d = 0; d < 3; ++d) s->corrL[d] = corrL[d];
+  if (corrMod == 1) return;
+  if (corrMod == 3) { nu = 0.5; }
+  double sc = tgamma(nu) / (2.0 * sqrt(M_PI) * tgamma(nu + 0.5)), a[3];
+  for (int d = 0; d < 3; ++d) { a[d] = corrL[d] * sc; s->t[d] = 4.0 * M_PI * M_PI * a[d] * a[d]; }
+  s->c = 8.0 * pow(M_PI, 1.5) * tgamma(nu + 1.5) / tgamma(nu) * a[0] * a[1] * a[2];
+  s->p = -(nu + 1.5);
+}
+
+static double so_spec_eval(const so_spec* s, const double f[3]) {
+  if (s->corrMod == 1) {
     double S = 1.0;
-    for (int d = 0; d < 3; ++d) S *= corrL[d] * exp(-M_PI * corrL[d] * corrL[d] * f[d] * f[d]);
+    for (int d = 0; d < 3; ++d)
+      S *= s->corrL[d] * exp(-M_PI * s->corrL[d] * s->corrL[d] * f[d] * f[d]);
     return S;
   }
-  double a[3], q = 0.0, c, p;
-  if (corrMod == 3) { nu = 0.5; }
-  double sc = tgamma(nu) / (2.0 * sqrt(M_PI) * tgamma(nu + 0.5));
-  for (int d = 0; d < 3; ++d) { a[d] = corrL[d] * sc; q += 4.0 * M_PI * M_PI * a[d] * a[d] * f[d] * f[d]; }
-  c = 8.0 * pow(M_PI, 1.5) * tgamma(nu + 1.5) / tgamma(nu) * a[0] * a[1] * a[2];
-  p = -(nu + 1.5);
-  return c * pow(1.0 + q, p);
+  double q = 0.0;
+  for (int d = 0; d < 3; ++d) q += s->t[d] * f[d] * f[d];
+  return s->c * pow(1.0 + q, s->p);
+}
+
+double so_spectrum(int corrMod, double nu, const double corrL[3], const double f[3]) {
+  so_spec s;
+  so_spec_prep(&s, corrMod, nu, corrL);
+  return so_spec_eval(&s, f);
 }
 
 static inline double so_freq(int k, int P, double dx) {
@@ -979,6 +1065,8 @@ double so_spectrum_sum(int corrMod, double nu, const int P[3], const double dx[3
   const int Hx = P[0] / 2 + 1;
   const double dk3 = (1.0 / (P[0] * dx[0])) * (1.0 / (P[1] * dx[1])) * (1.0 / (P[2] * dx[2]));
   double* part = (double*)calloc(P[2], sizeof(double));
+  so_spec sp;
+  so_spec_prep(&sp, corrMod, nu, corrL);
 #pragma omp parallel for schedule(static)
   for (int kz = 0; kz < P[2]; ++kz) {
     double s = 0.0;
@@ -986,7 +1074,7 @@ double so_spectrum_sum(int corrMod, double nu, const int P[3], const double dx[3
       for (int kx = 0; kx < Hx; ++kx) {
         double f[3] = {so_freq(kx, P[0], dx[0]), so_freq(ky, P[1], dx[1]), so_freq(kz, P[2], dx[2])};
         double c = (kx == 0 || 2 * kx == P[0]) ? 1.0 : 2.0;
-        s += c * so_spectrum(corrMod, nu, corrL, f) * dk3;
+        s += c * so_spec_eval(&sp, f) * dk3;
       }
     part[kz] = s;
   }
@@ -1001,14 +1089,15 @@ double so_spectrum_sum(int corrMod, double nu, const int P[3], const double dx[3
  *   g = 1 on the kx = 0 and kx = P0/2 planes, 1/sqrt(2) elsewhere,
  * so that the C2R output has variance sum_m S dk^3 / norm (1 when
  * normalised).  xi: injected pairs, or canonical Philox normals. */
-void so_padded_spectrum(int corrMod, double nu, const int P[3], const double dx[3],
-                        const double corrL[3], int normalise, uint64_t seed, uint32_t stream,
-                        const double* xi, double* Hd) {
+static void so_padded_spectrum_n(int corrMod, double nu, const int P[3], const double dx[3],
+                                 const double corrL[3], double norm, uint64_t seed,
+                                 uint32_t stream, const double* xi, double* Hd) {
   zc* H = (zc*)Hd;
   const int Hx = P[0] / 2 + 1;
   const int64_t M = (int64_t)Hx * P[1] * P[2];
   const double dk3 = (1.0 / (P[0] * dx[0])) * (1.0 / (P[1] * dx[1])) * (1.0 / (P[2] * dx[2]));
-  double norm = normalise ? so_spectrum_sum(corrMod, nu, P, dx, corrL) : 1.0;
+  so_spec sp;
+  so_spec_prep(&sp, corrMod, nu, corrL);
   double* own = NULL;
   if (!xi) {
     own = (double*)malloc(sizeof(double) * 2 * M);
@@ -1022,20 +1111,36 @@ void so_padded_spectrum(int corrMod, double nu, const int P[3], const double dx[
         int64_t m = kx + (int64_t)Hx * (ky + (int64_t)P[1] * kz);
         double f[3] = {so_freq(kx, P[0], dx[0]), so_freq(ky, P[1], dx[1]), so_freq(kz, P[2], dx[2])};
         double g = (kx == 0 || 2 * kx == P[0]) ? 1.0 : M_SQRT1_2;
-        double A = sqrt(so_spectrum(corrMod, nu, corrL, f) * dk3 / norm) * g;
+        double A = sqrt(so_spec_eval(&sp, f) * dk3 / norm) * g;
         H[m] = A * xi[2 * m] + I * (A * xi[2 * m + 1]);
       }
   free(own);
 }
 
+void so_padded_spectrum(int corrMod, double nu, const int P[3], const double dx[3],
+                        const double corrL[3], int normalise, uint64_t seed, uint32_t stream,
+                        const double* xi, double* Hd) {
+  double norm = normalise ? so_spectrum_sum(corrMod, nu, P, dx, corrL) : 1.0;
+  so_padded_spectrum_n(corrMod, nu, P, dx, corrL, norm, seed, stream, xi, Hd);
+}
+
+/* so_gen_padded with the normalisation sum given (tiles of one sample share
+ * their padded grid, so the sum is formed once per sample). */
+static void so_gen_padded_n(double* out, const int Np[3], const int P[3], const double dx[3],
+                            const double corrL[3], int corrMod, double nu, double norm,
+                            uint64_t seed, uint32_t stream, const double* xi) {
+  const int Hx = P[0] / 2 + 1;
+  double* H = (double*)malloc(sizeof(double) * 2 * (int64_t)Hx * P[1] * P[2]);
+  so_padded_spectrum_n(corrMod, nu, P, dx, corrL, norm, seed, stream, xi, H);
+  so_c2r_3d_crop(H, P, Np, out);
+  free(H);
+}
+
 void so_gen_padded(double* out, const int Np[3], const int P[3], const double dx[3],
                    const double corrL[3], int corrMod, double nu, int normalise,
                    uint64_t seed, uint32_t stream, const double* xi) {
-  const int Hx = P[0] / 2 + 1;
-  double* H = (double*)malloc(sizeof(double) * 2 * (int64_t)Hx * P[1] * P[2]);
-  so_padded_spectrum(corrMod, nu, P, dx, corrL, normalise, seed, stream, xi, H);
-  so_c2r_3d_crop(H, P, Np, out);
-  free(H);
+  double norm = normalise ? so_spectrum_sum(corrMod, nu, P, dx, corrL) : 1.0;
+  so_gen_padded_n(out, Np, P, dx, corrL, corrMod, nu, norm, seed, stream, xi);
 }
 
 /* so_gen_padded with the spectrum synthesised inside the z pass (no full
@@ -1052,6 +1157,8 @@ void so_gen_padded_stream(double* out, const int Np[3], const int P[3], const do
   const int st = line_stride < 1 ? 1 : line_stride;
   zc* T = (zc*)calloc((size_t)Hx * P[1] * Nz, sizeof(zc));
   so_plan_get(P[0]); so_plan_get(P[1]); so_plan_get(P[2]);
+  so_spec sp;
+  so_spec_prep(&sp, corrMod, nu, corrL);
   int mx = P[0] > P[1] ? P[0] : P[1];
   if (P[2] > mx) mx = P[2];
 #pragma omp parallel
@@ -1068,7 +1175,7 @@ void so_gen_padded_stream(double* out, const int Np[3], const int P[3], const do
           const int kz = kz0 + half * h;
           double f[3] = {so_freq(kx, P[0], dx[0]), so_freq(ky, P[1], dx[1]), so_freq(kz, P[2], dx[2])};
           double g = (kx == 0 || 2 * kx == P[0]) ? 1.0 : M_SQRT1_2;
-          double A = sqrt(so_spectrum(corrMod, nu, corrL, f) * dk3 / norm) * g;
+          double A = sqrt(so_spec_eval(&sp, f) * dk3 / norm) * g;
           line[kz] = A * nv[2 * half] + I * (A * nv[2 * half + 1]);
         }
       }
@@ -1133,6 +1240,10 @@ int so_generate_sample(int generator, const double xMin[3], const double xMax[3]
   const int nb = topo[0] * topo[1] * topo[2];
   const int64_t n = (int64_t)Np[0] * Np[1] * Np[2];
   double** RF = (double**)malloc(sizeof(double*) * nb);
+  int Ppad[3];
+  for (int d = 0; d < 3; ++d) Ppad[d] = pad ? pad[d] : so_pow2_pad(Np[d]);
+  const double norm = (generator == 3 && normalise_spectrum)
+                          ? so_spectrum_sum(corrMod, nu, Ppad, xStep, corrL) : 1.0;
   for (int r = 0; r < nb; ++r) {
     RF[r] = (double*)malloc(sizeof(double) * n);
     int pos[3], p0[3], pN[3];
@@ -1151,10 +1262,8 @@ int so_generate_sample(int generator, const double xMin[3], const double xMax[3]
     } else if (generator == 2) {
       so_gen_std_gauss_shino_fft(RF[r], Np, xr, corrL, seedStart, 0);
     } else {
-      int P[3];
-      for (int d = 0; d < 3; ++d) P[d] = pad ? pad[d] : so_pow2_pad(Np[d]);
-      so_gen_padded(RF[r], Np, P, xStep, corrL, corrMod, nu, normalise_spectrum,
-                    (uint64_t)(uint32_t)seedStart, 0, NULL);
+      so_gen_padded_n(RF[r], Np, Ppad, xStep, corrL, corrMod, nu, norm,
+                      (uint64_t)(uint32_t)seedStart, 0, NULL);
     }
     so_apply_unity_partition(Np, No, 1, pos, topo, RF[r]);
   }

@@ -85,7 +85,8 @@ def test_dct3_3d(oracle):
     np.testing.assert_allclose(oracle.dct3_3d(x), sfft.dctn(x, type=3), rtol=1e-12, atol=1e-12)
 
 
-@pytest.mark.parametrize("n", [1, 2, 8, 12, 64, 97, 513])
+# 97 and 513 = 27 x 19: Bluestein; 12, 320, 384, 448, 1792: mixed radix (4, 2, 3, 5, 7)
+@pytest.mark.parametrize("n", [1, 2, 8, 12, 64, 97, 513, 320, 384, 448, 1792, 2048])
 def test_fft_backward_forward(oracle, n):
     z = np.random.default_rng(n).random(n) + 1j * np.random.default_rng(n + 1).random(n)
     np.testing.assert_allclose(oracle.fft1d(z, -1), np.fft.fft(z), rtol=1e-12, atol=1e-11)
