@@ -17,7 +17,8 @@ with every DFT on the CUDA cores in FP32 (fp32_path) and the plain GPU path
 
 N > 1: one process per GPU (torchrun), independent replicas (the path does
 not shard across GPUs), weak scaling.  --impl reference times the CPU
-restatement of the same path on the host cores (tile sample).
+restatement of the same path (the oracle, C FP64 with OpenMP) on the host
+cores: per step the whole 513^3 field on the same padded grid.
 """
 import argparse
 import datetime
@@ -204,45 +205,55 @@ def pass_bytes(lay, P, dtype_bytes=4):
     return {"k_gen_z": b1, "k_gen_z_tc": b1, "k_mid_y": b2, "k_c2r_x": b3}
 
 
-def cpu_sample(lay, P, steps, warmup, stride=8):
-    """The oracle (CPU restatement, OpenMP) on every stride-th line of each
-    pass of tile 0 on padded grid P: per step, 1/stride of one tile's work."""
+def oracle_layout():
+    """Layout and SMOOTH padded grid of the headline deck from the oracle's
+    restatements (no product code)."""
     from oracle import oracle as O
-    Np = [int(v) for v in lay["Np"]]
-    dx = [float(v) for v in lay["xStep"]]
-    norm = O.spectrum_sum(DECK["corrMod"], DECK["nu"], P, dx, DECK["corrL"])
-    out = __import__("numpy").zeros(Np, order="F")
+    d = DECK
+    lay = O.sample_layout(d["xMinGlob"], d["xMaxGlob"], d["corrL"], d["overlap"], d["pointsPerCorrL"],
+                          1, 8, TOPO)
+    P = O.pad_size(3, d["corrMod"], d["corrL"], lay["xStep"], lay["Np"], PAD_TOL)
+    return lay, [int(v) for v in P]
+
+
+def cpu_field(lay, P, steps, warmup, seedBase=0):
+    """The oracle (C, FP64, OpenMP) on the whole headline field: per step the
+    8 tiles on padded grid P, the PoU weights, the overlap sums, the lognormal
+    marginal and the assembly of the 513^3 field (so_generate_sample).
+    Returns the baseline record, seconds per field and the last field."""
+    from oracle import oracle as O
+    d = DECK
+
+    def one():
+        return O.generate_sample(3, d["xMinGlob"], d["xMaxGlob"], d["corrL"], d["overlap"],
+                                 d["pointsPerCorrL"], d["corrMod"], d["nu"], d["margiFirst"],
+                                 d["avg"], d["std_dev"], seedBase, 8, TOPO, P)[0]
+    g = None
     for _ in range(warmup):
-        O.gen_padded_stream(Np, P, dx, DECK["corrL"], DECK["corrMod"], DECK["nu"], norm, 1, 0,
-                            stride, out)
+        g = one()
     t0 = time.perf_counter()
     for _ in range(steps):
-        O.gen_padded_stream(Np, P, dx, DECK["corrL"], DECK["corrMod"], DECK["nu"], norm, 1, 0,
-                            stride, out)
-    dt = (time.perf_counter() - t0) / steps
-    nb = int(lay["nb_tiles"])
-    field_points = int(lay["L"][0]) * int(lay["L"][1]) * int(lay["L"][2])
-    # one tile accounts for field_points / nb points; the sample is 1/stride tile
-    mpts = (field_points / nb) / (dt * stride) / 1e6
+        g = one()
+    dt = (time.perf_counter() - t0) / max(steps, 1)
+    npts = int(lay["L"][0]) * int(lay["L"][1]) * int(lay["L"][2])
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": round(mpts, 4), "unit": "Mpoints/s", "cores": cores, "kind": "port",
-            "sample": f"oracle (C, FP64, OpenMP, radix-2 FFT) on every {stride}th line of the three "
-                      f"passes of tile 0 of {nb} on the power-of-two padded grid {list(P)}; "
-                      f"{dt:.3f} s per sample, scaled x{stride} to one tile and by 1/{nb} of the "
-                      f"{field_points}-point field"}, dt
+    return {"value": round(npts / dt / 1e6, 4), "unit": "Mpoints/s", "cores": cores, "kind": "port",
+            "sample": f"oracle (C, FP64, OpenMP, mixed-radix FFT) on the whole {npts}-point field: "
+                      f"{int(lay['topo'][0] * lay['topo'][1] * lay['topo'][2])} tiles on the padded "
+                      f"grid {list(P)}, PoU, overlap sums, lognormal marginal, assembly; "
+                      f"{dt:.2f} s per field"}, dt, g
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
-    import scarl_b200 as S
-    _, lay = layout_of(S)
-    base, dt = cpu_sample(lay, pads(S, lay, S.PAD_AUTO), args.steps, args.warmup)
+    lay, P = oracle_layout()
+    base, dt, _ = cpu_field(lay, P, args.steps, args.warmup)
     line = {"metric": METRIC, "value": base["value"], "unit": "Mpoints/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": config_of(lay, pads(S, lay, S.PAD_SMOOTH)),
+            "config": config_of(lay, P),
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "Mpoints/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -710,9 +721,21 @@ def main():
     if rank == 0 and not args.no_learned:
         learned = bench_learned(S, ctx)
 
+    # ---- the CPU baseline: the oracle on the same field (seed, grid), whose
+    #      FP64 output is also the reference of the headline's error
     cpu = None
+    rel_o = relmax_o = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu, _ = cpu_sample(lay, P_pow2, 1, 0)
+        olay, P_o = oracle_layout()
+        assert P_o == P_auto, (P_o, P_auto)
+        cpu, _, g = cpu_field(olay, P_o, 1, 0, seedBase=int(sample.seedBase))
+        step()
+        torch.cuda.synchronize()
+        ref = torch.from_numpy(g.reshape(-1, order="F")).to("cuda")
+        dlt = field.double() - ref
+        rel_o = float(torch.linalg.vector_norm(dlt) / torch.linalg.vector_norm(ref))
+        relmax_o = float(dlt.abs().max() / ref.abs().max())
+        del ref, dlt, g
 
     if dist is not None:
         dist.barrier()
@@ -722,10 +745,17 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 (z DFT: bf16 head/tail products, f32 accumulation)",
                 "data": "synthetic (Philox normals, seeded per rank)",
-                "config": config_of(lay, P_auto), "rel_l2_vs_fp64": rel, "max_err_vs_fp64": relmax,
+                "config": config_of(lay, P_auto),
+                "rel_l2_vs_fp64": rel_o if rel_o is not None else rel,
+                "max_err_vs_fp64": relmax_o if relmax_o is not None else relmax,
+                "rel_l2_reference": ("the oracle's FP64 field (C, same seed and grid)" if rel_o is not None
+                                     else "the GPU FP64 path (same seed and grid)"),
+                "rel_l2_vs_gpu_fp64": rel, "max_err_vs_gpu_fp64": relmax,
                 "roofline": roof, "tensor_stages": tensor, "kernels": kern, "launch_variants": tuned, "plain_path": plain,
                 "fp32_path": fp32, "fp64_path": fp64, "pow2_grid_path": pow2,
                 "speedup_vs_plain_path": round(ms_full / ms, 3),
+                "split_vs_fp32_same_grid": round(ms_f32 / ms, 3),
+                "padding_policy_gain_fp32": round(ms_full / ms_f32, 3),
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
                 "ensemble": ens, "large_field": large, "learned_padding": learned}
         print(json.dumps(line), flush=True)

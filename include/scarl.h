@@ -269,10 +269,15 @@ int scarl_gen_padded(scarl_ctx* ctx, void* out, int dtype, const int Np[3], cons
  * process exits; requests whose intermediate and tables do not fit (the
  * intermediate is round_up(P0/2+1, 16) * P1 * Np[2] complex values: about
  * 8.3 M in FP32, 4.1 M in FP64, e.g. a 256^3 padded grid with Np[2] <= 225 in
- * FP32) return SCARL_EINVAL with the needed size in msg.
- * out must be device memory of the current GPU; work is enqueued on
- * cuda_stream (NULL = the legacy default stream).  The first call on a
- * device looks up the array's address: make it before any stream capture.
+ * FP32) return SCARL_EINVAL with the needed size in msg.  Padded lengths and
+ * their default are those of scarl_gen_padded (SCARL_EUNSUPPORTED outside
+ * them); dtype SCARL_F32 or SCARL_F64.
+ * out must be device memory of the current GPU (a pointer to another GPU's
+ * memory returns SCARL_EINVAL); work is enqueued on cuda_stream (NULL = the
+ * legacy default stream).  The first call on a device looks up the array's
+ * address: make it before any stream capture.  Every call uploads its
+ * tables from host memory; with normalise = 1 the host also waits for the
+ * FP64 spectral sum on cuda_stream before the passes are enqueued.
  * Calls share the array: calls whose GPU work may overlap race and must be
  * serialised.  Output equals scarl_gen_padded with xi = NULL. */
 int scarl_gen_padded_noalloc(void* out, int dtype, const int Np[3], const int pad[3],

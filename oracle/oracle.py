@@ -451,3 +451,50 @@ def axis_cov(f, maxlag):
     m = C.c_double()
     lib().so_axis_cov(f.ctypes.data_as(_d), pL, int(maxlag), C.byref(m), _dp(cov))
     return m.value, cov.reshape(3, maxlag + 1)
+
+
+# ---------------- padded grid policies ----------------
+def _axis_correlation(corrMod, l, r):
+    if r <= 0.0:
+        return 1.0
+    if corrMod == 1:
+        return float(np.exp(-np.pi * r * r / (l * l)))
+    if corrMod == 3:
+        return float(np.exp(-2.0 * r / l))
+    raise ValueError("closed-form axis correlation only for the Gaussian and exponential models")
+
+
+def fft_length_supported(n):
+    """Powers of two and 3, 5, 7 times a power of two >= 16, from 8 to 2048."""
+    if n < 8 or n > 2048:
+        return False
+    m = n
+    while m % 2 == 0:
+        m //= 2
+    return m == 1 or (m in (3, 5, 7) and n // m >= 16)
+
+
+def pad_size(policy, corrMod, corrL, xStep, Np, tol=1e-3):
+    """Padded grid per axis.  policy 0: 2^ceil(log2 2 Np) (SRC_F/fftw_ScaRL.f90:194);
+    1: smallest power of two P >= Np with C((P - Np + 1) dx) <= tol; 3: the
+    same rule over every supported length.  Gaussian and exponential models."""
+    P = []
+    for d in range(3):
+        n, l, dx = int(Np[d]), float(corrL[d]), float(xStep[d])
+        p = 8
+        if policy == 0:
+            while p < 2 * n:
+                p <<= 1
+        elif policy == 1:
+            while p < n or _axis_correlation(corrMod, l, (p - n + 1) * dx) > tol:
+                p <<= 1
+        elif policy == 3:
+            p = max(n, 8)
+            while not fft_length_supported(p) or _axis_correlation(corrMod, l, (p - n + 1) * dx) > tol:
+                p += 1
+                if p > 2048:
+                    raise ValueError("beyond the largest supported length")
+        else:
+            raise ValueError("unknown padding policy")
+        P.append(p)
+    return P

@@ -15,7 +15,10 @@
 // The array's device address is looked up once per device (the first call
 // made with that device current), so make that first call before any CUDA
 // stream capture.  The call itself allocates nothing: no cudaMalloc,
-// cudaFree or allocating library routine.
+// cudaFree or allocating library routine.  Each call uploads its spectrum
+// and twiddle tables from host memory with cudaMemcpyAsync, and with
+// normalise = 1 it also waits on the stream for the FP64 spectral sum (the
+// host blocks until the GPU has reached that point).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -25,6 +28,7 @@
 #include <vector>
 
 #include "../../include/scarl.h"
+#include "host_maps.h"
 #include "scarl_internal.h"
 
 namespace {
@@ -66,17 +70,23 @@ extern "C" int scarl_gen_padded_noalloc(void* out, int dtype, const int Np[3], c
   for (int d = 0; d < 3; ++d) {
     if (Np[d] < 1 || !(xStep[d] > 0.0) || !(corrL[d] > 0.0))
       return say(msg, msg_len, SCARL_EINVAL, "Np >= 1, xStep > 0 and corrL > 0 required");
-    int p = 8;
+    int p = 1;  // default: 2^ceil(log2(2 Np)), as scarl_gen_padded
     while (p < 2 * Np[d]) p <<= 1;
     P[d] = (pad && pad[d] > 0) ? pad[d] : p;
-    if (P[d] < 8 || P[d] > 2048 || (P[d] & (P[d] - 1)) || P[d] < Np[d])
-      return say(msg, msg_len, SCARL_EINVAL,
-                 "padded grid must be a power of two in [8, 2048] and >= Np");
+    if (!fft_length_supported(P[d]))
+      return say(msg, msg_len, SCARL_EUNSUPPORTED,
+                 "padded grid lengths must lie in [8, 2048] and be a power of two or 3, 5 or 7 "
+                 "times a power of two >= 16");
+    if (P[d] < Np[d]) return say(msg, msg_len, SCARL_EINVAL, "padded grid smaller than the tile");
   }
   const cudaStream_t s = (cudaStream_t)cuda_stream;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    return say(msg, msg_len, SCARL_EDEVICE, "no usable current CUDA device");
   cudaPointerAttributes pa;
   if (cudaPointerGetAttributes(&pa, out) != cudaSuccess ||
-      (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged)) {
+      (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) ||
+      (pa.type == cudaMemoryTypeDevice && pa.device != dev)) {
     cudaGetLastError();
     return say(msg, msg_len, SCARL_EINVAL, "out must be device memory of the current GPU");
   }
@@ -108,9 +118,6 @@ extern "C" int scarl_gen_padded_noalloc(void* out, int dtype, const int Np[3], c
   }
 
   // ---- the array's address on this device (looked up once per device) ----
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-    return say(msg, msg_len, SCARL_EDEVICE, "no usable current CUDA device");
   unsigned char* base = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);

@@ -227,3 +227,23 @@ def test_streaming_generator_matches(oracle):
     a = oracle.gen_padded(*args, 1, seed=4, stream=2)
     b = oracle.gen_padded_stream(*args, seed=4, stream=2)
     np.testing.assert_array_equal(a, b)
+
+
+def test_pad_size_restatement_matches_library(oracle):
+    """The oracle's padded-grid rule (used by the CPU reference arm) equals the
+    library's host rule on random tiles (Gaussian and exponential models)."""
+    import scarl_b200 as S
+    rng = np.random.default_rng(11)
+    for _ in range(200):
+        cm = int(rng.choice([1, 3]))
+        Np = rng.integers(5, 700, 3)
+        cl = rng.uniform(1.0, 60.0, 3)
+        dx = rng.uniform(0.25, 2.0, 3)
+        for policy in (S.PAD_FULL, S.PAD_AUTO, S.PAD_SMOOTH):
+            try:
+                ref = [int(v) for v in S.pad_size(policy, cm, cl, dx, Np, 0.5, 1e-3)]
+            except S.ScarlError:
+                with pytest.raises(ValueError):
+                    oracle.pad_size(policy, cm, cl, dx, Np, 1e-3)
+                continue
+            assert oracle.pad_size(policy, cm, cl, dx, Np, 1e-3) == ref
