@@ -4,7 +4,8 @@ Field: the 512^3 deck re-fitted to 513^3, exponential correlation
 C(r) = exp(-2 |r|_l) with |r|_l = sqrt(sum (r_d / l_d)^2), l = (40, 20, 10) at
 spacing 1, lognormal marginal with mean 1 and CV 0.3, 2 x 2 x 2 tiles with
 overlap 2 l, split-BF16 path, on the SMOOTH (448 x 384 x 320) and AUTO (512^3)
-padded grids; K = 32 realisations (deck seeds 100..131).
+padded grids; K = 32 realisations (deck seeds 1000 i, i < 32: tile r of a
+sample draws with key seedBase + 1 + r, so no two realisations share a tile).
 
 Checked (estimators of SRC_F/Stat_ScaRL/statistics_RF.f90:18-174 (moments)
 and the axis covariance of :258-486 as direct FP64 lag sums):
@@ -110,7 +111,7 @@ def test_headline_field_statistics(ctx, policy, P):
     cov = [np.zeros(h + 1) for h in H]
     for i in range(K):
         s = S.make_sample((0, 0, 0), (512, 512, 512), CL, (2, 2, 2), (41, 21, 11), corrMod=3,
-                          margiFirst=2, avg=MEAN, std_dev=CV * MEAN, seedBase=100 + i)
+                          margiFirst=2, avg=MEAN, std_dev=CV * MEAN, seedBase=1000 * i)
         S.generate_sample(ctx, s, dtype=SPLIT, nb_procs=8, topo=(2, 2, 2), pad_policy=policy, out=y)
         ctx.sync()
         yd = y.double()
@@ -118,6 +119,8 @@ def test_headline_field_statistics(ctx, policy, P):
         yvar.append(float(yd.var(unbiased=False)))
         x = (torch.log(yd) - mug) / sg
         del yd
+        # x is written on torch's stream, read on the library's own stream
+        torch.cuda.synchronize()
         m, _, c = S.axis_cov(ctx, x, L, max(H), known_mean=0.0)
         xmean.append(m)
         for d in range(3):
