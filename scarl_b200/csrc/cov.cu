@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
 #pragma unroll
       for (int r = 0; r < RL; ++r) sm[b * (N + 1) + j + r * (N / RL)] = o[r];
     };
-    line_ifft<C, N, E, O, B, LS, true>(sm, b, t, tw, 2, load, store);
+    line_ifft<C, N, E, O, B, LS, true, 2>(sm, b, t, tw, load, store);
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < QB; ++q) {

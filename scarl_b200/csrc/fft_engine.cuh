@@ -185,36 +185,64 @@ template <SmemOrder O, int B, int LS, int SK> __device__ __forceinline__ int sid
   const int p = n + n / SK;
   return O == SmemOrder::BatchFast ? p * B + b : b * LS + p;
 }
+// Slot distance of one step of p along the layout (B lines apart in
+// BatchFast order, adjacent in LineFast order).
+template <SmemOrder O, int B> __host__ __device__ constexpr int sstep() {
+  return O == SmemOrder::BatchFast ? B : 1;
+}
+// Where m is a multiple of SK, p(n + m) = p(n) + m + m / SK: a thread's
+// accesses at n0 + c (c a compile-time multiple of SK) are one base address
+// plus compile-time offsets (immediate offsets of the shared-memory loads).
+template <int SK> __host__ __device__ constexpr int skew_span(int m) { return m + m / SK; }
 
 // One Stockham stage reading/writing shared memory (middle stages).
-// tw: e^{+2 pi i m / (N * twmul)} table, so w_{Ns R}^{q} = tw[q * (N / (Ns R)) * twmul];
+// tw: e^{+2 pi i m / (N * TWMUL)} table, so w_{Ns R}^{q} = tw[q * (N / (Ns R)) * TWMUL];
 // it may live in global or shared memory (plain loads, no read-only-cache path).
-template <typename C, int N, int E, int R, int Ns, SmemOrder O, int B, int LS, int SK>
+template <typename C, int N, int E, int R, int Ns, SmemOrder O, int B, int LS, int SK, int TWMUL>
 __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, int t,
-                                                    const C* __restrict__ tw, int twmul) {
+                                                    const C* __restrict__ tw) {
   constexpr int TPL = N / E;
   constexpr int NB = E / R;  // butterflies per thread
+  constexpr int ST = sstep<O, B>();
   C v[E];
+  if constexpr ((N / R) % SK == 0 && TPL % SK == 0) {
+    // reads at j + r N/R, j = t + TPL q: base of t plus constant offsets
+    const int a0 = sidx<O, B, LS, SK>(t, b);
 #pragma unroll
-  for (int q = 0; q < NB; ++q) {
-    const int j = t + TPL * q;
+    for (int q = 0; q < NB; ++q)
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[q * R + r] = sm[sidx<O, B, LS, SK>(j + r * (N / R), b)];
+      for (int r = 0; r < R; ++r)
+        v[q * R + r] = sm[a0 + (skew_span<SK>(TPL * q) + skew_span<SK>(r * (N / R))) * ST];
+  } else {
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+      const int j = t + TPL * q;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q * R + r] = sm[sidx<O, B, LS, SK>(j + r * (N / R), b)];
+    }
   }
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < NB; ++q) {
     const int j = t + TPL * q;
     const int k = j % Ns;
+    const int tk = k * ((N / (Ns * R)) * TWMUL);
 #pragma unroll
     for (int r = 1; r < R; ++r) {
-      const C w = tw[(size_t)(r * k) * (N / (Ns * R)) * twmul];  // global or shared table
+      const C w = tw[r * tk];  // global or shared table
       v[q * R + r] = cmul(v[q * R + r], w);
     }
     dft_reg<R>(v + q * R);
     const int base = (j / Ns) * Ns * R + k;
+    if constexpr (Ns % SK == 0) {
+      // writes at base + r Ns
+      const int a0 = sidx<O, B, LS, SK>(base, b);
 #pragma unroll
-    for (int r = 0; r < R; ++r) sm[sidx<O, B, LS, SK>(base + r * Ns, b)] = v[q * R + operm<R>(r)];
+      for (int r = 0; r < R; ++r) sm[a0 + skew_span<SK>(r * Ns) * ST] = v[q * R + operm<R>(r)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) sm[sidx<O, B, LS, SK>(base + r * Ns, b)] = v[q * R + operm<R>(r)];
+    }
   }
   __syncthreads();
 }
@@ -227,9 +255,9 @@ __device__ __forceinline__ void stockham_smem_stage(C* __restrict__ sm, int b, i
 // threads of the block must call.  With SYNC_STORE every thread has finished
 // its shared-memory reads before the first store, so store may write sm.
 template <typename C, int N, int E, SmemOrder O, int B, int LS, bool SYNC_STORE = false,
-          class Load, class Store>
+          int TWMUL = 1, class Load, class Store>
 __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, const C* __restrict__ tw,
-                                          int twmul, Load&& load, Store&& store) {
+                                          Load&& load, Store&& store) {
   using P = StagePlan<N, E>;
   constexpr int TPL = N / E;
   constexpr int R1 = P::radix(0);
@@ -254,39 +282,53 @@ __device__ __forceinline__ void line_ifft(C* __restrict__ sm, int b, int t, cons
 #pragma unroll
     for (int q = 0; q < NB1; ++q) dft_reg<R1>(v + q * R1);
     __syncthreads();  // the loader may have read shared memory
+    constexpr int ST = sstep<O, B>();
+    {
+      // output j R1 + r of the first stage (r < R1 = SK) sits at slot p = j (R1 + 1) + r
+      const int a0 = sidx<O, B, LS, SK>(t * R1, b);
 #pragma unroll
-    for (int q = 0; q < NB1; ++q) {
-      const int j = t + TPL * q;
+      for (int q = 0; q < NB1; ++q)
 #pragma unroll
-      for (int r = 0; r < R1; ++r) sm[sidx<O, B, LS, SK>(j * R1 + r, b)] = v[q * R1 + operm<R1>(r)];
+        for (int r = 0; r < R1; ++r)
+          sm[a0 + (TPL * q * (R1 + 1) + r) * ST] = v[q * R1 + operm<R1>(r)];
     }
     __syncthreads();
     if constexpr (P::S >= 3)
-      stockham_smem_stage<C, N, E, P::radix(1), R1, O, B, LS, SK>(sm, b, t, tw, twmul);
+      stockham_smem_stage<C, N, E, P::radix(1), R1, O, B, LS, SK, TWMUL>(sm, b, t, tw);
     if constexpr (P::S >= 4)
-      stockham_smem_stage<C, N, E, P::radix(2), R1 * P::radix(1), O, B, LS, SK>(sm, b, t, tw, twmul);
+      stockham_smem_stage<C, N, E, P::radix(2), R1 * P::radix(1), O, B, LS, SK, TWMUL>(sm, b, t, tw);
     if constexpr (P::S >= 5)
-      stockham_smem_stage<C, N, E, P::radix(3), R1 * P::radix(1) * P::radix(2), O, B, LS, SK>(
-          sm, b, t, tw, twmul);
+      stockham_smem_stage<C, N, E, P::radix(3), R1 * P::radix(1) * P::radix(2), O, B, LS, SK, TWMUL>(
+          sm, b, t, tw);
     static_assert(P::S <= 5, "line length too long for the register budget");
     // last stage
     constexpr int RL = P::radix(P::S - 1);
     constexpr int NsL = N / RL;
     constexpr int NBL = E / RL;
+    if constexpr ((N / RL) % SK == 0 && TPL % SK == 0) {
+      const int a0 = sidx<O, B, LS, SK>(t, b);
 #pragma unroll
-    for (int q = 0; q < NBL; ++q) {
-      const int j = t + TPL * q;
+      for (int q = 0; q < NBL; ++q)
 #pragma unroll
-      for (int r = 0; r < RL; ++r) v[q * RL + r] = sm[sidx<O, B, LS, SK>(j + r * (N / RL), b)];
+        for (int r = 0; r < RL; ++r)
+          v[q * RL + r] = sm[a0 + (skew_span<SK>(TPL * q) + skew_span<SK>(r * (N / RL))) * ST];
+    } else {
+#pragma unroll
+      for (int q = 0; q < NBL; ++q) {
+        const int j = t + TPL * q;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) v[q * RL + r] = sm[sidx<O, B, LS, SK>(j + r * (N / RL), b)];
+      }
     }
     if constexpr (SYNC_STORE) __syncthreads();
 #pragma unroll
     for (int q = 0; q < NBL; ++q) {
       const int j = t + TPL * q;
       const int k = j % NsL;
+      const int tk = k * TWMUL;
 #pragma unroll
       for (int r = 1; r < RL; ++r) {
-        const C w = tw[(size_t)(r * k) * twmul];
+        const C w = tw[r * tk];
         v[q * RL + r] = cmul(v[q * RL + r], w);
       }
       dft_reg<RL>(v + q * RL);

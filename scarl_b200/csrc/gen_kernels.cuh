@@ -135,15 +135,18 @@ __device__ __forceinline__ void gen_z_body(const GenArgs& a, int bx, int ky) {
   };
   const int Nz = a.Nout[2];
   constexpr int RL = last_radix<N, E>();
+  const size_t zstride = (size_t)a.P[1] * a.Hpad;
+  C* wcol = work + (size_t)ky * a.Hpad + kx;
   auto store = [&](int j, const C* o) {
+    C* wj = wcol + (size_t)j * zstride;
 #pragma unroll
     for (int r = 0; r < RL; ++r) {
       const int z = j + r * (N / RL);
-      if (valid && z < Nz) work[((size_t)z * a.P[1] + ky) * a.Hpad + kx] = o[r];
+      if (valid && z < Nz) wj[(size_t)(r * (N / RL)) * zstride] = o[r];
     }
   };
-  line_ifft<C, N, E, SmemOrder::BatchFast, B, 0>(sm, b, t, static_cast<const C*>(a.tw_z), 1, load,
-                                                 store);
+  line_ifft<C, N, E, SmemOrder::BatchFast, B, 0, false, 1>(sm, b, t, static_cast<const C*>(a.tw_z),
+                                                          load, store);
 }
 
 // ---------------------------------------------------------------------------
@@ -175,14 +178,15 @@ __device__ __forceinline__ void mid_y_body(const GenArgs& a, int bx, int z) {
   constexpr int RL = last_radix<N, E>();
   C* col = colblk + b;
   auto store = [&](int j, const C* o) {
+    C* cj = col + (size_t)j * pitch;
 #pragma unroll
     for (int r = 0; r < RL; ++r) {
       const int y = j + r * (N / RL);
-      if (valid && y < Ny) col[(size_t)y * pitch] = o[r];
+      if (valid && y < Ny) cj[(size_t)(r * (N / RL)) * pitch] = o[r];
     }
   };
-  line_ifft<C, N, E, SmemOrder::BatchFast, B, 0>(sm, b, t, static_cast<const C*>(a.tw_y), 1, load,
-                                                 store);
+  line_ifft<C, N, E, SmemOrder::BatchFast, B, 0, false, 1>(sm, b, t, static_cast<const C*>(a.tw_y),
+                                                          load, store);
 }
 
 // ---------------------------------------------------------------------------
@@ -265,7 +269,7 @@ __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
     }
     ep.template put_group<2 * RL>(xs, v, Nx);
   };
-  line_ifft<C, N, E, SmemOrder::LineFast, B, LS>(sm, b, t, tws, 2, load, store);
+  line_ifft<C, N, E, SmemOrder::LineFast, B, LS, false, 2>(sm, b, t, tws, load, store);
 }
 
 // ---------------------------------------------------------------------------
