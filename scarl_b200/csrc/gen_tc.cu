@@ -29,7 +29,6 @@
 // consecutive kx.  Every wait on the tensor core is bounded; on timeout the
 // kernel raises a status word and returns after freeing its tensor memory.
 #include <algorithm>
-#include <cstdlib>
 
 #include "gen_kernels.cuh"
 #include "tc_sm100.cuh"
@@ -403,372 +402,6 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
   if (warp == 0) tc::tmem_free(tmem, Cfg::TMEM_COLS);
 }
 
-// ---------------------------------------------------------------------------
-// Warp-specialised form: one CTA per SM, two thread groups that overlap.
-//   synthesis group (SYN = LB N1 threads, warps 0 .. SYN/32 - 1): per item
-//     builds its stage-1 row in registers, waits until the previous item's
-//     stage-1 MMAs have read the operand buffer, stores the row, and its
-//     leader issues the stage-1 MMAs into tensor-memory region k & 1;
-//   epilogue group (128 threads, the next four warps, one per lane quarter):
-//     per item drains stage 1 (twiddle, split, stage-2 operand), issues the
-//     stage-2 MMAs into the same region, drains them through shared memory
-//     to global memory and frees the region.
-// So item k + 1's synthesis runs while item k's MMAs and epilogue run.  The
-// arithmetic per element is that of gen_z_tc_body (identical outputs).
-// mbarriers: m1(r) (stage 1 into region r done), m2 (stage 2 done),
-// rfree(r) (region r drained); every wait is bounded as in gen_z_tc_body.
-template <int N1_, int N2_, int LB_, int NCH_>
-struct TcWsCfg : TcCfg<N1_, N2_, LB_, NCH_> {
-  using B = TcCfg<N1_, N2_, LB_, NCH_>;
-  static constexpr int SYN = B::ROWS1, EPI = 128, THREADS = SYN + EPI;
-  static constexpr int NC = B::K1 / 8;  // 16-byte K chunks of a stage-1 row
-  static constexpr int REG2 = (2 * B::A2B > B::STAGEB ? 2 * B::A2B : B::STAGEB);
-  static constexpr int OFF_A1H = 0, OFF_A1L = B::A1B, OFF_A2H = 2 * B::A1B, OFF_A2L = OFF_A2H + B::A2B;
-  static constexpr int OFF_B1H = OFF_A2H + REG2, OFF_B1L = OFF_B1H + B::B1B;
-  static constexpr int OFF_B2H = OFF_B1L + B::B1B, OFF_B2L = OFF_B2H + B::B2B;
-  static constexpr int OFF_ZT = OFF_B2L + B::B2B;
-  static constexpr int OFF_TW = OFF_ZT + 4 * B::N;
-  static constexpr int OFF_BAR = OFF_TW + 8 * B::N;  // m1 x2, m2, rfree x2 (8 B each), tmem slot
-  static constexpr int SMEM = OFF_BAR + 64;
-  static constexpr int REGION = 256;  // tensor-memory columns per region (two regions)
-  static_assert(SYN == 256 && B::TMEM_USED <= REGION, "one stage-1 row per synthesis thread");
-  static_assert(SMEM + 2 * (int)sizeof(GenArgs) + 1024 <= 227 * 1024, "shared memory");
-};
-
-template <int N1, int N2, int LB, int NCH, int AMP, bool BATCH>
-__device__ __forceinline__ void gen_z_tc_ws_body(const GenArgs& a0, const GenArgs* __restrict__ bargs,
-                                                 const int* __restrict__ bitems,
-                                                 const int* __restrict__ bstart, int bn, int btotal) {
-  using Cfg = TcWsCfg<N1, N2, LB, NCH>;
-  constexpr int N = Cfg::N;
-  extern __shared__ __align__(128) unsigned char sm[];
-  __shared__ GenArgs sa_syn, sa_epi;  // batch: the current realisation of each group
-  unsigned char* A1H = sm + Cfg::OFF_A1H;
-  unsigned char* A1L = sm + Cfg::OFF_A1L;
-  unsigned char* A2H = sm + Cfg::OFF_A2H;
-  unsigned char* A2L = sm + Cfg::OFF_A2L;
-  const uint32_t sA1H = tc::smem_u32(A1H), sA1L = tc::smem_u32(A1L);
-  const uint32_t sA2H = tc::smem_u32(A2H), sA2L = tc::smem_u32(A2L);
-  const uint32_t sB1H = tc::smem_u32(sm + Cfg::OFF_B1H), sB1L = tc::smem_u32(sm + Cfg::OFF_B1L);
-  const uint32_t sB2H = tc::smem_u32(sm + Cfg::OFF_B2H), sB2L = tc::smem_u32(sm + Cfg::OFF_B2L);
-  const uint32_t bar0 = tc::smem_u32(sm + Cfg::OFF_BAR);
-  auto m1 = [bar0](int r) -> uint32_t { return bar0 + 8u * (uint32_t)r; };          // r = 0, 1
-  const uint32_t m2 = bar0 + 16;
-  auto rfree = [bar0](int r) -> uint32_t { return bar0 + 24u + 8u * (uint32_t)r; };  // r = 0, 1
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + Cfg::OFF_BAR + 40);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-  if (tid == 0) {
-    tc::mbar_init(m1(0), 1);
-    tc::mbar_init(m1(1), 1);
-    tc::mbar_init(m2, 1);
-    tc::mbar_init(rfree(0), 1);
-    tc::mbar_init(rfree(1), 1);
-  }
-  if (warp == 0) tc::tmem_alloc(tc::smem_u32(tslot), 2 * Cfg::REGION);
-  fill_dft_b<N2, Cfg::SBO1, true>(sm + Cfg::OFF_B1H, sm + Cfg::OFF_B1L);
-  fill_dft_b<N1, Cfg::SBO2, false>(sm + Cfg::OFF_B2H, sm + Cfg::OFF_B2L);
-  float* zt = reinterpret_cast<float*>(sm + Cfg::OFF_ZT);
-  float2* tw2 = reinterpret_cast<float2*>(sm + Cfg::OFF_TW);
-  {
-    const float2* tw = static_cast<const float2*>(a0.tw_z);  // e^{2 pi i m / N}
-    for (int i = tid; i < N; i += Cfg::THREADS) tw2[i] = tw[(i / N1) * (i % N1)];  // [n2][k1]
-    if (!BATCH) {
-      const float* zsrc = static_cast<const float*>(AMP == AMP_SEPARABLE ? a0.az : a0.qz);
-      for (int i = tid; i < N; i += Cfg::THREADS) zt[i] = zsrc[i];
-    }
-  }
-  tc::fence_smem_to_async();
-  tc::fence_before_sync();
-  __syncthreads();
-  tc::fence_after_sync();
-  const uint32_t tmem = *tslot;
-
-  constexpr uint32_t ID1 = tc::idesc_bf16(128, Cfg::K1, false);
-  constexpr uint32_t ID2 = tc::idesc_bf16(128, Cfg::K2, true);  // A MN-major
-  const bool wait_test = a0.wait_test != 0;
-  const uint64_t wait_ns = wait_test ? 20000000ull : kWaitNs;
-  const int nitems0 = BATCH ? btotal : (a0.Hx * a0.P[1] + LB - 1) / LB;
-  bool ok = true;
-  int m1_last = -1, m2_last = -1;  // last item whose stage-1 / stage-2 MMAs the leader committed
-
-  // item -> (realisation, local item); the group's argument copy reloaded
-  // when the realisation changes (id / cnt: the group's named barrier)
-  auto locate = [&](int gitem, GenArgs& sa, int& cur, uint32_t id, uint32_t cnt, int gtid,
-                    bool with_zt) -> int {
-    if constexpr (!BATCH) {
-      return gitem;
-    } else {
-      int lo = 0, hi = bn;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(bstart + mid) <= gitem) lo = mid;
-        else hi = mid;
-      }
-      const int r = __ldg(bitems + lo);
-      if (r != cur) {  // uniform over the group: every thread walks the same items
-        tc::group_sync(id, cnt);
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(bargs + r);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
-        for (int i = gtid; i < (int)(sizeof(GenArgs) / 4); i += cnt) dst[i] = __ldg(src + i);
-        tc::group_sync(id, cnt);
-        if (with_zt) {
-          const float* zsrc = static_cast<const float*>(AMP == AMP_SEPARABLE ? sa.az : sa.qz);
-          for (int i = gtid; i < N; i += cnt) zt[i] = zsrc[i];
-          tc::group_sync(id, cnt);
-        }
-        cur = r;
-      }
-      return gitem - __ldg(bstart + lo);
-    }
-  };
-
-  if (tid < Cfg::SYN) {
-    // ================= synthesis group =================
-    const int R1 = tid;
-    const int s_line = (R1 >> 3) % LB, s_k1 = (R1 & 7) + 8 * (R1 / (8 * LB));
-    const uint32_t rowoff = (uint32_t)((R1 >> 3) * Cfg::SBO1 + (R1 & 7) * 16);
-    int cur = -1;
-    int k = 0;
-    for (int gitem = blockIdx.x; gitem < nitems0; gitem += gridDim.x, ++k) {
-      const int item = locate(gitem, sa_syn, cur, 1, Cfg::SYN, tid, true);
-      const GenArgs& a = BATCH ? sa_syn : a0;
-      const int nlines = a.Hx * a.P[1];
-      const uint64_t mz = (uint64_t)a.Hx * (uint64_t)a.P[1];
-      const float* ax = static_cast<const float*>(a.ax);
-      const float* ay = static_cast<const float*>(a.ay);
-      const float* qx = static_cast<const float*>(a.qx);
-      const float* qy = static_cast<const float*>(a.qy);
-      const int l = item * LB + s_line;
-      const bool valid = l < nlines;
-      const int ky = valid ? l / a.Hx : 0, kx = valid ? l - ky * a.Hx : 0;
-      float fx = 0.f, fy = 0.f;
-      if (valid) {
-        if (AMP == AMP_SEPARABLE) { fx = ax[kx] * ay[ky]; }
-        else { fx = ax[kx]; fy = 1.f + qx[kx] + qy[ky]; }
-      }
-      auto amp = [&](int kz) -> float {
-        if (AMP == AMP_SEPARABLE) return fx * zt[kz];
-        if (AMP == AMP_RECIP) return __fdividef(fx, fy + zt[kz]);
-        return fx * powf(fy + zt[kz], (float)a.expo);
-      };
-      // the row in registers: chunk c holds K columns 8c .. 8c + 7 (draw order)
-      uint4 rh[Cfg::NC], rl[Cfg::NC];
-#pragma unroll
-      for (int d0 = 0; d0 < N2 / 2; d0 += 4) {
-        float v[16];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int kz0 = s_k1 + N1 * (d0 + e);
-          if (valid) {
-            const uint64_t c = (uint64_t)l + mz * (uint64_t)kz0;
-            const u32x4 o = philox4x32_10_ks({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.ks);
-            const float2 x0 = split_normals(o.x, o.y);
-            const float2 x1 = split_normals(o.z, o.w);
-            const float A0 = amp(kz0), A1 = amp(kz0 + N / 2);
-            v[4 * e] = A0 * x0.x;
-            v[4 * e + 1] = A0 * x0.y;
-            v[4 * e + 2] = A1 * x1.x;
-            v[4 * e + 3] = A1 * x1.y;
-          } else {
-            v[4 * e] = v[4 * e + 1] = v[4 * e + 2] = v[4 * e + 3] = 0.f;
-          }
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const float* w = v + 8 * h;
-          uint4& H = rh[d0 / 2 + h];
-          uint4& L = rl[d0 / 2 + h];
-          tc::split2(w[0], w[1], H.x, L.x);
-          tc::split2(w[2], w[3], H.y, L.y);
-          tc::split2(w[4], w[5], H.z, L.z);
-          tc::split2(w[6], w[7], H.w, L.w);
-        }
-      }
-      // the previous item's stage-1 MMAs have read the operand buffer
-      if (k >= 1) ok = tc::mbar_wait(m1((k - 1) & 1), ((k - 1) >> 1) & 1, wait_ns);
-      if (ok) {
-#pragma unroll
-        for (int c = 0; c < Cfg::NC; ++c) {
-          const uint32_t off = rowoff + c * Cfg::LBO1;
-          *reinterpret_cast<uint4*>(A1H + off) = rh[c];
-          *reinterpret_cast<uint4*>(A1L + off) = rl[c];
-        }
-      }
-      tc::fence_smem_to_async();
-      ok = tc::group_and(1, Cfg::SYN, ok);
-      if (!ok) break;
-      if (tid == 0) {
-        const int r = k & 1;
-        // region r: the epilogue has drained item k - 2
-        bool free_ok = k < 2 || tc::mbar_wait(rfree(r), ((k >> 1) - 1) & 1, wait_ns);
-        tc::fence_after_sync();
-        if (free_ok && !wait_test) {
-#pragma unroll 1
-          for (int t = 0; t < Cfg::T1; ++t) {
-#pragma unroll
-            for (int s = 0; s < Cfg::K1 / 16; ++s) {
-              const uint32_t ao = t * Cfg::TILE1 + s * 2 * Cfg::LBO1, bo = s * 2 * Cfg::LBO1;
-              const uint64_t ah = tc::desc(sA1H + ao, Cfg::LBO1, Cfg::SBO1);
-              const uint64_t al = tc::desc(sA1L + ao, Cfg::LBO1, Cfg::SBO1);
-              const uint64_t bh = tc::desc(sB1H + bo, Cfg::LBO1, Cfg::SBO1);
-              const uint64_t bl = tc::desc(sB1L + bo, Cfg::LBO1, Cfg::SBO1);
-              const uint32_t d = tmem + r * Cfg::REGION + t * Cfg::K1;
-              tc::mma_bf16(d, ah, bh, ID1, s > 0 ? 1u : 0u);
-              tc::mma_bf16(d, ah, bl, ID1, 1u);
-              tc::mma_bf16(d, al, bh, ID1, 1u);
-            }
-          }
-          tc::commit(m1(r));
-          m1_last = k;
-        }
-        // free_ok false: nothing is committed; the epilogue's wait runs out
-      }
-    }
-  } else {
-    // ================= epilogue group =================
-    const int etid = tid - Cfg::SYN;
-    const int q = (warp - Cfg::SYN / 32) & 3;  // lane quarter of tensor memory (warp % 4)
-    int cur = -1;
-    int k = 0;
-    for (int gitem = blockIdx.x; gitem < nitems0; gitem += gridDim.x, ++k) {
-      const int item = locate(gitem, sa_epi, cur, 2, Cfg::EPI, etid, false);
-      const GenArgs& a = BATCH ? sa_epi : a0;
-      const int nlines = a.Hx * a.P[1];
-      float2* work = static_cast<float2*>(a.work);
-      const int Nz = a.Nout[2];
-      const int l0 = item * LB;
-      const int r = k & 1;
-      const uint32_t treg = tmem + r * Cfg::REGION;
-      ok = tc::mbar_wait(m1(r), (k >> 1) & 1, wait_ns);
-      if (!tc::group_and(2, Cfg::EPI, ok)) { ok = false; break; }
-      tc::fence_after_sync();
-      // ---- stage-1 rows back, twiddled, split into the MN-major stage-2 operand
-#pragma unroll 1
-      for (int t = 0; t < Cfg::T1; ++t) {
-        const int R = t * 128 + q * 32 + lane;
-        const int line = (R >> 3) % LB, k1 = (R & 7) + 8 * (R / (8 * LB));
-        const float2* twk = tw2 + k1;  // e^{2 pi i n2 k1 / N} at twk[n2 N1]
-        const uint32_t base = (uint32_t)(N2 * line / 8) * Cfg::SBO2 + (k1 >> 3) * Cfg::LBO2 + (k1 & 7) * 16;
-        constexpr uint32_t IM = (N1 / 8) * Cfg::LBO2;
-        const uint32_t col = treg + ((uint32_t)(q * 32) << 16) + t * Cfg::K1;
-#pragma unroll 2
-        for (int g = 0; g < N2 / 8; ++g) {
-          float v[16];
-          tc::tmem_ld<8>(col + 8 * g, v);
-          tc::tmem_ld<8>(col + N2 + 8 * g, v + 8);
-          tc::tmem_wait_ld();
-          uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-          for (int e = 0; e < 8; e += 2) {
-            const int n2 = 8 * g + e;
-            const float2 w0 = twk[n2 * N1], w1 = twk[(n2 + 1) * N1];
-            const float yr0 = v[e] * w0.x - v[8 + e] * w0.y, yi0 = v[e] * w0.y + v[8 + e] * w0.x;
-            const float yr1 = v[e + 1] * w1.x - v[9 + e] * w1.y, yi1 = v[e + 1] * w1.y + v[9 + e] * w1.x;
-            tc::split2(yr0, yr1, rh[e / 2], rl[e / 2]);
-            tc::split2(yi0, yi1, ih[e / 2], il[e / 2]);
-          }
-          const uint32_t off = base + (uint32_t)g * Cfg::SBO2;
-          *reinterpret_cast<uint4*>(A2H + off) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-          *reinterpret_cast<uint4*>(A2L + off) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-          *reinterpret_cast<uint4*>(A2H + off + IM) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-          *reinterpret_cast<uint4*>(A2L + off + IM) = make_uint4(il[0], il[1], il[2], il[3]);
-        }
-      }
-      tc::fence_smem_to_async();
-      tc::fence_before_sync();
-      tc::group_sync(2, Cfg::EPI);
-      // ---- stage 2 on the tensor cores, into the same region
-      if (etid == 0) {
-        tc::fence_after_sync();
-#pragma unroll 1
-        for (int t = 0; t < Cfg::T2; ++t) {
-#pragma unroll
-          for (int s = 0; s < Cfg::K2 / 16; ++s) {
-            const uint32_t ao = t * Cfg::TILE2 + s * 2 * Cfg::LBO2, bo = s * 2 * Cfg::LBO1;
-            const uint64_t ah = tc::desc(sA2H + ao, Cfg::LBO2, Cfg::SBO2);
-            const uint64_t al = tc::desc(sA2L + ao, Cfg::LBO2, Cfg::SBO2);
-            const uint64_t bh = tc::desc(sB2H + bo, Cfg::LBO1, Cfg::SBO2);
-            const uint64_t bl = tc::desc(sB2L + bo, Cfg::LBO1, Cfg::SBO2);
-            const uint32_t d = treg + t * Cfg::K2;
-            tc::mma_bf16(d, ah, bh, ID2, s > 0 ? 1u : 0u);
-            tc::mma_bf16(d, ah, bl, ID2, 1u);
-            tc::mma_bf16(d, al, bh, ID2, 1u);
-          }
-        }
-        tc::commit(m2);
-        m2_last = k;
-      }
-      ok = tc::mbar_wait(m2, k & 1, wait_ns);
-      if (!tc::group_and(2, Cfg::EPI, ok)) { ok = false; break; }
-      tc::fence_after_sync();
-      // ---- results X[n2 + N2 n1] of row (line, n2) through the z-major
-      //      staging area (the stage-2 operand region, read by now)
-      float2* stage = reinterpret_cast<float2*>(A2H);
-      constexpr int CN1 = N1 / Cfg::NCH, CZ = N / Cfg::NCH;
-#pragma unroll 1
-      for (int ch = 0; ch < Cfg::NCH; ++ch) {
-        if (ch * CZ < Nz) {
-#pragma unroll 1
-          for (int t = 0; t < Cfg::T2; ++t) {
-            const int R = t * 128 + q * 32 + lane;
-            const int line = R / N2, n2 = R % N2;
-            float v[2 * CN1];
-            const uint32_t col = treg + ((uint32_t)(q * 32) << 16) + t * Cfg::K2 + ch * CN1;
-            tc::tmem_ld<CN1>(col, v);
-            tc::tmem_ld<CN1>(col + N1, v + CN1);
-            tc::tmem_wait_ld();
-#pragma unroll
-            for (int n1 = 0; n1 < CN1; ++n1)
-              stage[(n2 + N2 * n1) * Cfg::STAGE_LD + line] = make_float2(v[n1], v[CN1 + n1]);
-          }
-        }
-        tc::fence_before_sync();
-        tc::group_sync(2, Cfg::EPI);
-        if (ch == Cfg::NCH - 1 && etid == 0) tc::mbar_arrive(rfree(r));  // region drained
-        if (ch * CZ < Nz) {
-          const int line = etid % LB;
-          const int ll = l0 + line;
-          const bool valid = ll < nlines;
-          const int ky = valid ? ll / a.Hx : 0, kx = valid ? ll - ky * a.Hx : 0;
-          const size_t zstride = (size_t)a.P[1] * a.Hpad;
-          float2* dst = work + (size_t)ky * a.Hpad + kx + (size_t)(ch * CZ) * zstride;
-          const int zn = min(CZ, Nz - ch * CZ);
-          if (valid)
-#pragma unroll 4
-            for (int z = etid / LB; z < zn; z += Cfg::EPI / LB)
-              dst[(size_t)z * zstride] = stage[z * Cfg::STAGE_LD + line];
-        }
-        tc::group_sync(2, Cfg::EPI);  // the staging area: next chunk, or the next item's operand
-      }
-    }
-  }
-  // ---- teardown: after a failed wait, give the MMAs each group issued one
-  //      more bounded wait before the tensor memory they write is released
-  __syncthreads();
-  const bool all_ok = __syncthreads_and(ok);
-  if (!all_ok) {
-    if (tid == 0) {
-      atomicOr(a0.status, 1);  // the context's status word, shared by a batch
-      if (m1_last >= 0) tc::mbar_wait(m1(m1_last & 1), (m1_last >> 1) & 1, wait_ns);
-    }
-    if (tid == Cfg::SYN && m2_last >= 0) tc::mbar_wait(m2, m2_last & 1, wait_ns);
-  }
-  __syncthreads();
-  tc::fence_after_sync();
-  if (warp == 0) tc::tmem_free(tmem, 2 * Cfg::REGION);
-}
-
-template <int N1, int N2, int LB, int NCH, int AMP>
-__global__ void __launch_bounds__(TcWsCfg<N1, N2, LB, NCH>::THREADS, 1) k_gen_z_tc_ws(const GenArgs a) {
-  gen_z_tc_ws_body<N1, N2, LB, NCH, AMP, false>(a, nullptr, nullptr, nullptr, 0, 0);
-}
-template <int N1, int N2, int LB, int NCH, int AMP>
-__global__ void __launch_bounds__(TcWsCfg<N1, N2, LB, NCH>::THREADS, 1)
-    k_gen_z_tc_ws_batch(const GenArgs rep, const BatchMap m) {
-  gen_z_tc_ws_body<N1, N2, LB, NCH, AMP, true>(rep, m.args, m.items, m.start, m.n, m.total);
-}
-
 template <int N1, int N2, int LB, int NCH, int AMP>
 __global__ void __launch_bounds__(256, 2) k_gen_z_tc(const GenArgs a) {
   gen_z_tc_body<N1, N2, LB, NCH, AMP, false>(a, nullptr, nullptr, nullptr, 0, 0);
@@ -801,36 +434,12 @@ cudaError_t tc_prepare(K kern, int smem, int (&sms)[kMaxDev], int* sms_out) {
   return cudaSuccess;
 }
 
-// SCARL_TC_PIPELINE=1 in the environment selects the warp-specialised
-// kernel (one CTA per SM); otherwise the serial one (two CTAs per SM, each
-// running its items' phases in turn).  Both give identical outputs.
-bool tc_serial() {
-  const char* e = std::getenv("SCARL_TC_PIPELINE");
-  return !(e && *e && *e != '0');
-}
-
 // bm == nullptr: one tile; else the batched kernel over bm->total items.
 template <int N1, int N2, int LB, int NCH, int AMP>
 cudaError_t launch_tc(const GenArgs& a, const BatchMap* bm, cudaStream_t s) {
   using Cfg = TcCfg<N1, N2, LB, NCH>;
-  using Ws = TcWsCfg<N1, N2, LB, NCH>;
   int sms = 0;
   cudaError_t e;
-  if (!tc_serial()) {  // one CTA per SM
-    if (bm) {
-      static int cache[kMaxDev] = {};
-      auto kern = k_gen_z_tc_ws_batch<N1, N2, LB, NCH, AMP>;
-      if ((e = tc_prepare(kern, Ws::SMEM, cache, &sms)) != cudaSuccess) return e;
-      kern<<<std::min(bm->total, sms), Ws::THREADS, Ws::SMEM, s>>>(a, *bm);
-    } else {
-      static int cache[kMaxDev] = {};
-      auto kern = k_gen_z_tc_ws<N1, N2, LB, NCH, AMP>;
-      if ((e = tc_prepare(kern, Ws::SMEM, cache, &sms)) != cudaSuccess) return e;
-      const int nitems = (a.Hx * a.P[1] + LB - 1) / LB;
-      kern<<<std::min(nitems, sms), Ws::THREADS, Ws::SMEM, s>>>(a);
-    }
-    return cudaGetLastError();
-  }
   // two resident CTAs per SM (registers, shared and tensor memory are sized for it)
   if (bm) {
     static int cache[kMaxDev] = {};

@@ -102,31 +102,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint64
   return true;
 }
 
-// One arrival on an mbarrier (the calling thread's shared-memory writes
-// before it are released to the waiters).
-__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
-  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
-}
-
-// Named barrier `id` over `count` threads (a multiple of 32): every
-// participating thread waits, shared-memory writes before it are visible
-// after it.  group_and also returns the AND of v over the participants.
-__device__ __forceinline__ void group_sync(uint32_t id, uint32_t count) {
-  asm volatile("barrier.cta.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
-}
-__device__ __forceinline__ bool group_and(uint32_t id, uint32_t count, bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "barrier.cta.red.and.pred q, %2, %3, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}\n"
-      : "=r"(r)
-      : "r"((uint32_t)v), "r"(id), "r"(count)
-      : "memory");
-  return r != 0;
-}
-
 // Tensor-memory allocation (one full warp calls; the base column address is
 // written to shared memory at slot).
 __device__ __forceinline__ void tmem_alloc(uint32_t slot, uint32_t ncols) {

@@ -179,40 +179,3 @@ def test_fp32_tiles_run_per_tile(ctx):
     (_, _), st = _ran_tc(ctx, lambda: S.generate_sample(ctx, s, dtype=S.F32, nb_procs=8, topo=(2, 2, 2)))
     assert st["k_gen_z"][1] == 8 and st["k_mid_y"][1] == 8 and st["k_c2r_x"][1] == 8
 
-
-@pytest.mark.parametrize("Np,P,cm,nu", [
-    ((12, 10, 300), (16, 16, 512), 3, 0.5),    # 16 x 32, reciprocal amplitude
-    ((9, 7, 500), (16, 8, 512), 1, 0.5),       # separable amplitude, ragged last item
-    ((20, 6, 267), (32, 16, 512), 2, 1.5),     # power-law amplitude
-    ((11, 9, 200), (32, 16, 256), 3, 0.5),     # 16 x 16
-    ((9, 6, 600), (16, 16, 1024), 3, 0.5),     # 32 x 32, two output chunks
-    ((70, 40, 267), (128, 64, 320), 3, 0.5),   # 8 x 40, many items per CTA
-    ((12, 8, 300), (48, 16, 384), 1, 0.5),     # 16 x 24
-])
-def test_warp_specialised_equals_serial(ctx, Np, P, cm, nu, monkeypatch):
-    """The warp-specialised tensor-core pass 1 (SCARL_TC_PIPELINE=1) and the
-    serial one give the same field bit for bit."""
-    args = (Np, (1, 1, 1), (3, 3, 20), cm, nu)
-    a = S.gen_padded(ctx, *args, pad=P, seed=21, stream=2, dtype=SPLIT)
-    monkeypatch.setenv("SCARL_TC_PIPELINE", "1")
-    b = S.gen_padded(ctx, *args, pad=P, seed=21, stream=2, dtype=SPLIT)
-    monkeypatch.delenv("SCARL_TC_PIPELINE")
-    np.testing.assert_array_equal(a, b)
-
-
-def test_warp_specialised_equals_serial_batched(ctx, monkeypatch):
-    """The same for the batched launch over the 8 tiles of the headline deck
-    (513^3, SMOOTH grid, device output)."""
-    import torch
-    s = S.make_sample((0, 0, 0), (512, 512, 512), (40, 20, 10), (2, 2, 2), (41, 21, 11),
-                      corrMod=3, margiFirst=2, avg=1.0, std_dev=0.3)
-    kw = dict(dtype=SPLIT, nb_procs=8, topo=(2, 2, 2), pad_policy=S.PAD_SMOOTH)
-    a = torch.empty(513 ** 3, dtype=torch.float32, device="cuda")
-    b = torch.empty_like(a)
-    S.generate_sample(ctx, s, out=a, **kw)
-    ctx.sync()
-    monkeypatch.setenv("SCARL_TC_PIPELINE", "1")
-    S.generate_sample(ctx, s, out=b, **kw)
-    ctx.sync()
-    monkeypatch.delenv("SCARL_TC_PIPELINE")
-    assert torch.equal(a, b)
