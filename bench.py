@@ -441,8 +441,9 @@ def config_of(lay, P):
 def bench_learned(S, ctx):
     """The learned padding predictor: trained on the GPU (4096 generated
     configurations, 3000 Adam steps), then judged on 512 held-out
-    configurations against full padding: FFT volume cut and the covariance
-    error at the predicted padding (target: cut >= 30 % at <= 1 % error)."""
+    configurations against full padding and the analytic AUTO and SMOOTH
+    rules: FFT volume cut and the covariance error at each padding (target:
+    cut >= 30 % against full padding at <= 1 % error)."""
     import scarl_b200.learned as LRN
     t0 = time.perf_counter()
     fit = LRN.fit(ctx, n_train=4096, seed=1, steps=3000, lr=3e-3)
@@ -454,9 +455,13 @@ def bench_learned(S, ctx):
             "s_train_incl_labels": round(t1 - t0, 2), "s_evaluate": round(t2 - t1, 2),
             "held_out_configs": ev["configs"],
             "fft_volume_cut_vs_full": round(ev["volume_reduction"], 4),
+            "fft_volume_cut_vs_auto": round(ev["volume_reduction_vs_auto"], 4),
+            "fft_volume_cut_vs_smooth": round(ev["volume_reduction_vs_smooth"], 4),
             "frac_axes_within_1pct": round(ev["frac_axes_within_1pct"], 4),
             "max_cov_error_learned": round(ev["max_cov_error_learned"], 5),
             "max_cov_error_full": round(ev["max_cov_error_full"], 5),
+            "max_cov_error_auto": round(ev["max_cov_error_auto"], 5),
+            "max_cov_error_smooth": round(ev["max_cov_error_smooth"], 5),
             "fallbacks": ev["fallbacks"]}
 
 

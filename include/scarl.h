@@ -416,7 +416,9 @@ int scarl_mlp_train(scarl_ctx* ctx, const float* X, const float* T, int n, int s
                     double* loss_hist);
 int scarl_mlp_predict(scarl_ctx* ctx, const float* X, int n, float* Y);
 /* Padded grid and overlap width per axis from the trained model, with a
- * 2^0.25 safety margin; full padding (SRC_F/fftw_ScaRL.f90:194) when the
+ * 2^0.25 safety margin, rounded up to the next length the generator runs
+ * (powers of two, 3, 5, 7 times a power of two >= 16); full padding
+ * (SRC_F/fftw_ScaRL.f90:194) when the
  * inputs leave the trained range or the prediction exceeds it (fallback:
  * bit 0 out of range, bit 1 capped).  W may be NULL. */
 int scarl_pad_size_learned(scarl_ctx* ctx, int corrMod, double nu, const double corrL[3],

@@ -2181,13 +2181,15 @@ int scarl_pad_size_learned(scarl_ctx* ctx, int corrMod, double nu, const double 
     }
     const double D = ell[d] * std::exp2((double)Y[2 * d] + kLearnMargin);
     const double need = (double)Np[d] - 1.0 + std::ceil(D);
-    int p2 = 8;
-    while ((double)p2 < need || p2 < Np[d]) p2 <<= 1;
-    if (p2 > full[d] || !std::isfinite(D)) {
-      p2 = full[d];
+    // the smallest length the generator runs (powers of two and 3, 5, 7
+    // times a power of two >= 16) that covers the prediction
+    int p = std::max(8, Np[d]);
+    while (p <= 2048 && ((double)p < need || !fft_length_supported(p))) ++p;
+    if (p > full[d] || p > 2048 || !std::isfinite(D)) {
+      p = full[d];
       fb |= 2;
     }
-    P[d] = p2;
+    P[d] = p;
     if (W) {
       const double w = std::ceil(ell[d] * std::exp2((double)Y[2 * d + 1] + kLearnMargin));
       W[d] = (int)std::min<double>((double)Np[d], std::max(2.0, std::isfinite(w) ? w : (double)Np[d]));

@@ -217,9 +217,9 @@ __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
   const int64_t nlines = (int64_t)Ny * Nz;
   const C* work = static_cast<const C*>(a.work);
   const int b = threadIdx.x / TPL, t = threadIdx.x % TPL;
-  const int64_t l = (int64_t)bx * B + b;
-  const bool valid = l < nlines;
-  const int y = valid ? (int)(l % Ny) : 0, z = valid ? (int)(l / Ny) : 0;
+  const int l = bx * B + b;  // lines of a tile: Ny Nz <= 2048^2
+  const bool valid = l < (int)nlines;
+  const int y = valid ? l % Ny : 0, z = valid ? l / Ny : 0;
   const bool blend = a.epi.mode != 0;
   {  // the block's tables, then the raw half-spectrum line (N + 1 values, padded to 16 bytes)
     const C* twx = static_cast<const C*>(a.tw_x);

@@ -6,8 +6,9 @@ configuration -- spectrum type, von Karman order, correlation length and
 grid size -- to the padded length and overlap width that keep the
 method's covariance error within 1 %.  Labels come from the method itself
 (scarl_pad_labels: the expected axis covariance of the padded periodic
-method in FP64 on the GPU); predictions carry a safety margin and fall back
-to the reference's full padding outside the trained range.
+method in FP64 on the GPU); predictions carry a safety margin, are rounded up to the next length the
+generator runs, and fall back to the reference's full padding outside the
+trained range.
 
 Workload: 4096 training and 512 held-out configurations, spectrum uniform
 in {Gaussian, exponential, von Karman with nu uniform in [0.3, 1.5]},
@@ -147,9 +148,19 @@ def fit(ctx, n_train=4096, seed=1, steps=3000, lr=3e-3):
     return {"loss": hist, "saturated": int(sat.sum()), "axes": len(P)}
 
 
+def rule_pad(cm, nu, ell, N, policy, tol=1e-3):
+    """Padded grids of the analytic rules (SCARL_PAD_AUTO, SCARL_PAD_SMOOTH)
+    for the same configurations, spacing 1."""
+    from . import api as S
+    return np.array([S.pad_size(policy, int(cm[i]), ell[i], (1, 1, 1), N[i],
+                                float(nu[i]) if cm[i] == _lib.CM_VON_KARMAN else 0.5, tol)
+                     for i in range(len(cm))])
+
+
 def evaluate(ctx, n_test=512, seed=2):
-    """Held-out comparison with full padding: FFT volume of the padded grids
-    and the covariance error at the predicted padding."""
+    """Held-out comparison with full padding and with the analytic AUTO and
+    SMOOTH rules (periodic-image tolerance 1e-3): FFT volume of the padded
+    grids and the covariance error at each padding."""
     cm, nu, N, ell = sample_configs(n_test, seed)
     Pl, Wl, fbs = [], [], []
     for i in range(n_test):
@@ -159,16 +170,25 @@ def evaluate(ctx, n_test=512, seed=2):
         fbs.append(fb)
     Pl = np.array(Pl)
     Pf = full_pad(N)
+    Pa = rule_pad(cm, nu, ell, N, _lib.PAD_AUTO)
+    Ps = rule_pad(cm, nu, ell, N, _lib.PAD_SMOOTH)
     a = _axes(cm, nu, N, ell)
     e_learn = pad_error(ctx, *a, Pl.reshape(-1))
     e_full = pad_error(ctx, *a, Pf.reshape(-1))
+    e_auto = pad_error(ctx, *a, Pa.reshape(-1))
+    e_smooth = pad_error(ctx, *a, Ps.reshape(-1))
     Plab, Wlab, _ = labels(ctx, *a)
-    vol_l = float(np.prod(Pl.astype(np.float64), axis=1).sum())
-    vol_f = float(np.prod(Pf.astype(np.float64), axis=1).sum())
+    vol = lambda P: float(np.prod(P.astype(np.float64), axis=1).sum())
+    vol_l, vol_f, vol_a, vol_s = vol(Pl), vol(Pf), vol(Pa), vol(Ps)
     return {"configs": n_test, "volume_learned": vol_l, "volume_full": vol_f,
+            "volume_auto": vol_a, "volume_smooth": vol_s,
             "volume_reduction": 1.0 - vol_l / vol_f,
+            "volume_reduction_vs_auto": 1.0 - vol_l / vol_a,
+            "volume_reduction_vs_smooth": 1.0 - vol_l / vol_s,
             "max_cov_error_learned": float(e_learn.max()),
             "max_cov_error_full": float(e_full.max()),
+            "max_cov_error_auto": float(e_auto.max()),
+            "max_cov_error_smooth": float(e_smooth.max()),
             "frac_axes_within_1pct": float(np.mean(e_learn <= 0.01 + 1e-12)),
             "fallbacks": int(np.count_nonzero(fbs)),
             "overlap_learned": np.array(Wl), "overlap_label": Wlab.reshape(n_test, 3),

@@ -152,3 +152,33 @@ def test_ensemble_split_bf16_batched_tensor_core(ctx, oracle):
             assert rel(fields[i], ref) < TOL32, i
     again = S.gen_ensemble(ctx, Np, cl, corrMod=3, pad_policy=S.PAD_SMOOTH, seeds=seeds, dtype=split)
     np.testing.assert_array_equal(again, out)  # the captured graph replays the same field
+
+
+def test_ensemble_256_every_group_vs_oracle(ctx, oracle):
+    """The benchmark ensemble itself (256 realisations, axes from {64, ..., 256},
+    l in [4, 32], exponential, seeds 0-255, SMOOTH padding): every one of the
+    256 split-BF16 fields against the FP64 batched ensemble of the same seeds
+    (rel-L2 <= 1e-5 each), and for every z length of pass 1 (one batched
+    launch each, tensor-core or CUDA-core) its largest realisation, in split
+    BF16 and in FP32, against the FP64 oracle (rel-L2 <= 1e-5)."""
+    Np, cl = S.ensemble_draw(0, 0, 256)
+    seeds = np.arange(256, dtype=np.uint64)
+    P = _pads(Np, cl, 3, policy=S.PAD_SMOOTH)
+    kw = dict(corrMod=3, pad_policy=S.PAD_SMOOTH, seeds=seeds)
+    f64 = S.ensemble_fields(S.gen_ensemble(ctx, Np, cl, dtype=S.F64, **kw), Np)
+    split = S.ensemble_fields(S.gen_ensemble(ctx, Np, cl, dtype=S.F32 | S.SPLIT_BF16, **kw), Np)
+    f32 = S.ensemble_fields(S.gen_ensemble(ctx, Np, cl, dtype=S.F32, **kw), Np)
+    errs = np.array([rel(a, b) for a, b in zip(split, f64)])
+    print(f"split vs FP64, 256 fields: max rel-L2 {errs.max():.2e}, median {np.median(errs):.2e}")
+    assert errs.max() < TOL32
+    groups = {}
+    for i, p in enumerate(P):
+        groups.setdefault(int(p[2]), []).append(i)
+    vol = np.prod(Np.astype(np.int64), axis=1)
+    for z, idx in sorted(groups.items()):
+        i = max(idx, key=lambda j: vol[j])
+        ref = oracle.gen_padded(Np[i], P[i], (1, 1, 1), cl[i], 3, 0.5, 1, seed=int(seeds[i]))
+        e_s, e_f = rel(split[i], ref), rel(f32[i], ref)
+        print(f"z length {z}: {len(idx)} realisations, largest {list(Np[i])}: split {e_s:.2e}, "
+              f"f32 {e_f:.2e}, f64 {rel(f64[i], ref):.2e}")
+        assert e_s < TOL32 and e_f < TOL32 and rel(f64[i], ref) < TOL64

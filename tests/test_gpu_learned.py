@@ -1,6 +1,7 @@
 """Learned padding on the GPU: labels and errors against the CPU oracle, the
 MLP's gradients against the oracle's BF16 network, training, the held-out
-gain over full padding, and the Monte Carlo judge.  Tolerances: labels
+gain over full padding and the analytic AUTO / SMOOTH rules, labels measured
+from 64 realisations against the method labels, and the Monte Carlo judge.  Tolerances: labels
 exact (or at a tie of the error with the 1 % threshold), errors rel 1e-9,
 gradients rel-L2 2e-3 per tensor (FP32 vs FP64 sums under BF16 rounding)."""
 import numpy as np
@@ -60,8 +61,10 @@ def test_training_and_held_out_gain_over_full_padding(ctx, trained):
     ev = L.evaluate(ctx, n_test=512, seed=2)
     print({k: v for k, v in ev.items() if not isinstance(v, np.ndarray)})
     assert ev["volume_reduction"] >= 0.30          # FFT volume cut vs full padding
+    assert ev["volume_reduction_vs_auto"] >= 0.30  # and vs the analytic power-of-two rule
+    assert ev["volume_reduction_vs_smooth"] > 0.0  # and vs the analytic smooth-length rule
     assert ev["frac_axes_within_1pct"] >= 0.99     # covariance error held
-    assert ev["max_cov_error_learned"] <= 0.02
+    assert ev["max_cov_error_learned"] <= 0.01
     # the learned policy through the generator
     s = S.make_sample((0, 0, 0), (99, 79, 63), (6, 9, 4), (0, 0, 0), (7, 10, 5), corrMod=3)
     a, lay = S.generate_sample(ctx, s, dtype=S.F64, pad_policy=S.PAD_LEARNED)
@@ -88,3 +91,83 @@ def test_monte_carlo_judge(ctx, trained):
         ef = np.max(np.abs(mf - ref))
         assert el <= ef + 0.01 + 4 * max(sl.max(), sf.max()), (cm, P, Pf, el, ef)
         assert np.prod(P) <= np.prod(Pf)
+
+
+def _supported(p):
+    m = p
+    while m % 2 == 0:
+        m //= 2
+    return 8 <= p <= 2048 and (m == 1 or (m in (3, 5, 7) and p // m >= 16))
+
+
+def _method_axis_cov(cm, nu, ell, P, d, H):
+    """Expected covariance along axis d of the 3-D padded method on grid P
+    (spacing 1, unit variance), lags 0..H: sum over the full periodic grid of
+    S(f) cos(2 pi k_d h / P_d) over sum S(f), with S the model's 3-D spectral
+    density (Gaussian exp(-pi sum l^2 f^2), Matern (1 + sum 4 pi^2 a^2 f^2)^-(nu + 3/2),
+    a = l Gamma(nu) / (2 sqrt(pi) Gamma(nu + 1/2)))."""
+    from scipy.special import gamma
+    f = [np.where(2 * np.arange(n) <= n, np.arange(n), np.arange(n) - n) / n for n in P]
+    if cm != 1:
+        v = 0.5 if cm == 3 else nu
+        a = [e * gamma(v) / (2 * np.sqrt(np.pi) * gamma(v + 0.5)) for e in ell]
+    marg = np.zeros(P[d])
+    o = [x for x in range(3) if x != d]
+    for c0 in range(0, P[o[1]], 8):
+        fd = f[d][:, None, None]
+        f1 = f[o[0]][None, :, None]
+        f2 = f[o[1]][None, None, c0:c0 + 8]
+        l = [ell[d], ell[o[0]], ell[o[1]]]
+        if cm == 1:
+            S = np.exp(-np.pi * (l[0] ** 2 * fd ** 2 + l[1] ** 2 * f1 ** 2 + l[2] ** 2 * f2 ** 2))
+        else:
+            A = [a[d], a[o[0]], a[o[1]]]
+            q = 1 + 4 * np.pi ** 2 * (A[0] ** 2 * fd ** 2 + A[1] ** 2 * f1 ** 2 + A[2] ** 2 * f2 ** 2)
+            S = q ** -(v + 1.5)
+        marg += S.sum(axis=(1, 2))
+    h = np.arange(H + 1)
+    k = np.arange(P[d])
+    return (marg[None, :] * np.cos(2 * np.pi * np.outer(h, k) / P[d])).sum(axis=1) / marg.sum()
+
+
+def test_measured_labels_agree_with_method_labels(ctx):
+    """Labels measured as the configuration describes them: per axis, the
+    smallest padded length (among the lengths the generator runs) whose axis
+    covariance, averaged over 64 realisations, is within 1 % of the method's
+    with that axis padded to 32 N (the other axes at full padding in both),
+    allowing 3 standard errors of the average; short correlations (l <= 6
+    points on 64-96 point axes) keep the standard error well below 1 %.  Each
+    measured label lies within one supported length of the method label
+    (from the axis model, rounded up to a supported length), and the measured
+    error at the rounded method label is within 1 % + 4 standard errors."""
+    cases = [(1, 0.0, (4.0, 5.5, 3.0), (64, 80, 72)),
+             (3, 0.5, (3.0, 4.5, 5.0), (72, 64, 96)),
+             (2, 0.9, (5.0, 3.5, 4.0), (64, 72, 64))]
+    for cm, nu, ell, N in cases:
+        full = [int(v) for v in L.full_pad(N)]
+        H = min(N) - 1
+        lab, _, _ = L.labels(ctx, np.full(3, cm, np.int32), np.full(3, nu), np.array(ell, float),
+                             np.array(N, np.int32))
+        for d in range(3):
+            Pref = list(full)
+            Pref[d] = 32 * N[d]
+            ref = _method_axis_cov(cm, nu, ell, Pref, d, H)
+            cands = [p for p in range(N[d], full[d] + 1) if _supported(p)]
+            rounded = min(p for p in cands if p >= lab[d])
+            measured, err_at = None, {}
+            for p in cands:
+                P = list(full)
+                P[d] = p
+                m, se = L.judge(ctx, cm, nu, ell, N, P, realisations=64, seed0=1000 * d)
+                e = float(np.max(np.abs(m[d] - ref)))
+                err_at[p] = (e, float(se[d].max()))
+                if measured is None and e <= 0.01 + 3 * se[d].max():
+                    measured = p
+                if p >= rounded and measured is not None:
+                    break
+            print(f"cm {cm} axis {d}: N {N[d]} l {ell[d]}: method label {lab[d]} -> {rounded}, "
+                  f"measured {measured}; error at {rounded}: {err_at[rounded][0]:.4f} "
+                  f"(se {err_at[rounded][1]:.4f})")
+            assert measured is not None, (cm, d, err_at)
+            assert abs(cands.index(measured) - cands.index(rounded)) <= 1, (cm, d, measured, rounded)
+            assert err_at[rounded][0] <= 0.01 + 4 * err_at[rounded][1]
