@@ -49,6 +49,7 @@ module scarl_gpu
     integer(c_int) :: autotune = 0
     type(c_ptr) :: phiK = c_null_ptr
     integer(c_int) :: gen_meth = SCARL_FFT
+    type(c_ptr) :: moments = c_null_ptr   ! c_loc of real(c_double) :: m(2), or c_null_ptr
   end type scarl_gen_opts
 
   interface

@@ -129,6 +129,10 @@ typedef struct {
                              partition of unity; SCARL_FFT_MPI: the whole re-fitted grid as
                              one global transform (DCT: spectrum over every kz, phases
                              L0/2 x L1/2 x L2) */
+  double* moments;        /* non-NULL (host, 2 values): receives sum f and sum f^2 over
+                             the output field in FP64, accumulated inside the C2R pass as
+                             each point becomes final (no second read of the field;
+                             padded and Shino generators, not with normalize_field) */
 } scarl_gen_opts;
 
 /* ------------------------------------------------------------------ */
@@ -144,7 +148,13 @@ int scarl_sync(scarl_ctx* ctx);
  * padded grid P and tile Np, keeps the fastest per (dtype, pass, line
  * length) in the context, and merges the choices into cache_path (text
  * lines "dtype pass N variant"; NULL = no file).  Contexts also load the
- * file named by the environment variable SCARL_TUNE_CACHE when created. */
+ * file named by the environment variable SCARL_TUNE_CACHE when created.
+ * FP32 pass 3 has three more variants after the shared-memory engine's five
+ * (5, 6, 7: the line transform in registers and warp shuffles with 8, 16
+ * and 32 lanes a line, for half lengths N = N2 L with N2 <= 32 of the form
+ * 2^a, 3, 5 or 7 x 2^a); an untuned FP32 pass 3 runs variant 7, else 6,
+ * where it serves the length.  scarl_tune_get gives the stored choice (-1
+ * when the triple has none); scarl_tune_set with variant -1 forgets it. */
 int scarl_autotune(scarl_ctx* ctx, int dtype, int corrMod, double nu, const int P[3],
                    const int Np[3], const double xStep[3], const double corrL[3],
                    const char* cache_path);
@@ -378,6 +388,11 @@ int scarl_rebuild_sk(scarl_ctx* ctx, const void* field, int dtype, const int L[3
  * maxlag < L[d] and L[d] + maxlag <= 4096. */
 int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
                    const double* known_mean, double* mean, double* var, double* cov);
+/* scarl_axis_cov with the field's sums already known: sums = (sum f,
+ * sum f^2), as scarl_gen_opts.moments streams them out of the generator's
+ * C2R pass, so that only the per-axis passes read the field. */
+int scarl_axis_cov_sums(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
+                        const double sums[2], double* mean, double* var, double* cov);
 /* [host] rebuild_corrL (statistics_RF.f90:468-486). */
 int scarl_rebuild_corrL(const double* SkTot, const int L[3], const double xStep[3],
                         double corrL_out[3]);

@@ -50,7 +50,7 @@ class GenOpts(C.Structure):
                 ("pad_policy", C.c_int), ("pad_tol", C.c_double),
                 ("no_spectral_normalisation", C.c_int), ("normalize_field", C.c_int),
                 ("stream", C.c_uint32), ("autotune", C.c_int), ("phiK", C.POINTER(C.c_double)),
-                ("gen_meth", C.c_int)]
+                ("gen_meth", C.c_int), ("moments", C.POINTER(C.c_double))]
 
 
 _vp = C.c_void_p
@@ -131,6 +131,7 @@ SIGNATURES = {
     "scarl_h5_read_attr": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _dp, C.c_int,
                                      C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
     "scarl_axis_cov": (C.c_int, [_vp, _vp, C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp]),
+    "scarl_axis_cov_sums": (C.c_int, [_vp, _vp, C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp]),
     "scarl_ensemble_draw": (C.c_int, [C.c_uint64, C.c_longlong, C.c_int, _ip, C.c_int, C.c_double,
                                       C.c_double, _ip, _dp]),
     "scarl_gen_ensemble": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _ip, _dp, _dp, C.c_int,

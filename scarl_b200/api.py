@@ -375,9 +375,11 @@ def axis_correlation(corrMod, l, r, nu=0.5):
 def generate_sample(ctx, sample, generator=GEN_PADDED, dtype=F32, nb_procs=1, topo=None,
                     pad=None, pad_policy=PAD_FULL, pad_tol=1e-3, normalise_spectrum=True,
                     normalize_field=False, stream=0, phiK=None, autotune=False, out=None,
-                    gen_meth=1):
+                    gen_meth=1, moments=None):
     """One deck sample end to end (layout, tiles, PoU blend, marginal).
-    gen_meth 2 (FFT_MPI): the whole re-fitted grid as one global transform."""
+    gen_meth 2 (FFT_MPI): the whole re-fitted grid as one global transform.
+    moments: a float64 array of 2 that receives sum f and sum f^2 over the
+    output field, accumulated inside the C2R pass."""
     lay = sample_layout(sample, gen_meth, nb_procs, topo)
     out = _alloc_out(out, tuple(int(v) for v in lay["L"]), dtype)
     o = GenOpts()
@@ -396,6 +398,9 @@ def generate_sample(ctx, sample, generator=GEN_PADDED, dtype=F32, nb_procs=1, to
     if phiK is not None:
         keep = np.ascontiguousarray(phiK, dtype=np.float64)
         o.phiK = keep.ctypes.data_as(C.POINTER(C.c_double))
+    if moments is not None:
+        assert moments.dtype == np.float64 and moments.size >= 2 and moments.flags.c_contiguous
+        o.moments = moments.ctypes.data_as(C.POINTER(C.c_double))
     _check(lib().scarl_generate_sample(ctx.handle, C.byref(sample), C.byref(o), _ptr(out)), ctx)
     return out, lay
 
@@ -465,13 +470,22 @@ def rebuild_Sk(ctx, field, L, avg, stdDev, tukey_literal=True):
     return out
 
 
-def axis_cov(ctx, field, L, maxlag, known_mean=None):
+def axis_cov(ctx, field, L, maxlag, known_mean=None, sums=None):
     """Mean, variance and covariance (3, maxlag + 1) along each axis of one
     field (numpy array or device tensor, column-major L), FP64 sums; the
-    lag products are centred by known_mean when given, else the sample mean."""
+    lag products are centred by known_mean when given, else the sample mean.
+    sums: (sum f, sum f^2) streamed from generate_sample(moments=...), which
+    spares the moment pass (known_mean must then be None)."""
     L = [int(v) for v in L]
     cov = np.zeros(3 * (maxlag + 1))
     m, v = C.c_double(), C.c_double()
+    if sums is not None:
+        assert known_mean is None
+        sm = np.ascontiguousarray(sums, dtype=np.float64)
+        _check(lib().scarl_axis_cov_sums(ctx.handle, _ptr(field), _dtype_of(field), _i3(L), int(maxlag),
+                                         sm.ctypes.data_as(C.POINTER(C.c_double)), C.byref(m), C.byref(v),
+                                         cov.ctypes.data_as(C.POINTER(C.c_double))), ctx)
+        return m.value, v.value, cov.reshape(3, maxlag + 1)
     km = None if known_mean is None else C.byref(C.c_double(float(known_mean)))
     _check(lib().scarl_axis_cov(ctx.handle, _ptr(field), _dtype_of(field), _i3(L), int(maxlag),
                                 km, C.byref(m), C.byref(v),

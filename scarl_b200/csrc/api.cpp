@@ -147,6 +147,7 @@ struct scarl_ctx {
   std::string err;
   Buf work, tile, stage_out, stage_in, stage_in2, tabs, dtabs, part, t1, t2, sk, pmpw;
   Buf status;  // device word raised by kernels whose bounded waits expired
+  Buf mom;     // FP64 partial pairs of the streamed moments (pass 3) and their sum
   int wait_test = 0;  // test hook of the bounded tensor-core waits
   void* pin = nullptr;
   size_t pin_n = 0;
@@ -900,7 +901,7 @@ int gen_args(scarl_ctx* ctx, int dt, const int P[3], const int Np[3], GenArgs* a
   const int Nl[3] = {P[2], P[1], P[0] / 2};
   for (int p = 0; p < 3; ++p) {
     auto it = ctx->tune.find(tune_key(dt, p + 1, Nl[p]));
-    a->var[p] = it == ctx->tune.end() ? 0 : it->second;
+    a->var[p] = it == ctx->tune.end() ? gen_default_variant(dt, p + 1, *a) : it->second;
   }
   return SCARL_OK;
 }
@@ -1122,7 +1123,7 @@ int ens_build(scarl_ctx* ctx, int dt, int split, int n, const int* Np, const dou
         return (long long)p[0] * p[1] * p[2] > (long long)q[0] * q[1] * q[2];
       });
       auto it = ctx->tune.find(tune_key(dt, pass, g.N));
-      g.var = it == ctx->tune.end() ? 0 : it->second;
+      g.var = it == ctx->tune.end() ? gen_default_variant(dt, pass, e->args[g.items[0]]) : it->second;
       std::vector<int> st;
       if (ens_starts(ctx, e, g, g.var, &st) != SCARL_OK) g.var = 0;
       RC(ens_starts(ctx, e, g, g.var, &st));
@@ -1650,7 +1651,7 @@ int scarl_ctx_destroy(scarl_ctx* ctx) {
   flush_marks(ctx);
   for (Buf* b : {&ctx->work, &ctx->targs, &ctx->tile, &ctx->stage_out, &ctx->stage_in, &ctx->stage_in2,
                  &ctx->tabs, &ctx->dtabs, &ctx->part, &ctx->t1, &ctx->t2, &ctx->sk, &ctx->pmpw,
-                 &ctx->status})
+                 &ctx->status, &ctx->mom})
     release(ctx, *b);
   for (auto& kv : ctx->plans) release(ctx, kv.second.tabs);
   for (auto& kv : ctx->twiddles) release(ctx, kv.second);
@@ -1729,12 +1730,16 @@ int scarl_autotune(scarl_ctx* ctx, int dtype, int corrMod, double nu, const int 
 int scarl_tune_get(scarl_ctx* ctx, int dtype, int pass, int N, int* variant) {
   if (!ctx || !variant || pass < 1 || pass > 3) return SCARL_EINVAL;
   auto it = ctx->tune.find(tune_key(dtype, pass, N));
-  *variant = it == ctx->tune.end() ? 0 : it->second;
+  *variant = it == ctx->tune.end() ? -1 : it->second;
   return SCARL_OK;
 }
 
 int scarl_tune_set(scarl_ctx* ctx, int dtype, int pass, int N, int variant) {
   if (!ctx || pass < 1 || pass > 3 || (dtype != SCARL_F32 && dtype != SCARL_F64)) return SCARL_EINVAL;
+  if (variant == -1) {  // forget the choice: the default variant runs again
+    ctx->tune.erase(tune_key(dtype, pass, N));
+    return SCARL_OK;
+  }
   if (variant < 0 || variant >= gen_variant_count(dtype, pass)) return SCARL_EINVAL;
   ctx->tune[tune_key(dtype, pass, N)] = variant;
   return SCARL_OK;
@@ -2686,7 +2691,14 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   void* dev;
   bool host;
   RC(out_dev(ctx, global, ng * dt, &dev, &host));
+  if (o.moments && (gen == SCARL_GEN_DCT || o.normalize_field))
+    return fail(ctx, SCARL_EUNSUPPORTED,
+                "streamed moments need the padded or Shino generator without normalize_field");
   if (s->std_dev == 0.0) {  // write_constant_field, SRC_F/main_ScaRL.f90:145-155
+    if (o.moments) {
+      o.moments[0] = s->avg * (double)ng;
+      o.moments[1] = s->avg * s->avg * (double)ng;
+    }
     if (dt == 8) {
       CK(cudaMemsetAsync(dev, 0, ng * 8, ctx->stream));
       RC(launch_marginal(8, dev, (int64_t)ng, 1, 0.0, s->avg, ctx->stream) == cudaSuccess ? SCARL_OK : SCARL_EDEVICE);
@@ -2779,6 +2791,8 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
     if (kb > 1 && ensure(ctx, ctx->work, wtile * kb) != SCARL_OK) kb = 1;  // budget: one tile at a time
   }
   std::vector<GenArgs> grp;
+  double* mom_base = nullptr;
+  size_t mom_cnt = 0;
   auto padded_args = [&](int r, GenArgs* a) -> int {
     scarl_tile t;
     tile_geometry(&lay, s->xMinGlob, r, &t);
@@ -2793,6 +2807,38 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
       a->epi.off[d] = t.pos_0[d] - 1;
       a->epi.ax[d] = axes[(size_t)r * 3 + d];
     }
+    a->epi.mom = mom_base ? mom_base + 2 * mom_cnt * (size_t)r : nullptr;
+    return SCARL_OK;
+  };
+  // streamed moments: tile r's pass 3 writes mom_cnt FP64 partial pairs at
+  // mom_base + 2 mom_cnt r, summed in a fixed order after the last tile
+  if (o.moments) {
+    GenArgs a0;
+    if (gen == SCARL_GEN_PADDED) {
+      RC(padded_args(0, &a0));
+    } else {
+      scarl_tile t0;
+      tile_geometry(&lay, s->xMinGlob, 0, &t0);
+      RC(shino_args(ctx, lay.Np, t0.xRange, s->corrL, (int32_t)((uint32_t)s->seedBase + 1u), &a0));
+    }
+    const int c = gen_pass3_partials(gen == SCARL_GEN_PADDED ? dt : 8, a0.var[2], a0);
+    if (c < 1) return fail(ctx, SCARL_EDEVICE, "no pass-3 launch for the streamed moments");
+    mom_cnt = (size_t)c;
+    RC(ensure(ctx, ctx->mom, (2 * mom_cnt * lay.nb_tiles + 2 + 2 * (size_t)pair_sum_parts()) * sizeof(double)));
+    mom_base = static_cast<double*>(ctx->mom.p);
+  }
+  // the moments' pair sum, queued after the last tile; read once the stream is idle
+  auto moments_sum = [&]() -> int {
+    if (!mom_base) return SCARL_OK;
+    CK(launch_pair_sum(mom_base, (int64_t)(mom_cnt * lay.nb_tiles), mom_base + 2 * mom_cnt * lay.nb_tiles + 2,
+                       mom_base + 2 * mom_cnt * lay.nb_tiles, ctx->stream));
+    return SCARL_OK;
+  };
+  auto moments_read = [&]() -> int {
+    if (!mom_base) return SCARL_OK;
+    CK(cudaMemcpyAsync(o.moments, mom_base + 2 * mom_cnt * lay.nb_tiles, 2 * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return SCARL_OK;
   };
   const int rc_tiles = [&]() -> int {
@@ -2826,6 +2872,7 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
         GenArgs a;
         RC(shino_args(ctx, lay.Np, t.xRange, s->corrL, seedStart, &a));
         a.epi = e;
+        a.epi.mom = mom_base ? mom_base + 2 * mom_cnt * (size_t)r : nullptr;
         RC(run_passes(ctx, 8, a));
       } else {
         const double* phi = phi_all ? (const double*)phi_all + nk * r : nullptr;
@@ -2856,6 +2903,7 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
   const int rc_slabs = slab_end(slabs);
   RC(rc_tiles);
   RC(rc_slabs);
+  RC(moments_sum());
   if (ring_out) {
     if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     const int rc_ring = ring_copy(ctx, global, dev, plane_b, ring_pieces, ctx->copy_stream);
@@ -2863,12 +2911,14 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
     RC(rc_ring);
     CK(cudaStreamSynchronize(ctx->stream));
     RC(check_status(ctx));
+    RC(moments_read());
     CK(cudaGetLastError());
     return SCARL_OK;
   }
   if (stream_out) {
     CK(cudaStreamSynchronize(ctx->stream));
     RC(check_status(ctx));
+    RC(moments_read());
     CK(cudaGetLastError());
     return SCARL_OK;
   }
@@ -2878,7 +2928,8 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
     Prof p(ctx, "k_marginal");
     CK(launch_marginal(dt, dev, (int64_t)ng, s->margiFirst, ms, mmu, ctx->stream));
   }
-  return finish_out(ctx, global, dev, ng * dt, host);
+  RC(finish_out(ctx, global, dev, ng * dt, host));
+  return moments_read();
 }
 
 // ---- post steps ----
@@ -3046,8 +3097,11 @@ int scarl_moments(scarl_ctx* ctx, const void* field, int dtype, long long xN, in
   return SCARL_OK;
 }
 
-int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
-                   const double* known_mean, double* mean, double* var, double* cov) {
+// sums: (sum f, sum f^2) of the field when already known (streamed from the
+// generator), so that the moment pass is skipped; NULL = run it.
+static int axis_cov_impl(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
+                         const double* known_mean, const double* sums, double* mean, double* var,
+                         double* cov) {
   RC(begin(ctx));
   if (!field || !L || !mean || !var || !cov) return fail(ctx, SCARL_EINVAL, "null argument");
   if (dtype != SCARL_F32 && dtype != SCARL_F64) return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64");
@@ -3070,18 +3124,22 @@ int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3],
   const void* dev;
   RC(in_dev(ctx, ctx->stage_in, field, n * dtype, &dev));
   // mean (FP64 sums)
-  const int nb = sums_blocks((int64_t)n);
-  RC(ensure(ctx, ctx->part, (size_t)nb * 2 * 8));
-  {
-    Prof p(ctx, "k_sums");
-    CK(launch_sums(dtype, dev, (int64_t)n, 1, (double*)ctx->part.p, nb, ctx->stream));
-  }
-  std::vector<double> h((size_t)nb * 2);
-  CK(cudaMemcpyAsync(h.data(), ctx->part.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  ctx->d2h += h.size() * 8;
   double s1 = 0.0;
-  for (int b = 0; b < nb; ++b) s1 += h[2 * (size_t)b];
+  if (sums) {
+    s1 = sums[0];
+  } else {
+    const int nb = sums_blocks((int64_t)n);
+    RC(ensure(ctx, ctx->part, (size_t)nb * 2 * 8));
+    {
+      Prof p(ctx, "k_sums");
+      CK(launch_sums(dtype, dev, (int64_t)n, 1, (double*)ctx->part.p, nb, ctx->stream));
+    }
+    std::vector<double> h((size_t)nb * 2);
+    CK(cudaMemcpyAsync(h.data(), ctx->part.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->d2h += h.size() * 8;
+    for (int b = 0; b < nb; ++b) s1 += h[2 * (size_t)b];
+  }
   const double sample_mean = s1 / (double)n;
   const double mu = known_mean ? *known_mean : sample_mean;
   // per axis: power pass, FP64 lag sums
@@ -3124,6 +3182,17 @@ int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3],
   *mean = sample_mean;
   *var = cov[0];
   return SCARL_OK;
+}
+
+int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
+                   const double* known_mean, double* mean, double* var, double* cov) {
+  return axis_cov_impl(ctx, field, dtype, L, maxlag, known_mean, nullptr, mean, var, cov);
+}
+
+int scarl_axis_cov_sums(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
+                        const double sums[2], double* mean, double* var, double* cov) {
+  if (!sums) return fail(ctx, SCARL_EINVAL, "null argument");
+  return axis_cov_impl(ctx, field, dtype, L, maxlag, nullptr, sums, mean, var, cov);
 }
 
 int scarl_rebuild_sk(scarl_ctx* ctx, const void* field, int dtype, const int L[3], double avg,

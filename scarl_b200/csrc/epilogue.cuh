@@ -71,13 +71,23 @@ struct LineEpilogue {
     return v;
   }
   // K outputs at once: every read of an earlier tile's partial sum is issued
-  // before any write.
-  template <int K>
-  __device__ __forceinline__ void put_group(const int* xs, const T* v, int Nx) const {
+  // before any write.  With MOM, every final value w (a crop point, or a
+  // blended point whose last tile this is) is added to *s1 and w^2 to *s2 in
+  // FP64.
+  template <int K, bool MOM = false>
+  __device__ __forceinline__ void put_group(const int* xs, const T* v, int Nx, double* s1 = nullptr,
+                                            double* s2 = nullptr) const {
     if (mode == 0) {
 #pragma unroll
       for (int i = 0; i < K; ++i)
-        if (xs[i] < Nx) out[base + xs[i]] = marg(v[i]);
+        if (xs[i] < Nx) {
+          const T w = marg(v[i]);
+          out[base + xs[i]] = w;
+          if constexpr (MOM) {
+            *s1 += (double)w;
+            *s2 = fma((double)w, (double)w, *s2);
+          }
+        }
       return;
     }
     uint8_t f[K];
@@ -92,7 +102,13 @@ struct LineEpilogue {
       if (!(f[i] & 1)) continue;
       T w = pou ? v[i] * (syz * sx[xs[i]]) : v[i];
       if (!(f[i] & 2)) w = old[i] + w;
-      if (f[i] & 4) w = marg(w);
+      if (f[i] & 4) {
+        w = marg(w);
+        if constexpr (MOM) {
+          *s1 += (double)w;
+          *s2 = fma((double)w, (double)w, *s2);
+        }
+      }
       out[base + xs[i]] = w;
     }
   }

@@ -255,6 +255,8 @@ __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
     ep.sx = sxs;
   }
   constexpr int RL = last_radix<N, E>();
+  const bool mom = a.epi.mom != nullptr;
+  double s1 = 0.0, s2 = 0.0;
   auto store = [&](int j, const C* o) {
     if (!valid) return;
     T v[2 * RL];
@@ -267,9 +269,33 @@ __device__ __forceinline__ void c2r_x_body(const GenArgs& a, int bx) {
       xs[2 * r] = 2 * n;
       xs[2 * r + 1] = 2 * n + 1;
     }
-    ep.template put_group<2 * RL>(xs, v, Nx);
+    if (mom) ep.template put_group<2 * RL, true>(xs, v, Nx, &s1, &s2);
+    else ep.template put_group<2 * RL>(xs, v, Nx);
   };
   line_ifft<C, N, E, SmemOrder::LineFast, B, LS, false, 2>(sm, b, t, tws, load, store);
+  if (mom) {  // the block's FP64 partial sums of the final values, at mom[2 bx]
+    __shared__ double red[2][32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    const int w = (int)threadIdx.x >> 5, nw = ((int)blockDim.x + 31) >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      red[0][w] = s1;
+      red[1][w] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t1 = 0.0, t2 = 0.0;
+      for (int i = 0; i < nw; ++i) {
+        t1 += red[0][i];
+        t2 += red[1][i];
+      }
+      a.epi.mom[2 * (int64_t)bx] = t1;
+      a.epi.mom[2 * (int64_t)bx + 1] = t2;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

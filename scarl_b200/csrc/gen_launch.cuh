@@ -4,6 +4,9 @@
 // grid and keeps the fastest per (precision, pass, line length).
 #pragma once
 
+#include <type_traits>
+
+#include "c2r_shfl.cuh"
 #include "gen_kernels.cuh"
 
 namespace scarl {
@@ -115,6 +118,34 @@ inline cudaError_t run_c2r_x_v(const GenArgs& a, const BatchMap* bm, int* blocks
   }
 }
 
+// Pass 3 with the line transform in registers and warp shuffles
+// (c2r_shfl.cuh), L lanes a line, one group of lines a warp: FP32 only,
+// needs the status word.  With blocks != nullptr nothing is launched and
+// *blocks receives the block count (the FP64 moment pairs a single-tile
+// launch writes: one a block).
+template <typename T, int N, int L>
+inline cudaError_t run_c2r_shfl(const GenArgs& a, const BatchMap* bm, int* blocks, cudaStream_t s) {
+  using Cfg = ShflCfg<N, L>;
+  if constexpr (!std::is_same<T, float>::value || !Cfg::valid()) {
+    return cudaErrorInvalidConfiguration;
+  } else {
+    const int64_t nlines = (int64_t)a.Nout[1] * a.Nout[2];
+    const int64_t per_block = (int64_t)Cfg::WPB * Cfg::G;
+    dim3 grid((unsigned)((nlines + per_block - 1) / per_block), 1, 1);
+    if (blocks) {
+      *blocks = (int)grid.x;
+      return cudaSuccess;
+    }
+    if (!a.status) return cudaErrorInvalidValue;
+    if (bm)
+      return launch_k(k_c2r_x_shfl_batch<N, L>, dim3(bm->total), dim3(Cfg::THREADS), Cfg::SMEM, s, *bm);
+    return launch_k(k_c2r_x_shfl<N, L>, grid, dim3(Cfg::THREADS), Cfg::SMEM, s, a);
+  }
+}
+// Pass-3 variants after the engine's (RowVars) ones: the register transform
+// with 8, 16 and 32 lanes a line (FP32).
+template <typename T> constexpr int kShflVars = std::is_same<T, float>::value ? 3 : 0;
+
 // Variant v of pass `pass` for line length N (pass 3: N = P0/2).  Lengths
 // below 128 (64 for pass 3) have only variant 0; SPEC_INJECT / SPEC_SHINO
 // pass-1 kernels only variant 0.
@@ -159,6 +190,11 @@ inline cudaError_t run_pass_n(int pass, int v, const GenArgs& a, const BatchMap*
     }
   }
   if (pass == 3) {
+    if (v >= RV::n && v < RV::n + kShflVars<T>) {
+      if (v == RV::n) return run_c2r_shfl<T, N, 8>(a, bm, nb, s);
+      if (v == RV::n + 1) return run_c2r_shfl<T, N, 16>(a, bm, nb, s);
+      return run_c2r_shfl<T, N, 32>(a, bm, nb, s);
+    }
     if (v == 0) return run_c2r_x_v<T, N, RV::v[0].E, RV::v[0].B>(a, bm, nb, s);
     switch (v) {
       SCARL_ROWV(1)

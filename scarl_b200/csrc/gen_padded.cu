@@ -84,8 +84,22 @@ int gen_pass_blocks(int dt, int pass, int v, const GenArgs& a) {
   return nb;
 }
 
+// Every pass-3 kernel stores one moment pair a block.
+int gen_pass3_partials(int dt, int v, const GenArgs& a) { return gen_pass_blocks(dt, 3, v, a); }
+
+// The variant an untuned (precision, pass, length) runs: the FP32 pass 3 on
+// the register transform with 32 lanes a line (else 16) where it serves the
+// length and the status word exists; variant 0 otherwise.
+int gen_default_variant(int dt, int pass, const GenArgs& a) {
+  if (dt == 4 && pass == 3 && a.status) {
+    for (int v : {RowVars<float>::n + 2, RowVars<float>::n + 1})
+      if (gen_pass_blocks(dt, pass, v, a) > 0) return v;
+  }
+  return 0;
+}
+
 int gen_variant_count(int dt, int pass) {
-  if (pass == 3) return dt == 8 ? RowVars<double>::n : RowVars<float>::n;
+  if (pass == 3) return dt == 8 ? RowVars<double>::n : RowVars<float>::n + kShflVars<float>;
   return dt == 8 ? ColVars<double>::n : ColVars<float>::n;
 }
 

@@ -29,6 +29,8 @@ struct Epilogue {
   int marginal;        // 0 none, 1 Gaussian (x*s+mu), 2 lognormal exp(x*s+mu)
   double ms, mmu;
   int apply_pou;
+  double* mom;         // non-null: pass 3 stores per-block FP64 partial sums of the final
+                       // values and their squares here (gen_pass3_partials pairs)
 };
 
 // Spectrum synthesis for the padded periodic grid.
@@ -112,6 +114,15 @@ cudaError_t launch_gen_z_tc_batch(const GenArgs& rep, const BatchMap& m, cudaStr
 int gen_pass_blocks(int dt, int pass, int v, const GenArgs& a);
 // Number of launch variants of a pass (valid ones depend on the line length).
 int gen_variant_count(int dt, int pass);
+// Variant of an untuned (precision, pass, line length) for the grid of a.
+int gen_default_variant(int dt, int pass, const GenArgs& a);
+// FP64 partial pairs (sum x, sum x^2) a single-tile pass-3 launch of variant v
+// writes at a.epi.mom (-1: the variant does not serve the grid).
+int gen_pass3_partials(int dt, int v, const GenArgs& a);
+// out[0..1] = sums of the n pairs at pairs (device), in a fixed order; part:
+// 2 pair_sum_parts() doubles of device scratch.
+cudaError_t launch_pair_sum(const double* pairs, int64_t n, double* part, double* out, cudaStream_t s);
+int pair_sum_parts();
 // FP64 sum over the full periodic grid of S(k) dk^3: separable tables r*
 // (A_raw = rx ry rz) or Matern q tables with A_raw^2 = craw2 (1+q)^(2 expo).
 cudaError_t launch_spectrum_sum(const GenArgs& a, const double* rx, const double* ry,

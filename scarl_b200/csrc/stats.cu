@@ -101,4 +101,52 @@ cudaError_t launch_lag_cov(int dt, const void* f, const int L[3], int dir, doubl
   return cudaGetLastError();
 }
 
+// Sum of n FP64 pairs (x, y) into out[0], out[1] in a fixed order: block b
+// sums the pairs b, b + gridDim.x, ... (each thread a fixed stride, then a
+// fixed tree) into part[b]; one block then sums the gridDim.x parts.
+constexpr int kPairBlocks = 148;
+__device__ __forceinline__ void pair_tree(double a, double b, double* out) {
+  __shared__ double r0[256], r1[256];
+  r0[threadIdx.x] = a;
+  r1[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      r0[threadIdx.x] += r0[threadIdx.x + w];
+      r1[threadIdx.x] += r1[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = r0[0];
+    out[1] = r1[0];
+  }
+}
+__global__ void __launch_bounds__(256) k_pair_part(const double* __restrict__ p, int64_t n,
+                                                   double* __restrict__ part) {
+  double a = 0.0, b = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+    a += p[2 * i];
+    b += p[2 * i + 1];
+  }
+  pair_tree(a, b, part + 2 * blockIdx.x);
+}
+__global__ void __launch_bounds__(256) k_pair_final(const double* __restrict__ part, int nparts,
+                                                    double* __restrict__ out) {
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += 256) {
+    a += part[2 * i];
+    b += part[2 * i + 1];
+  }
+  pair_tree(a, b, out);
+}
+
+// part: 2 kPairBlocks doubles of scratch.
+cudaError_t launch_pair_sum(const double* pairs, int64_t n, double* part, double* out, cudaStream_t s) {
+  k_pair_part<<<kPairBlocks, 256, 0, s>>>(pairs, n, part);
+  k_pair_final<<<1, 256, 0, s>>>(part, kPairBlocks, out);
+  return cudaGetLastError();
+}
+int pair_sum_parts() { return kPairBlocks; }
+
 }  // namespace scarl
