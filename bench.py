@@ -202,7 +202,7 @@ def pass_bytes(lay, P, dtype_bytes=4):
             own *= Np[d] - (No[d] if pos[d] > 0 and No[d] >= 2 else 0)
         reread += Np[0] * Np[1] * Np[2] - own
     b3 = Hx * Np[1] * Np[2] * c + Np[0] * Np[1] * Np[2] * dtype_bytes + reread * dtype_bytes // nb
-    return {"k_gen_z": b1, "k_gen_z_tc": b1, "k_mid_y": b2, "k_c2r_x": b3}
+    return {"k_gen_z": b1, "k_gen_z_tc": b1, "k_mid_y": b2, "k_c2r_x": b3, "k_c2r_x_tc": b3}
 
 
 def oracle_layout():
@@ -616,6 +616,18 @@ def main():
     ms_f32 = timed_steps(dtype=S.F32)
     # ---- the split path on the power-of-two grid of the AUTO rule
     ms_pow2 = timed_steps(policy=S.PAD_AUTO)
+    # ---- the same grid with pass 3's x DFT on the tensor cores too
+    SPLIT_X = S.F32 | S.SPLIT_BF16_X
+    for _ in range(args.warmup):
+        step(dtype=SPLIT_X)
+    ms_splitx = timed_steps(dtype=SPLIT_X)
+    ctx.profile(True)
+    ctx.profile_reset()
+    for _ in range(2):
+        step(dtype=SPLIT_X)
+    torch.cuda.synchronize()
+    stx = ctx.profile_stats().get("k_c2r_x_tc")
+    ctx.profile(False)
 
     # ---- per-kernel device times (separate, profiled steps)
     ctx.profile(True)
@@ -684,6 +696,7 @@ def main():
                 float(d.abs().max() / f64.abs().max()))
 
     rel32, max32 = rel_to_f64(S.F32)
+    relx, maxx = rel_to_f64(SPLIT_X)
     rel, relmax = rel_to_f64(HEAD)
     # ---- the reference's precision: every DFT and sum in FP64, same grid
     for _ in range(args.warmup):
@@ -694,6 +707,11 @@ def main():
             "padded_grid": P_auto, "precision": "f64 (every DFT and sum in FP64, as the reference)"}
     pow2 = {"value": round(world * npts / (ms_pow2 * 1e-3) / 1e6, 2), "ms_per_step": round(ms_pow2, 4),
             "padded_grid": P_pow2, "pad_policy": "auto: smallest powers of two under the same rule"}
+    splitx = {"value": round(world * npts / (ms_splitx * 1e-3) / 1e6, 2), "ms_per_step": round(ms_splitx, 4),
+              "padded_grid": P_auto,
+              "precision": "f32, z DFT of pass 1 and x DFT of pass 3 as bf16 head/tail tensor-core products",
+              "k_c2r_x_tc_ms_per_tile": round(stx[0] / stx[1], 4) if stx and stx[1] else None,
+              "rel_l2_vs_gpu_fp64": relx, "max_err_vs_gpu_fp64": maxx}
     fp32 = {"value": round(world * npts / (ms_f32 * 1e-3) / 1e6, 2), "ms_per_step": round(ms_f32, 4),
             "padded_grid": P_auto, "precision": "f32 (every DFT on the CUDA cores)",
             "rel_l2_vs_fp64": rel32, "max_err_vs_fp64": max32}
@@ -766,7 +784,7 @@ def main():
                                      else "the GPU FP64 path (same seed and grid)"),
                 "rel_l2_vs_gpu_fp64": rel, "max_err_vs_gpu_fp64": relmax,
                 "roofline": roof, "tensor_stages": tensor, "kernels": kern, "launch_variants": tuned, "plain_path": plain,
-                "fp32_path": fp32, "fp64_path": fp64, "pow2_grid_path": pow2,
+                "fp32_path": fp32, "fp64_path": fp64, "pow2_grid_path": pow2, "split_x_path": splitx,
                 "speedup_vs_plain_path": round(ms_full / ms, 3),
                 "split_vs_fp32_same_grid": round(ms_f32 / ms, 3),
                 "padding_policy_gain_fp32": round(ms_full / ms_f32, 3),

@@ -19,6 +19,7 @@ module scarl_gpu
   integer(c_int), parameter :: SCARL_F32 = 4, SCARL_F64 = 8
   ! OR'ed into SCARL_F32: pass 1's z DFT as split-BF16 tensor-core products
   integer(c_int), parameter :: SCARL_SPLIT_BF16 = 256
+  integer(c_int), parameter :: SCARL_SPLIT_BF16_X = 512
   integer(c_int), parameter :: SCARL_GEN_DCT = 1, SCARL_GEN_SHINO = 2, SCARL_GEN_PADDED = 3
   integer(c_int), parameter :: SCARL_PAD_FULL = 0, SCARL_PAD_AUTO = 1, SCARL_PAD_LEARNED = 2, &
                                SCARL_PAD_SMOOTH = 3

@@ -59,6 +59,15 @@ extern "C" {
  * kernel, and injected or literal spectra, run the FP32 pass instead.  No
  * counterpart in the reference. */
 #define SCARL_SPLIT_BF16 0x100
+/* Flag OR'ed into SCARL_F32 (implies SCARL_SPLIT_BF16): pass 3's Hermitian
+ * C2R along x also runs on the tensor cores, its half length N = P0 / 2 as two
+ * split-BF16 DFT stages N1 x N2 (N2 = 32 with N1 = 2..8, or N2 = 16 with N1 =
+ * 2, 3, 5, 7), in front of the same crop / blend epilogue; other half lengths
+ * and batched ensembles keep the CUDA-core pass 3.  Field error bounded by
+ * 1e-5 relative L2 against FP64.  Slower than the CUDA-core pass 3 on B200
+ * (0.151 against 0.109 ms per tile of the 513^3 headline field), so it is
+ * not part of SCARL_SPLIT_BF16.  No counterpart in the reference. */
+#define SCARL_SPLIT_BF16_X 0x200
 
 /* ---- generators for scarl_generate_sample ---- */
 #define SCARL_GEN_DCT 1      /* gen_std_gauss_FFT, SRC_F/fftw_ScaRL.f90:261 */

@@ -7,7 +7,7 @@ front end.  Importing it without the built library raises ImportError.
 from ._lib import (CM_EXPONENTIAL, CM_GAUSSIAN, CM_VON_KARMAN, F32, F64, FOM_GAUSSIAN,
                    FOM_LOGNORMAL, GEN_DCT, GEN_PADDED, GEN_SHINO, PAD_AUTO, PAD_FULL, PAD_LEARNED,
                    PAD_SMOOTH,
-                   SPLIT_BF16, ScarlError,
+                   SPLIT_BF16, SPLIT_BF16_X, ScarlError,
                    lib)
 from .api import *  # noqa: F401,F403
 

@@ -21,6 +21,7 @@ FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
 F32, F64 = 4, 8
 # flag on F32: pass 1's z DFT as split-BF16 tensor-core products
 SPLIT_BF16 = 0x100
+SPLIT_BF16_X = 0x200
 GEN_DCT, GEN_SHINO, GEN_PADDED = 1, 2, 3
 PAD_FULL, PAD_AUTO, PAD_LEARNED, PAD_SMOOTH = 0, 1, 2, 3
 

@@ -15,7 +15,7 @@ LIB = os.path.join(HERE, "libscarl_b200.so")
 OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-CUDA_SOURCES = ["gen_padded.cu", "gen_tc.cu", "dct_literal.cu", "post.cu", "stats.cu", "cov.cu",
+CUDA_SOURCES = ["gen_padded.cu", "gen_tc.cu", "c2r_tc.cu", "dct_literal.cu", "post.cu", "stats.cu", "cov.cu",
                 "mlp.cu", "noalloc.cu"]
 # gen_inst.cu once per (precision, line-length group): the generator pass
 # instantiations compile in parallel

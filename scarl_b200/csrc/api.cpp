@@ -573,10 +573,11 @@ int ensure_status(scarl_ctx* ctx) {
 }
 
 // dtype argument of the padded generator: SCARL_F32 / SCARL_F64, optionally
-// SCARL_F32 | SCARL_SPLIT_BF16.
+// SCARL_F32 | SCARL_SPLIT_BF16 (or SCARL_SPLIT_BF16_X).
 int parse_dtype(scarl_ctx* ctx, int dtype, int* dt, int* split) {
-  *split = (dtype & SCARL_SPLIT_BF16) ? 1 : 0;
-  *dt = dtype & ~SCARL_SPLIT_BF16;
+  // bit 0: pass 1's z DFT on the tensor cores; bit 1: pass 3's x DFT too
+  *split = (dtype & SCARL_SPLIT_BF16_X) ? 3 : (dtype & SCARL_SPLIT_BF16) ? 1 : 0;
+  *dt = dtype & ~(SCARL_SPLIT_BF16 | SCARL_SPLIT_BF16_X);
   if (*dt != SCARL_F32 && *dt != SCARL_F64)
     return fail(ctx, SCARL_EINVAL, "dtype must be SCARL_F32 or SCARL_F64 (SCARL_F32 | SCARL_SPLIT_BF16)");
   if (*split && *dt != SCARL_F32) return fail(ctx, SCARL_EINVAL, "SCARL_SPLIT_BF16 applies to SCARL_F32 only");
@@ -794,7 +795,7 @@ int run_passes(scarl_ctx* ctx, int dt, const GenArgs& a) {
     CK(launch_gen_pass(dt, 2, a, ctx->stream));
   }
   {
-    Prof p(ctx, "k_c2r_x");
+    Prof p(ctx, c2r_x_tc_used(dt, a) ? "k_c2r_x_tc" : "k_c2r_x");
     CK(launch_gen_pass(dt, 3, a, ctx->stream));
   }
   return SCARL_OK;
@@ -2862,7 +2863,7 @@ int scarl_generate_sample(scarl_ctx* ctx, const scarl_sample* s, const scarl_gen
           }
           RC(run_passes12_batched(ctx, dt, grp.data(), k));
         }
-        Prof p(ctx, "k_c2r_x");
+        Prof p(ctx, c2r_x_tc_used(dt, grp[r % kb]) ? "k_c2r_x_tc" : "k_c2r_x");
         CK(launch_gen_pass(dt, 3, grp[r % kb], ctx->stream));
       } else if (gen == SCARL_GEN_PADDED) {
         GenArgs a;

@@ -189,7 +189,7 @@ __device__ __forceinline__ void epi_chunk(const LineEpilogue<float>& ep, const f
     xs[j] = x0 + lane + 32 * j;
     vv[j] = xs[j] < Nx ? ob[xs[j]] : 0.f;
   }
-  ep.template put_group<KC, MOM>(xs, vv, Nx, s1, s2);
+  ep.template put_group_line<KC, MOM>(xs, vv, Nx, s1, s2);
 }
 
 // Block bx of a launch: warp w takes the G lines of group bx WPB + w.  With

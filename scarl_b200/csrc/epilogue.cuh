@@ -60,6 +60,22 @@ struct LineEpilogue {
       sx = sw_of<T>(e.ax[0]);
     }
   }
+  // The same epilogue from a line's precomputed base, y-z flags and s_y s_z
+  // (the values the constructor above derives) and the x tables fx, sx.
+  __device__ __forceinline__ LineEpilogue(const Epilogue& e, size_t base_, uint8_t fyz_, T syz_,
+                                          const uint8_t* fx_, const T* sx_) {
+    out = static_cast<T*>(e.out);
+    mode = e.mode;
+    marginal = e.marginal;
+    ms = (T)e.ms;
+    mu = (T)e.mmu;
+    pou = e.apply_pou;
+    base = base_;
+    fyz = fyz_;
+    syz = syz_;
+    fx = fx_;
+    sx = sx_;
+  }
   // lognormal in FP32 with the hardware exponential (relative error a few
   // 2^-23, far inside the FP32 field's 1e-5 tolerance); FP64 keeps exp
   __device__ __forceinline__ T marg(T v) const {
@@ -110,6 +126,47 @@ struct LineEpilogue {
         }
       }
       out[base + xs[i]] = w;
+    }
+  }
+  // put_group through one line pointer (out + base), each access a 32-bit
+  // offset from it.
+  template <int K, bool MOM = false>
+  __device__ __forceinline__ void put_group_line(const int* xs, const T* v, int Nx, double* s1 = nullptr,
+                                                 double* s2 = nullptr) const {
+    T* o = out + base;
+    if (mode == 0) {
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if (xs[i] < Nx) {
+          const T w = marg(v[i]);
+          o[xs[i]] = w;
+          if constexpr (MOM) {
+            *s1 += (double)w;
+            *s2 = fma((double)w, (double)w, *s2);
+          }
+        }
+      return;
+    }
+    uint8_t f[K];
+    T old[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      f[i] = xs[i] < Nx ? (uint8_t)(fyz & fx[xs[i]]) : (uint8_t)0;
+      old[i] = ((f[i] & 3) == 1) ? o[xs[i]] : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      if (!(f[i] & 1)) continue;
+      T w = pou ? v[i] * (syz * sx[xs[i]]) : v[i];
+      if (!(f[i] & 2)) w = old[i] + w;
+      if (f[i] & 4) {
+        w = marg(w);
+        if constexpr (MOM) {
+          *s1 += (double)w;
+          *s2 = fma((double)w, (double)w, *s2);
+        }
+      }
+      o[xs[i]] = w;
     }
   }
   __device__ __forceinline__ void put(int x, T v) const {

@@ -69,6 +69,7 @@ cudaError_t launch_gen_pass(int dt, int pass, const GenArgs& a_in, cudaStream_t 
   philox_schedule(&a);
   if (pass == 1 && a.split && dt == 4 && a.spec == SPEC_PHILOX && gen_z_tc_supported(a.P[2]))
     return launch_gen_z_tc(a, s);
+  if (pass == 3 && c2r_x_tc_used(dt, a)) return launch_c2r_x_tc(a, s);
   return run_pass_dt(dt, pass, a.var[pass - 1], a, nullptr, nullptr, s);
 }
 
@@ -85,7 +86,10 @@ int gen_pass_blocks(int dt, int pass, int v, const GenArgs& a) {
 }
 
 // Every pass-3 kernel stores one moment pair a block.
-int gen_pass3_partials(int dt, int v, const GenArgs& a) { return gen_pass_blocks(dt, 3, v, a); }
+int gen_pass3_partials(int dt, int v, const GenArgs& a) {
+  if (c2r_x_tc_used(dt, a)) return c2r_x_tc_blocks(a);
+  return gen_pass_blocks(dt, 3, v, a);
+}
 
 // The variant an untuned (precision, pass, length) runs: the FP32 pass 3 on
 // the register transform with 32 lanes a line (else 16) where it serves the

@@ -75,7 +75,7 @@ struct GenArgs {
   double shino_f;
   Epilogue epi;
   int var[3];            // launch variant of each pass (autotuned, 0 = default)
-  int split;             // FP32: pass 1's z DFT on the tensor cores in split BF16
+  int split;             // FP32, split BF16 on the tensor cores: bit 0 pass 1's z DFT, bit 1 pass 3's x DFT
   int* status;           // device word, bit 0 set when a bounded tensor-core wait expired
   int wait_test;         // test hook: the tensor-core pass issues no MMA and waits 20 ms
 };
@@ -110,6 +110,18 @@ cudaError_t launch_gen_z_tc(const GenArgs& a, cudaStream_t s);
 // work items, gen_z_tc_items per realisation; rep: any member).
 int gen_z_tc_items(const GenArgs& a);
 cudaError_t launch_gen_z_tc_batch(const GenArgs& rep, const BatchMap& m, cudaStream_t s);
+// Pass 3 with the x-axis DFT as split-BF16 tensor-core matrix products
+// (c2r_tc.cu): FP32, single-tile launches, half lengths P0 / 2 with
+// c2r_x_tc_supported; c2r_x_tc_blocks is its CTA count (one FP64 moment pair
+// each).  launch_gen_pass takes it for pass 3 when bit 1 of a.split is set
+// (SCARL_SPLIT_BF16_X).
+bool c2r_x_tc_supported(int N);
+cudaError_t launch_c2r_x_tc(const GenArgs& a, cudaStream_t s);
+int c2r_x_tc_blocks(const GenArgs& a);
+// True when pass 3 of a runs on the tensor cores.
+inline bool c2r_x_tc_used(int dt, const GenArgs& a) {
+  return (a.split & 2) && dt == 4 && a.status && c2r_x_tc_supported(a.P[0] / 2);
+}
 // Blocks one realisation needs in a pass with launch variant v.
 int gen_pass_blocks(int dt, int pass, int v, const GenArgs& a);
 // Number of launch variants of a pass (valid ones depend on the line length).
