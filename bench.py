@@ -629,6 +629,52 @@ def main():
     stx = ctx.profile_stats().get("k_c2r_x_tc")
     ctx.profile(False)
 
+    def timed_fn(fn, n):
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return R.max_over_ranks(e0.elapsed_time(e1) / n, dist, "cuda")
+
+    # ---- the same deck with von Karman nu = 1.5: the power-law amplitude of
+    #      the tensor-core pass 1 (its own SMOOTH grid)
+    vk = dict(DECK, corrMod=2, nu=1.5)
+    s_vk = S.make_sample(**vk)
+    s_vk.seedBase = sample.seedBase
+    lay_vk = S.sample_layout(s_vk, 1, 8, TOPO)
+    P_vk = [int(v) for v in S.pad_size(S.PAD_SMOOTH, 2, vk["corrL"], lay_vk["xStep"], lay_vk["Np"], 1.5,
+                                       PAD_TOL)]
+
+    def step_vk():
+        S.generate_sample(ctx, s_vk, generator=S.GEN_PADDED, dtype=HEAD, nb_procs=8, topo=TOPO,
+                          pad_policy=S.PAD_SMOOTH, pad_tol=PAD_TOL, autotune=True, out=field)
+
+    for _ in range(args.warmup):
+        step_vk()
+    ms_vk = timed_fn(step_vk, args.steps)
+    vk_line = {"value": round(world * npts / (ms_vk * 1e-3) / 1e6, 2), "ms_per_step": round(ms_vk, 4),
+               "padded_grid": P_vk, "corrMod": 2, "nu": 1.5,
+               "precision": "f32 (z DFT: bf16 head/tail products, power-law amplitude)"}
+    # ---- the reference's active generator (gen_std_gauss_FFT: the Gaussian
+    #      spectrum and an unnormalised 3-D DCT-III, FP64) on one tile of the deck
+    Np_t = [int(v) for v in lay["Np"]]
+    xr_t = [float(v) for v in S.tile_geometry(lay, DECK["xMinGlob"], 0)["xRange"]]
+    dct_out = torch.empty(Np_t[0] * Np_t[1] * Np_t[2], dtype=torch.float64, device="cuda")
+
+    def step_dct():
+        S.gen_std_gauss_FFT(ctx, Np_t, xr_t, DECK["corrL"], 1, seed=1, rank=0, out=dct_out)
+
+    step_dct()
+    ms_dct = timed_fn(step_dct, 3)
+    dct_line = {"value": round(world * Np_t[0] * Np_t[1] * Np_t[2] / (ms_dct * 1e-3) / 1e6, 2),
+                "ms_per_tile": round(ms_dct, 3), "tile_points": Np_t,
+                "precision": "f64 (direct DCT-III sums on the CUDA cores)"}
+    del dct_out
+
     # ---- per-kernel device times (separate, profiled steps)
     ctx.profile(True)
     ctx.profile_reset()
@@ -785,6 +831,7 @@ def main():
                 "rel_l2_vs_gpu_fp64": rel, "max_err_vs_gpu_fp64": relmax,
                 "roofline": roof, "tensor_stages": tensor, "kernels": kern, "launch_variants": tuned, "plain_path": plain,
                 "fp32_path": fp32, "fp64_path": fp64, "pow2_grid_path": pow2, "split_x_path": splitx,
+                "von_karman_1_5": vk_line, "literal_dct_tile": dct_line,
                 "speedup_vs_plain_path": round(ms_full / ms, 3),
                 "split_vs_fp32_same_grid": round(ms_f32 / ms, 3),
                 "padding_policy_gain_fp32": round(ms_full / ms_f32, 3),
