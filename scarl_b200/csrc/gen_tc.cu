@@ -88,6 +88,15 @@ __device__ __forceinline__ float2 split_normals(uint32_t a, uint32_t b) {
   return make_float2(-r * c, -r * s);
 }
 
+// b^e for b >= 1 as 2^(e log2 b) on the hardware approximations (lg2.approx,
+// ex2.approx): relative error a few 2^-22 for the exponents of the Matern
+// amplitude (e = -(nu + 3/2) / 2), far below the 2^-17 of the BF16 split.
+__device__ __forceinline__ float pow_split(float b, float e) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e * __log2f(b)));
+  return r;
+}
+
 // Byte offset of element (row, k) in a canonical K-major operand with
 // 16-byte K chunks 128 B apart and 8-row groups sbo apart (rows < 128).
 __device__ __forceinline__ uint32_t kmaj_off(int row, int k, int sbo) {
@@ -219,10 +228,11 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
         if (AMP == AMP_SEPARABLE) { fx = ax[kx] * ay[ky]; }
         else { fx = ax[kx]; fy = 1.f + qx[kx] + qy[ky]; }
       }
+      const float expo = (float)a.expo;
       auto amp = [&](int kz) -> float {
         if (AMP == AMP_SEPARABLE) return fx * zt[kz];
         if (AMP == AMP_RECIP) return __fdividef(fx, fy + zt[kz]);
-        return fx * powf(fy + zt[kz], (float)a.expo);
+        return fx * pow_split(fy + zt[kz], expo);
       };
       // K-major row R1 (tiles of 128 rows are contiguous); K in draw order:
       // draw d (modes k2 = d and d + N2/2) fills K columns 4d .. 4d + 3, so
