@@ -152,7 +152,11 @@ __device__ __forceinline__ void gen_z_body(const GenArgs& a, int bx, int ky) {
 // ---------------------------------------------------------------------------
 // Pass 2: inverse DFT along y, in place, keep y < Ny.
 // ---------------------------------------------------------------------------
-template <typename T, int N, int E, int B>
+// DIRECT: the first stage reads its inputs straight from global memory (no
+// staged copy of the column block); every input is read before the line's
+// last stage stores, which the plan's block barriers order (two or more
+// stages).
+template <typename T, int N, int E, int B, bool DIRECT = false>
 __device__ __forceinline__ void mid_y_body(const GenArgs& a, int bx, int z) {
   using C = cplx_t<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -163,18 +167,7 @@ __device__ __forceinline__ void mid_y_body(const GenArgs& a, int bx, int z) {
   const bool valid = kx < a.Hx;
   C* colblk = static_cast<C*>(a.work) + (size_t)z * a.P[1] * a.Hpad + kx0;
   const size_t pitch = (size_t)a.Hpad;
-  {  // stage the N x B column block: raw[n * B + b], 16-byte async copies
-    constexpr int CPR = B * (int)sizeof(C) / 16;  // chunks per row
-    for (int c = threadIdx.x; c < N * CPR; c += blockDim.x) {
-      const int n = c / CPR, q = c - n * CPR;
-      cp_async16(reinterpret_cast<char*>(sm + n * B) + q * 16,
-                 reinterpret_cast<const char*>(colblk + (size_t)n * pitch) + q * 16);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-  }
   const int Ny = a.Nout[1];
-  auto load = each_load<C, N, E>([&](int ky) -> C { return sm[ky * B + b]; });
   constexpr int RL = last_radix<N, E>();
   C* col = colblk + b;
   auto store = [&](int j, const C* o) {
@@ -185,8 +178,29 @@ __device__ __forceinline__ void mid_y_body(const GenArgs& a, int bx, int z) {
       if (valid && y < Ny) cj[(size_t)(r * (N / RL)) * pitch] = o[r];
     }
   };
-  line_ifft<C, N, E, SmemOrder::BatchFast, B, 0, false, 1>(sm, b, t, static_cast<const C*>(a.tw_y),
-                                                          load, store);
+  if constexpr (DIRECT) {
+    static_assert(StagePlan<N, E>::S >= 2, "direct loads need a barrier before the stores");
+    const C* src = col;
+    auto load = each_load<C, N, E>([&](int ky) -> C {
+      return valid ? src[(size_t)ky * pitch] : mk(T(0), T(0));
+    });
+    line_ifft<C, N, E, SmemOrder::BatchFast, B, 0, false, 1>(sm, b, t, static_cast<const C*>(a.tw_y),
+                                                            load, store);
+  } else {
+    {  // stage the N x B column block: raw[n * B + b], 16-byte async copies
+      constexpr int CPR = B * (int)sizeof(C) / 16;  // chunks per row
+      for (int c = threadIdx.x; c < N * CPR; c += blockDim.x) {
+        const int n = c / CPR, q = c - n * CPR;
+        cp_async16(reinterpret_cast<char*>(sm + n * B) + q * 16,
+                   reinterpret_cast<const char*>(colblk + (size_t)n * pitch) + q * 16);
+      }
+      cp_async_wait_all();
+      __syncthreads();
+    }
+    auto load = each_load<C, N, E>([&](int ky) -> C { return sm[ky * B + b]; });
+    line_ifft<C, N, E, SmemOrder::BatchFast, B, 0, false, 1>(sm, b, t, static_cast<const C*>(a.tw_y),
+                                                            load, store);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -328,16 +342,16 @@ __global__ void __launch_bounds__(B*(N / E)) k_gen_z_batch(const BatchMap m) {
   gen_z_body<T, N, E, B, SPEC>(a, loc % gx, loc / gx);
 }
 
-template <typename T, int N, int E, int B>
+template <typename T, int N, int E, int B, bool DIRECT = false>
 __global__ void __launch_bounds__(B*(N / E)) k_mid_y(const GenArgs a) {
-  mid_y_body<T, N, E, B>(a, blockIdx.x, blockIdx.y);
+  mid_y_body<T, N, E, B, DIRECT>(a, blockIdx.x, blockIdx.y);
 }
-template <typename T, int N, int E, int B>
+template <typename T, int N, int E, int B, bool DIRECT = false>
 __global__ void __launch_bounds__(B*(N / E)) k_mid_y_batch(const BatchMap m) {
   int loc;
   const GenArgs a = m.args[batch_item(m, &loc)];
   const int gx = (a.Hx + B - 1) / B;
-  mid_y_body<T, N, E, B>(a, loc % gx, loc / gx);
+  mid_y_body<T, N, E, B, DIRECT>(a, loc % gx, loc / gx);
 }
 
 template <typename T, int N, int E, int B>

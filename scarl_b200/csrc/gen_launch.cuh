@@ -25,6 +25,12 @@ template <> struct ColVars<double> {
   static constexpr int n = 4;
   static constexpr VarEB v[n] = {{16, 4}, {8, 8}, {8, 4}, {16, 8}};
 };
+// pass 2 with the first stage read straight from global memory (FP32)
+struct ColDirectVars {
+  static constexpr int n = 3;
+  static constexpr VarEB v[n] = {{32, 8}, {16, 8}, {16, 16}};
+};
+template <typename T> constexpr int kDirectVars = std::is_same<T, float>::value ? ColDirectVars::n : 0;
 // pass 3 (contiguous lines, lanes span a line)
 template <typename T> struct RowVars;
 template <> struct RowVars<float> {
@@ -81,10 +87,10 @@ inline cudaError_t run_gen_z_v(const GenArgs& a, const BatchMap* bm, int* blocks
   }
 }
 
-template <typename T, int N, int E0, int B>
+template <typename T, int N, int E0, int B, bool DIRECT = false>
 inline cudaError_t run_mid_y_v(const GenArgs& a, const BatchMap* bm, int* blocks, cudaStream_t s) {
   constexpr int E = eff_E<N, E0>();
-  if constexpr (!variant_ok<T, N, E, B, false>()) {
+  if constexpr (!variant_ok<T, N, E, B, false>() || (DIRECT && StagePlan<N, E>::S < 2)) {
     return cudaErrorInvalidConfiguration;
   } else {
     dim3 grid((a.Hx + B - 1) / B, a.Nout[2], 1);
@@ -94,8 +100,8 @@ inline cudaError_t run_mid_y_v(const GenArgs& a, const BatchMap* bm, int* blocks
     }
     dim3 block(B * (N / E));
     size_t smem = (size_t)B * line_slots<N, E>() * sizeof(cplx_t<T>);
-    if (bm) return launch_k(k_mid_y_batch<T, N, E, B>, dim3(bm->total), block, smem, s, *bm);
-    return launch_k(k_mid_y<T, N, E, B>, grid, block, smem, s, a);
+    if (bm) return launch_k(k_mid_y_batch<T, N, E, B, DIRECT>, dim3(bm->total), block, smem, s, *bm);
+    return launch_k(k_mid_y<T, N, E, B, DIRECT>, grid, block, smem, s, a);
   }
 }
 
@@ -174,6 +180,15 @@ inline cudaError_t run_pass_n(int pass, int v, const GenArgs& a, const BatchMap*
     if (a.spec == SPEC_INJECT)
       return run_gen_z_v<T, N, CV::v[0].E, CV::v[0].B, SPEC_INJECT>(a, bm, nb, s);
     return run_gen_z_v<T, N, CV::v[0].E, CV::v[0].B, SPEC_SHINO>(a, bm, nb, s);
+  }
+  if (pass == 2 && v >= CV::n && v < CV::n + kDirectVars<T>) {
+    if constexpr (tuned_col && kDirectVars<T> > 0) {
+      using DV = ColDirectVars;
+      if (v == CV::n) return run_mid_y_v<T, N, DV::v[0].E, DV::v[0].B, true>(a, bm, nb, s);
+      if (v == CV::n + 1) return run_mid_y_v<T, N, DV::v[1].E, DV::v[1].B, true>(a, bm, nb, s);
+      return run_mid_y_v<T, N, DV::v[2].E, DV::v[2].B, true>(a, bm, nb, s);
+    }
+    return cudaErrorInvalidConfiguration;
   }
   if (pass == 1 || pass == 2) {
     if (v == 0) {

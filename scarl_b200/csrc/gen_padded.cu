@@ -104,6 +104,7 @@ int gen_default_variant(int dt, int pass, const GenArgs& a) {
 
 int gen_variant_count(int dt, int pass) {
   if (pass == 3) return dt == 8 ? RowVars<double>::n : RowVars<float>::n + kShflVars<float>;
+  if (pass == 2 && dt == 4) return ColVars<float>::n + kDirectVars<float>;
   return dt == 8 ? ColVars<double>::n : ColVars<float>::n;
 }
 

@@ -238,6 +238,12 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
       // draw d (modes k2 = d and d + N2/2) fills K columns 4d .. 4d + 3, so
       // two draws make one 16-byte chunk
       const uint32_t rowoff = (uint32_t)((R1 >> 3) * Cfg::SBO1 + (R1 & 7) * 16);
+      // the Philox round keys and stream in registers for the item's draws
+      // (a batch's argument block lives in shared memory beside the operands)
+      uint32_t kr[20];
+#pragma unroll
+      for (int r = 0; r < 20; ++r) kr[r] = a.ks[r];
+      const uint32_t strm = a.stream;
       auto put = [&](const float* v, int chunk) {
         uint4 h, t;
         tc::split2(v[0], v[1], h.x, t.x);
@@ -256,7 +262,7 @@ __device__ __forceinline__ void gen_z_tc_body(const GenArgs& a0, const GenArgs* 
           const int kz0 = s_k1 + N1 * (d0 + e);
           if (valid) {
             const uint64_t c = (uint64_t)l + mz * (uint64_t)kz0;
-            const u32x4 o = philox4x32_10_ks({(uint32_t)c, (uint32_t)(c >> 32), a.stream, 0u}, a.ks);
+            const u32x4 o = philox4x32_10_ks({(uint32_t)c, (uint32_t)(c >> 32), strm, 0u}, kr);
             const float2 x0 = split_normals(o.x, o.y);
             const float2 x1 = split_normals(o.z, o.w);
             const float A0 = amp(kz0), A1 = amp(kz0 + N / 2);

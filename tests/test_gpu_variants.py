@@ -1,6 +1,7 @@
 """Every launch variant of the three generator passes (the autotuner's
-search space) against the oracle, in FP64 (rel-L2 <= 1e-12) and FP32
-(<= 1e-5), for line lengths 128..2048 on each pass."""
+search space, including the FP32 pass-2 variants that read their first stage
+straight from global memory) against the oracle, in FP64 (rel-L2 <= 1e-12)
+and FP32 (<= 1e-5), for line lengths 128..2048 and 384 on each pass."""
 import functools
 
 import numpy as np
@@ -11,7 +12,7 @@ from scarl_b200 import _lib
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [128, 256, 512, 1024, 2048]
+SIZES = [128, 256, 384, 512, 1024, 2048]
 
 
 def _shape(pass_, N):
@@ -39,7 +40,7 @@ def test_every_variant_matches_oracle(ctx, dtype, tol, pass_, N):
     Np, P = _shape(pass_, N)
     Nl = (P[2], P[1], P[0] // 2)[pass_ - 1]
     ref = _ref(pass_, N)
-    nvar = {(S.F32, 3): 8, (S.F64, 3): 3, (S.F32, 1): 6, (S.F32, 2): 6,
+    nvar = {(S.F32, 3): 8, (S.F64, 3): 3, (S.F32, 1): 6, (S.F32, 2): 9,
             (S.F64, 1): 4, (S.F64, 2): 4}[(dtype, pass_)]
     ran = 0
     try:
@@ -68,7 +69,7 @@ def test_autotune_picks_valid_variants_and_caches(ctx, tmp_path):
     assert len(lines) >= 12
     for pass_, N in ((1, 256), (2, 256), (3, 128)):
         v = ctx.tune_get(S.F32, pass_, N)
-        assert 0 <= v < (8 if pass_ == 3 else 6)
+        assert 0 <= v < {1: 6, 2: 9, 3: 8}[pass_]
     # a tuned context still generates the same field
     from oracle import oracle as O
     ref = O.gen_padded((40, 30, 20), (64, 64, 64), (1, 1, 1), (5, 5, 5), 3, 0.5, 1, seed=1)
