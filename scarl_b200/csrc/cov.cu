@@ -16,6 +16,15 @@
 //   S(h) = (1/M) sum_k |Y_k|^2 e^{-2 pi i k h / M},
 // equals the linear lag sum for h <= M - L_d (Wiener-Khinchin); the cosine
 // sum over k is formed in FP64 by k_cov_lags.
+//
+// FP32 fields whose lines and line groups start on 16-byte boundaries (L_0 a
+// multiple of 4; column layouts with a group width B that is a multiple of 4
+// and divides L_0) take the staged form: each line group's values are copied
+// into a shared-memory input buffer by 16-byte cp.async copies, and the next
+// group's copies are issued as soon as the current group's first-stage
+// values are in registers, so that the loads' latency overlaps the transform
+// and the power sums (no register prefetch).  Same values, same order: the
+// staged and the direct form give identical sums.
 #include <algorithm>
 
 #include "fft_engine.cuh"
@@ -69,7 +78,12 @@ struct CovGeom {
   double* partial; // gridDim.x * (N + 1)
 };
 
-template <typename T, int N, bool ROW>
+// Staged form: input buffer floats (B lines of L values, or L rows of B values).
+template <int N, bool ROW> __host__ __device__ constexpr int cov_in_floats(int L) {
+  return cov_B<float, N, ROW>() * L;
+}
+
+template <typename T, int N, bool ROW, bool ASYNC = false>
 __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>())
     k_axis_power(const CovGeom g) {
   using C = cplx_t<T>;
@@ -123,11 +137,56 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
         dst[q * R1 + r] = mk(val(2 * k), val(2 * k + 1));
       }
   };
-  C nxt[PF ? E : 1];
-  if constexpr (PF) fetch(blockIdx.x, nxt);
+  // staged form: the group's values in the input buffer after the twiddles
+  float* inb = reinterpret_cast<float*>(sm + cov_rows<T, N, ROW>() + 2 * N);
+  auto issue = [&](int64_t grp) {  // 16-byte copies of group grp (every thread)
+    const int64_t l0 = grp * B;
+    if constexpr (ROW) {
+      const int cpl = g.n / 4;  // chunks a line
+      for (int c = (int)threadIdx.x; c < B * cpl; c += (int)blockDim.x) {
+        const int bb = c / cpl, qq = c - bb * cpl;
+        const int64_t l = l0 + bb;
+        if (l >= g.nlines) continue;
+        const float* src = static_cast<const float*>(g.f) + (l % g.na) * g.sa + (l / g.na) * g.sb + 4 * qq;
+        cp_async16(inb + bb * g.n + 4 * qq, src);
+      }
+    } else {
+      constexpr int cpr = B >= 4 ? B / 4 : 1;  // chunks a row (staged_ok: B a multiple of 4)
+      const float* base = static_cast<const float*>(g.f) + (l0 % g.na) * g.sa + (l0 / g.na) * g.sb;
+      for (int c = (int)threadIdx.x; c < g.n * cpr; c += (int)blockDim.x) {
+        const int i = c / cpr, qq = c - i * cpr;
+        cp_async16(inb + i * B + 4 * qq, base + (int64_t)i * g.st + 4 * qq);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  auto fetch_staged = [&](int64_t grp, C* dst) {
+    const int64_t l = grp * B + b;
+    const bool valid = l < g.nlines;
+    auto val = [&](int i) -> T {
+      if (!valid || i >= g.n) return T(0);
+      return (T)(ROW ? inb[b * g.n + i] : inb[i * B + b]) - mu;
+    };
+#pragma unroll
+    for (int q = 0; q < E / R1; ++q)
+#pragma unroll
+      for (int r = 0; r < R1; ++r) {
+        const int k = t + TPL * q + r * (N / R1);
+        dst[q * R1 + r] = mk(val(2 * k), val(2 * k + 1));
+      }
+  };
+  C nxt[PF && !ASYNC ? E : 1];
+  if constexpr (ASYNC) issue(blockIdx.x);
+  else if constexpr (PF) fetch(blockIdx.x, nxt);
   for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     C cur[E];
-    if constexpr (PF) {
+    if constexpr (ASYNC) {
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+      __syncthreads();  // every thread's copies of this group have landed
+      fetch_staged(grp, cur);
+      __syncthreads();  // every thread has read the input buffer
+      if (grp + gridDim.x < ngroups) issue(grp + gridDim.x);
+    } else if constexpr (PF) {
 #pragma unroll
       for (int i = 0; i < E; ++i) cur[i] = nxt[i];
       if (grp + gridDim.x < ngroups) fetch(grp + gridDim.x, nxt);
@@ -180,10 +239,21 @@ template <typename T, int N, bool ROW> size_t cov_smem() {
   return ((size_t)cov_rows<T, N, ROW>() + (sizeof(T) == 4 ? 2 * N : 0)) * sizeof(cplx_t<T>);
 }
 
-template <typename T, int N, bool ROW>
-cudaError_t run_power(CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
-  auto kern = k_axis_power<T, N, ROW>;
-  const size_t smem = cov_smem<T, N, ROW>();
+// The staged form serves FP32 lines whose copies are 16-byte aligned: L_0 a
+// multiple of 4; a column layout's group width B a multiple of 4 dividing
+// L_0 (groups never wrap across x); the buffer fitting two blocks an SM.
+template <typename T, int N, bool ROW> bool staged_ok(const CovGeom& g, int L0) {
+  if (sizeof(T) != 4 || L0 % 4 != 0) return false;
+  constexpr int B = cov_B<T, N, ROW>();
+  if (!ROW && (B % 4 != 0 || L0 % B != 0)) return false;
+  const size_t smem = cov_smem<T, N, ROW>() + (size_t)cov_in_floats<N, ROW>(g.n) * 4;
+  return smem <= 110 * 1024;
+}
+
+template <typename T, int N, bool ROW, bool ASYNC>
+cudaError_t run_power_k(CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
+  auto kern = k_axis_power<T, N, ROW, ASYNC>;
+  const size_t smem = cov_smem<T, N, ROW>() + (ASYNC ? (size_t)cov_in_floats<N, ROW>(g.n) * 4 : 0);
   const int threads = cov_threads<T, N, ROW>();
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -206,25 +276,37 @@ cudaError_t run_power(CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <typename T, int N, bool ROW>
+cudaError_t run_power(CovGeom g, int L0, int want_blocks, int* blocks, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    // the query (g.f == nullptr) and the launch pick the same form, so the
+    // partial sums sized from the query match the launch's grid
+    const bool aligned = g.f == nullptr || (reinterpret_cast<uintptr_t>(g.f) & 15) == 0;
+    if (staged_ok<T, N, ROW>(g, L0) && aligned)
+      return run_power_k<T, N, ROW, true>(g, want_blocks, blocks, s);
+  }
+  return run_power_k<T, N, ROW, false>(g, want_blocks, blocks, s);
+}
+
 template <typename T, bool ROW>
-cudaError_t run_power_n(int N, CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
+cudaError_t run_power_n(int N, CovGeom g, int L0, int want_blocks, int* blocks, cudaStream_t s) {
   switch (N) {
-    case 4: return run_power<T, 4, ROW>(g, want_blocks, blocks, s);
-    case 8: return run_power<T, 8, ROW>(g, want_blocks, blocks, s);
-    case 16: return run_power<T, 16, ROW>(g, want_blocks, blocks, s);
-    case 32: return run_power<T, 32, ROW>(g, want_blocks, blocks, s);
-    case 64: return run_power<T, 64, ROW>(g, want_blocks, blocks, s);
-    case 128: return run_power<T, 128, ROW>(g, want_blocks, blocks, s);
-    case 256: return run_power<T, 256, ROW>(g, want_blocks, blocks, s);
-    case 512: return run_power<T, 512, ROW>(g, want_blocks, blocks, s);
-    case 1024: return run_power<T, 1024, ROW>(g, want_blocks, blocks, s);
-    case 2048: return run_power<T, 2048, ROW>(g, want_blocks, blocks, s);
-    case 320: return run_power<T, 320, ROW>(g, want_blocks, blocks, s);
-    case 384: return run_power<T, 384, ROW>(g, want_blocks, blocks, s);
-    case 640: return run_power<T, 640, ROW>(g, want_blocks, blocks, s);
-    case 768: return run_power<T, 768, ROW>(g, want_blocks, blocks, s);
-    case 1280: return run_power<T, 1280, ROW>(g, want_blocks, blocks, s);
-    case 1536: return run_power<T, 1536, ROW>(g, want_blocks, blocks, s);
+    case 4: return run_power<T, 4, ROW>(g, L0, want_blocks, blocks, s);
+    case 8: return run_power<T, 8, ROW>(g, L0, want_blocks, blocks, s);
+    case 16: return run_power<T, 16, ROW>(g, L0, want_blocks, blocks, s);
+    case 32: return run_power<T, 32, ROW>(g, L0, want_blocks, blocks, s);
+    case 64: return run_power<T, 64, ROW>(g, L0, want_blocks, blocks, s);
+    case 128: return run_power<T, 128, ROW>(g, L0, want_blocks, blocks, s);
+    case 256: return run_power<T, 256, ROW>(g, L0, want_blocks, blocks, s);
+    case 512: return run_power<T, 512, ROW>(g, L0, want_blocks, blocks, s);
+    case 1024: return run_power<T, 1024, ROW>(g, L0, want_blocks, blocks, s);
+    case 2048: return run_power<T, 2048, ROW>(g, L0, want_blocks, blocks, s);
+    case 320: return run_power<T, 320, ROW>(g, L0, want_blocks, blocks, s);
+    case 384: return run_power<T, 384, ROW>(g, L0, want_blocks, blocks, s);
+    case 640: return run_power<T, 640, ROW>(g, L0, want_blocks, blocks, s);
+    case 768: return run_power<T, 768, ROW>(g, L0, want_blocks, blocks, s);
+    case 1280: return run_power<T, 1280, ROW>(g, L0, want_blocks, blocks, s);
+    case 1536: return run_power<T, 1536, ROW>(g, L0, want_blocks, blocks, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -247,11 +329,11 @@ CovGeom geom(const void* f, const int L[3], int dir, double mu, const void* tw, 
   return g;
 }
 
-cudaError_t dispatch(int dt, int dir, int N, CovGeom g, int want, int* blocks, cudaStream_t s) {
-  if (dt == 8) return dir == 0 ? run_power_n<double, true>(N, g, want, blocks, s)
-                               : run_power_n<double, false>(N, g, want, blocks, s);
-  return dir == 0 ? run_power_n<float, true>(N, g, want, blocks, s)
-                  : run_power_n<float, false>(N, g, want, blocks, s);
+cudaError_t dispatch(int dt, int dir, int N, CovGeom g, int L0, int want, int* blocks, cudaStream_t s) {
+  if (dt == 8) return dir == 0 ? run_power_n<double, true>(N, g, L0, want, blocks, s)
+                               : run_power_n<double, false>(N, g, L0, want, blocks, s);
+  return dir == 0 ? run_power_n<float, true>(N, g, L0, want, blocks, s)
+                  : run_power_n<float, false>(N, g, L0, want, blocks, s);
 }
 
 // P_k = sum over blocks of the partial power (one thread per bin).
@@ -290,7 +372,7 @@ __global__ void k_cov_lags(const double* __restrict__ bins, int N, const double2
 int axis_power_blocks(int dt, const int L[3], int dir, int N) {
   int nb = -1;
   CovGeom g = geom(nullptr, L, dir, 0.0, nullptr, nullptr);
-  if (dispatch(dt, dir, N, g, -1, &nb, nullptr) != cudaSuccess) {
+  if (dispatch(dt, dir, N, g, L[0], -1, &nb, nullptr) != cudaSuccess) {
     cudaGetLastError();
     return -1;
   }
@@ -300,7 +382,7 @@ int axis_power_blocks(int dt, const int L[3], int dir, int N) {
 cudaError_t launch_axis_power(int dt, const void* f, const int L[3], int dir, int N, double mu,
                               const void* tw, double* partial, int nblocks, cudaStream_t s) {
   CovGeom g = geom(f, L, dir, mu, tw, partial);
-  return dispatch(dt, dir, N, g, nblocks, nullptr, s);
+  return dispatch(dt, dir, N, g, L[0], nblocks, nullptr, s);
 }
 
 cudaError_t launch_cov_lags(const double* partial, int nblocks, int N, int maxlag,

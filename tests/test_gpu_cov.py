@@ -56,6 +56,27 @@ def test_axis_cov_device_input_and_limits(ctx, oracle):
         S.axis_cov(ctx, np.zeros((4096, 3, 2), order="F"), (4096, 3, 2), 1)  # L + maxlag > 4096
 
 
+@pytest.mark.parametrize("shape,maxlag", [((64, 48, 33), 30), ((128, 64, 40), 20), ((600, 40, 36), 30)])
+def test_axis_cov_staged_equals_direct(ctx, oracle, shape, maxlag):
+    """FP32 fields whose lines start on 16-byte boundaries take the staged
+    power pass (cp.async copies into shared memory); the same values one
+    float off the boundary take the direct one.  Same grid, same order: the
+    covariances are identical, and within the FP32 tolerance of the oracle."""
+    torch = pytest.importorskip("torch")
+    f = _field(shape, 7).astype(np.float32)
+    flat = torch.from_numpy(f.reshape(-1, order="F")).cuda()
+    buf = torch.empty(flat.numel() + 4, dtype=torch.float32, device="cuda")
+    buf[1:1 + flat.numel()] = flat
+    off = buf[1:1 + flat.numel()]  # 4 bytes past a 16-byte boundary
+    assert flat.data_ptr() % 16 == 0 and off.data_ptr() % 16 == 4
+    m1, v1, c1 = S.axis_cov(ctx, flat, shape, maxlag)
+    m2, v2, c2 = S.axis_cov(ctx, off, shape, maxlag)
+    assert m1 == m2 and v1 == v2
+    np.testing.assert_array_equal(c1, c2)
+    _, c_ref = oracle.axis_cov(f.astype(np.float64), maxlag)
+    np.testing.assert_allclose(c1, c_ref, rtol=0, atol=2e-6 * c_ref[0, 0])
+
+
 def _blend_kappa(Np, No, T, L, maxlag):
     """Pair-averaged sum over tiles of sqrt(w(x) w(x + h)) of the 1-D
     partition-of-unity weights along one axis (the factor by which blending
