@@ -23,8 +23,10 @@
 // into a shared-memory input buffer by 16-byte cp.async copies, and the next
 // group's copies are issued as soon as the current group's first-stage
 // values are in registers, so that the loads' latency overlaps the transform
-// and the power sums (no register prefetch).  Same values, same order: the
-// staged and the direct form give identical sums.
+// and the power sums (no register prefetch); x lines are then transformed
+// with lanes across lines, like the column layouts (fewer shared-memory bank
+// conflicts than the line-fast layout).  Same values, same order: the staged
+// and the direct form give identical sums.
 #include <algorithm>
 
 #include "fft_engine.cuh"
@@ -78,9 +80,10 @@ struct CovGeom {
   double* partial; // gridDim.x * (N + 1)
 };
 
-// Staged form: input buffer floats (B lines of L values, or L rows of B values).
+// Staged form: input buffer floats (B lines of L values 16 bytes more than L
+// apart, or L rows of B values).
 template <int N, bool ROW> __host__ __device__ constexpr int cov_in_floats(int L) {
-  return cov_B<float, N, ROW>() * L;
+  return cov_B<float, N, ROW>() * (L + (ROW ? 4 : 0));
 }
 
 template <typename T, int N, bool ROW, bool ASYNC = false>
@@ -92,12 +95,16 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
   constexpr int TPL = N / E;
   constexpr int NT = B * TPL;
   constexpr int QB = (N + NT) / NT;  // bins per thread (bins 0..N)
-  constexpr SmemOrder O = ROW ? SmemOrder::LineFast : SmemOrder::BatchFast;
-  constexpr int LS = ROW ? line_slots<N, E>() : 0;
+  // lanes along a line (line-fast shared layout) only in the direct form of
+  // x lines; the staged form transforms x lines like the column layouts
+  // (lanes across lines), reading them from a line-major input buffer
+  constexpr bool LROW = ROW && !ASYNC;
+  constexpr SmemOrder O = LROW ? SmemOrder::LineFast : SmemOrder::BatchFast;
+  constexpr int LS = LROW ? line_slots<N, E>() : 0;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  const int b = ROW ? (int)threadIdx.x / TPL : (int)threadIdx.x % B;
-  const int t = ROW ? (int)threadIdx.x % TPL : (int)threadIdx.x / B;
+  const int b = LROW ? (int)threadIdx.x / TPL : (int)threadIdx.x % B;
+  const int t = LROW ? (int)threadIdx.x % TPL : (int)threadIdx.x / B;
   const T* f = static_cast<const T*>(g.f);
   // FP32: the 2N twiddles e^{2 pi i m / M} in shared memory (once per block)
   constexpr bool TWS = sizeof(T) == 4;
@@ -148,7 +155,7 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
         const int64_t l = l0 + bb;
         if (l >= g.nlines) continue;
         const float* src = static_cast<const float*>(g.f) + (l % g.na) * g.sa + (l / g.na) * g.sb + 4 * qq;
-        cp_async16(inb + bb * g.n + 4 * qq, src);
+        cp_async16(inb + bb * (g.n + 4) + 4 * qq, src);  // lines 16 bytes more than L apart
       }
     } else {
       constexpr int cpr = B >= 4 ? B / 4 : 1;  // chunks a row (staged_ok: B a multiple of 4)
@@ -165,7 +172,7 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
     const bool valid = l < g.nlines;
     auto val = [&](int i) -> T {
       if (!valid || i >= g.n) return T(0);
-      return (T)(ROW ? inb[b * g.n + i] : inb[i * B + b]) - mu;
+      return (T)(ROW ? inb[b * (g.n + 4) + i] : inb[i * B + b]) - mu;
     };
 #pragma unroll
     for (int q = 0; q < E / R1; ++q)
