@@ -42,10 +42,18 @@ template <> struct RowVars<double> {
   static constexpr VarEB v[n] = {{16, 4}, {8, 8}, {8, 4}};
 };
 
+// Every radix of the plan within the in-register DFTs (powers of two up to
+// 32, or 3, 5, 7).
+template <int N, int E> __host__ __device__ constexpr bool radices_ok() {
+  for (int s = 0; s < StagePlan<N, E>::S; ++s)
+    if (StagePlan<N, E>::radix(s) > 32) return false;
+  return true;
+}
+
 // E: the effective values per thread (eff_E of the variant).
 template <typename T, int N, int Ee, int B, bool ROW>
 __host__ __device__ constexpr bool variant_ok() {
-  if (!StagePlan<N, Ee>::valid()) return false;
+  if (!StagePlan<N, Ee>::valid() || !radices_ok<N, Ee>()) return false;
   constexpr int threads = B * (N / Ee);
   constexpr size_t smem = ROW ? c2r_smem<T, N, Ee, B>() : (size_t)B * line_slots<N, Ee>() * sizeof(cplx_t<T>);
   return threads >= 1 && threads <= 1024 && smem <= 220 * 1024 && (N % Ee) == 0;

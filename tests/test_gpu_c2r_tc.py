@@ -99,3 +99,11 @@ def test_tc_pass3_headline_deck_vs_oracle(ctx, oracle, pad):
     assert abs(mom[0] - s1) <= 1e-9 * abs(s1) and abs(mom[1] - s2) <= 1e-9 * s2, (mom, s1, s2)
     del y
     torch.cuda.empty_cache()
+
+
+def test_tc_pass3_flag_needs_fp32(ctx):
+    """SCARL_SPLIT_BF16_X applies to SCARL_F32 only."""
+    from scarl_b200 import _lib
+    with pytest.raises(S.ScarlError) as e:
+        S.gen_padded(ctx, (8, 8, 8), (1, 1, 1), (2, 2, 2), 1, dtype=S.F64 | S.SPLIT_BF16_X)
+    assert e.value.code == _lib.EINVAL
