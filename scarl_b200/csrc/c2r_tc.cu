@@ -1,8 +1,8 @@
 // c2r_tc.cu -- pass 3 of the padded generator (Hermitian C2R along x, crop,
 // blend epilogue) with the x DFT on the tensor cores in split BF16: the FP32
 // output of scarl_gen_padded / scarl_generate_sample when the caller asks for
-// SCARL_F32 | SCARL_SPLIT_BF16 and the half length N = P0 / 2 factors as
-// N1 x N2 with N2 = 32 or 16 and N1 <= 8.
+// SCARL_F32 | SCARL_SPLIT_BF16_X and the half length N = P0 / 2 factors as
+// N1 x N2 with N2 = 32 or 16 and N1 <= 8 (single-tile launches).
 //
 // A line of N + 1 half-spectrum values X[k] (a row of the pass-2 output) is
 // pre-combined into the complex sequence
@@ -25,8 +25,8 @@
 // the tensor core, on global loads and on its block barriers; four
 // independent CTAs keep the SM issuing), walk items of 16 consecutive lines
 // of the tile.  Each thread builds one stage-1 row from the line in global
-// memory (read once through the read-only path; X[N - k] comes from the
-// same line).  The epilogue's per-line tables (output base, y-z flags,
+// memory through the read-only path (every value is read twice, as X[k] by
+// one row and as X[N - k] by another; the second read hits the cache).  The epilogue's per-line tables (output base, y-z flags,
 // s_y s_z) are read into shared memory while the operand is built.  The
 // epilogue (crop, or partition-of-unity blend into the global field with the
 // marginal transform, and the FP64 moment sums; the same arithmetic as the
