@@ -354,7 +354,7 @@ int check_status(scarl_ctx* ctx) {
   CK(cudaMemcpy(&st, ctx->status.p, sizeof st, cudaMemcpyDeviceToHost));
   if (st == 0) return SCARL_OK;
   CK(cudaMemset(ctx->status.p, 0, sizeof st));
-  return fail(ctx, SCARL_ETIMEOUT, "a bounded tensor-core wait expired; the output is invalid");
+  return fail(ctx, SCARL_ETIMEOUT, "a bounded tensor-core or copy wait expired; the output is invalid");
 }
 
 // Device -> pageable host copy through the pinned ring: the DMA fills the
@@ -3154,6 +3154,7 @@ static int axis_cov_impl(scarl_ctx* ctx, const void* field, int dtype, const int
   }
   RC(ensure(ctx, ctx->t1, pbytes));
   RC(ensure(ctx, ctx->t2, (size_t)(2048 + 1) * 8 + (size_t)3 * H * 8));
+  RC(ensure_status(ctx));  // the bounded copy waits of the power pass report here
   double* bins = (double*)ctx->t2.p;
   double* S = bins + 2048 + 1;
   for (int d = 0; d < 3; ++d) {
@@ -3163,7 +3164,8 @@ static int axis_cov_impl(scarl_ctx* ctx, const void* field, int dtype, const int
     RC(twiddles(ctx, 2 * Nc[d], 8, &tw64));
     {
       Prof p(ctx, "k_axis_power");
-      CK(launch_axis_power(dtype, dev, L, d, Nc[d], mu, tw, (double*)ctx->t1.p, nblk[d], ctx->stream));
+      CK(launch_axis_power(dtype, dev, L, d, Nc[d], mu, tw, (double*)ctx->t1.p, nblk[d], ctx->stream,
+                           (int*)ctx->status.p));
     }
     {
       Prof p(ctx, "k_cov_lags", 2);
@@ -3175,6 +3177,7 @@ static int axis_cov_impl(scarl_ctx* ctx, const void* field, int dtype, const int
   CK(cudaMemcpyAsync(hs.data(), S, hs.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->d2h += hs.size() * 8;
+  RC(check_status(ctx));
   for (int d = 0; d < 3; ++d)
     for (int lag = 0; lag < H; ++lag) {
       const double pairs = (double)(L[d] - lag) * (double)(n / (size_t)L[d]);

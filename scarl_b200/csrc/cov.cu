@@ -20,17 +20,25 @@
 // FP32 fields whose lines and line groups start on 16-byte boundaries (L_0 a
 // multiple of 4; column layouts with a group width B that is a multiple of 4
 // and divides L_0) take the staged form: each line group's values are copied
-// into a shared-memory input buffer by 16-byte cp.async copies, and the next
-// group's copies are issued as soon as the current group's first-stage
-// values are in registers, so that the loads' latency overlaps the transform
-// and the power sums (no register prefetch); x lines are then transformed
-// with lanes across lines, like the column layouts (fewer shared-memory bank
-// conflicts than the line-fast layout).  Same values, same order: the staged
-// and the direct form give identical sums.
+// into a shared-memory input buffer by the TMA unit (one cp.async.bulk a line
+// of x; for y and z lines one cp.async.bulk.tensor a box of B x up to 256
+// rows through a tensor map of the field, issued by one thread and completing
+// on an mbarrier with a bounded wait), and the next group's copies are issued
+// as soon as the current group's first-stage values are in registers, so
+// that the loads' latency overlaps the transform and the power sums; x lines
+// are then transformed with lanes across lines, like the column layouts
+// (fewer shared-memory bank conflicts than the line-fast layout).  Without a
+// status word or a tensor map the same staging uses every thread's 16-byte
+// cp.async.  Same values, same order: the staged and the direct form give
+// identical sums.
+#include <cuda.h>
+
 #include <algorithm>
+#include <cstring>
 
 #include "fft_engine.cuh"
 #include "scarl_internal.h"
+#include "tc_sm100.cuh"
 
 namespace scarl {
 
@@ -78,17 +86,32 @@ struct CovGeom {
   double mu;
   const void* tw;  // e^{2 pi i m / M}, m < M, working precision
   double* partial; // gridDim.x * (N + 1)
+  int* status;     // device word, bit 0 set when a bounded copy wait expired (TMA form)
+  int box;         // TMA form, column layouts: rows a tensor box (<= 256)
+  int dir;         // line axis (0 x, 1 y, 2 z)
 };
 
 // Staged form: input buffer floats (B lines of L values 16 bytes more than L
-// apart, or L rows of B values).
-template <int N, bool ROW> __host__ __device__ constexpr int cov_in_floats(int L) {
-  return cov_B<float, N, ROW>() * (L + (ROW ? 4 : 0));
+// apart, or L rows of B values, rounded up to whole tensor boxes of `box`
+// rows in the TMA form); 16 bytes for the copies' mbarrier follow it.
+template <int N, bool ROW> __host__ __device__ constexpr int cov_in_floats(int L, int box = 1) {
+  return ROW ? cov_B<float, N, ROW>() * (L + 4) : cov_B<float, N, ROW>() * ((L + box - 1) / box) * box;
+}
+// Byte offset of the staged form's input buffer (after the transform's rows
+// and the twiddles), 128-byte aligned for the tensor copies.
+template <typename T, int N, bool ROW> __host__ __device__ constexpr int cov_in_off() {
+  return ((cov_rows<T, N, ROW>() + 2 * N) * (int)sizeof(cplx_t<T>) + 127) / 128 * 128;
 }
 
-template <typename T, int N, bool ROW, bool ASYNC = false>
+constexpr uint64_t kCopyWaitNs = 1000000000ull;  // 1 s per group's copies (TMA form)
+
+// ASYNC: the staged form.  TMA (with ASYNC): the group's copies are bulk
+// copies by the TMA unit issued by thread 0 (one cp.async.bulk a line of x,
+// one cp.async.bulk.tensor a box of a column group through tmap) completing
+// on an mbarrier, instead of every thread's 16-byte cp.async.
+template <typename T, int N, bool ROW, bool ASYNC = false, bool TMA = false>
 __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>())
-    k_axis_power(const CovGeom g) {
+    k_axis_power(const CovGeom g, const __grid_constant__ CUtensorMap tmap) {
   using C = cplx_t<T>;
   constexpr int E = cov_E<T, N>();
   constexpr int B = cov_B<T, N, ROW>();
@@ -145,7 +168,45 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
       }
   };
   // staged form: the group's values in the input buffer after the twiddles
-  float* inb = reinterpret_cast<float*>(sm + cov_rows<T, N, ROW>() + 2 * N);
+  float* inb = reinterpret_cast<float*>(smraw + cov_in_off<T, N, ROW>());
+  // TMA form: the mbarrier after the input buffer (128-byte aligned region)
+  const uint32_t cbar = tc::smem_u32(inb + (ROW ? B * (g.n + 4) : ((g.n + g.box - 1) / g.box) * g.box * B));
+  auto issue_tma = [&](int64_t grp) {  // thread 0: the group's bulk copies
+    const int64_t l0 = grp * B;
+    tc::fence_smem_to_async();
+    if constexpr (ROW) {
+      const int nv = (int)(g.nlines - l0 < B ? g.nlines - l0 : B);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cbar),
+                   "r"((uint32_t)(nv * g.n * 4))
+                   : "memory");
+      for (int bb = 0; bb < nv; ++bb) {
+        const int64_t l = l0 + bb;
+        const float* src = static_cast<const float*>(g.f) + (l % g.na) * g.sa + (l / g.na) * g.sb;
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                tc::smem_u32(inb + bb * (g.n + 4))),
+            "l"(src), "r"((uint32_t)(g.n * 4)), "r"(cbar)
+            : "memory");
+      }
+    } else {
+      const int nbox = (g.n + g.box - 1) / g.box;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cbar),
+                   "r"((uint32_t)(nbox * g.box * B * 4))
+                   : "memory");
+      // coordinates (x, y, z) of the box: x = first line's x (a multiple of
+      // B, so 16-byte aligned), the line axis stepping by box rows
+      const int x0 = (int)(l0 % g.na), o = (int)(l0 / g.na);
+      const bool ydir = g.dir == 1;  // y lines: the other axis is z; z lines: y
+      for (int r = 0; r < nbox; ++r) {
+        const int c1 = ydir ? r * g.box : o, c2 = ydir ? o : r * g.box;
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(tc::smem_u32(inb + r * g.box * B)),
+            "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(x0), "r"(c1), "r"(c2), "r"(cbar)
+            : "memory");
+      }
+    }
+  };
   auto issue = [&](int64_t grp) {  // 16-byte copies of group grp (every thread)
     const int64_t l0 = grp * B;
     if constexpr (ROW) {
@@ -183,11 +244,35 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
       }
   };
   C nxt[PF && !ASYNC ? E : 1];
-  if constexpr (ASYNC) issue(blockIdx.x);
-  else if constexpr (PF) fetch(blockIdx.x, nxt);
+  uint32_t cphase = 0;
+  bool pending = false;  // thread 0, TMA form: copies issued and not yet waited for
+  if constexpr (TMA) {
+    if (threadIdx.x == 0) tc::mbar_init(cbar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && (int64_t)blockIdx.x < ngroups) {
+      issue_tma(blockIdx.x);
+      pending = true;
+    }
+  } else if constexpr (ASYNC) {
+    issue(blockIdx.x);
+  } else if constexpr (PF) {
+    fetch(blockIdx.x, nxt);
+  }
   for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     C cur[E];
-    if constexpr (ASYNC) {
+    if constexpr (TMA) {
+      const bool ok = tc::mbar_wait(cbar, cphase, kCopyWaitNs);
+      if (!__syncthreads_and(ok)) break;  // reported after the loop
+      cphase ^= 1;
+      if (threadIdx.x == 0) pending = false;
+      fetch_staged(grp, cur);
+      tc::fence_smem_to_async();  // this thread's reads before the next copies' writes
+      __syncthreads();            // every thread has read the input buffer
+      if (threadIdx.x == 0 && grp + gridDim.x < ngroups) {
+        issue_tma(grp + gridDim.x);
+        pending = true;
+      }
+    } else if constexpr (ASYNC) {
       asm volatile("cp.async.wait_all;\n" ::: "memory");
       __syncthreads();  // every thread's copies of this group have landed
       fetch_staged(grp, cur);
@@ -235,6 +320,14 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
     }
     __syncthreads();
   }
+  if constexpr (TMA) {
+    // a group's copies did not land in time: report, and give them one more
+    // bounded wait (they write this block's shared memory)
+    if (threadIdx.x == 0 && pending) {
+      atomicOr(g.status, 1);
+      tc::mbar_wait(cbar, cphase, kCopyWaitNs);
+    }
+  }
 #pragma unroll
   for (int q = 0; q < QB; ++q) {
     const int k = (int)threadIdx.x + NT * q;
@@ -245,6 +338,11 @@ __global__ void __launch_bounds__(cov_threads<T, N, ROW>(), cov_minb<T, N, ROW>(
 template <typename T, int N, bool ROW> size_t cov_smem() {
   return ((size_t)cov_rows<T, N, ROW>() + (sizeof(T) == 4 ? 2 * N : 0)) * sizeof(cplx_t<T>);
 }
+// The staged form's dynamic shared memory: rows, twiddles, the input buffer
+// and its mbarrier.
+template <typename T, int N, bool ROW> size_t cov_smem_staged(const CovGeom& g) {
+  return (size_t)cov_in_off<T, N, ROW>() + (size_t)cov_in_floats<N, ROW>(g.n, g.box) * 4 + 16;
+}
 
 // The staged form serves FP32 lines whose copies are 16-byte aligned: L_0 a
 // multiple of 4; a column layout's group width B a multiple of 4 dividing
@@ -253,14 +351,51 @@ template <typename T, int N, bool ROW> bool staged_ok(const CovGeom& g, int L0) 
   if (sizeof(T) != 4 || L0 % 4 != 0) return false;
   constexpr int B = cov_B<T, N, ROW>();
   if (!ROW && (B % 4 != 0 || L0 % B != 0)) return false;
-  const size_t smem = cov_smem<T, N, ROW>() + (size_t)cov_in_floats<N, ROW>(g.n) * 4;
-  return smem <= 110 * 1024;
+  return cov_smem_staged<T, N, ROW>(g) <= 110 * 1024;
 }
 
-template <typename T, int N, bool ROW, bool ASYNC>
-cudaError_t run_power_k(CovGeom g, int want_blocks, int* blocks, cudaStream_t s) {
-  auto kern = k_axis_power<T, N, ROW, ASYNC>;
-  const size_t smem = cov_smem<T, N, ROW>() + (ASYNC ? (size_t)cov_in_floats<N, ROW>(g.n) * 4 : 0);
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when unavailable.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// The tensor map of a column layout's groups: the field as an L0 x L1 x L2
+// FP32 tensor, boxes of B x box rows along the line axis (x offsets of a
+// group are multiples of B >= 4 floats: 16-byte aligned).
+bool column_tmap(const CovGeom& g, const int L[3], int B, CUtensorMap* tm) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc || g.dir == 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)L[0], (cuuint64_t)L[1], (cuuint64_t)L[2]};
+  const cuuint64_t strides[2] = {(cuuint64_t)L[0] * 4, (cuuint64_t)L[0] * L[1] * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)B, (cuuint32_t)(g.dir == 1 ? g.box : 1),
+                             (cuuint32_t)(g.dir == 2 ? g.box : 1)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(g.f), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T, int N, bool ROW, bool ASYNC, bool TMA>
+cudaError_t run_power_k(CovGeom g, const CUtensorMap& tm, int want_blocks, int* blocks, cudaStream_t s) {
+  auto kern = k_axis_power<T, N, ROW, ASYNC, TMA>;
+  const size_t smem = ASYNC ? cov_smem_staged<T, N, ROW>(g) : cov_smem<T, N, ROW>();
   const int threads = cov_threads<T, N, ROW>();
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -279,41 +414,49 @@ cudaError_t run_power_k(CovGeom g, int want_blocks, int* blocks, cudaStream_t s)
     return cudaSuccess;
   }
   const int grid = want_blocks > 0 ? want_blocks : nb;
-  kern<<<grid, threads, smem, s>>>(g);
+  kern<<<grid, threads, smem, s>>>(g, tm);
   return cudaGetLastError();
 }
 
+// Form of a launch: staged where staged_ok and the field pointer is 16-byte
+// aligned, its copies by the TMA unit where the launch has a status word and
+// (column layouts) a tensor map; the blocks query (g.f == nullptr) sizes the
+// staged form, whose grid every form can run (the grid is only the stride
+// of the group loop).
 template <typename T, int N, bool ROW>
-cudaError_t run_power(CovGeom g, int L0, int want_blocks, int* blocks, cudaStream_t s) {
+cudaError_t run_power(CovGeom g, const int* L, int want_blocks, int* blocks, cudaStream_t s) {
+  CUtensorMap tm;
+  std::memset(&tm, 0, sizeof tm);
   if constexpr (sizeof(T) == 4) {
-    // the query (g.f == nullptr) and the launch pick the same form, so the
-    // partial sums sized from the query match the launch's grid
     const bool aligned = g.f == nullptr || (reinterpret_cast<uintptr_t>(g.f) & 15) == 0;
-    if (staged_ok<T, N, ROW>(g, L0) && aligned)
-      return run_power_k<T, N, ROW, true>(g, want_blocks, blocks, s);
+    if (staged_ok<T, N, ROW>(g, L[0]) && aligned) {
+      if (!blocks && g.status && (ROW || column_tmap(g, L, cov_B<T, N, ROW>(), &tm)))
+        return run_power_k<T, N, ROW, true, true>(g, tm, want_blocks, blocks, s);
+      return run_power_k<T, N, ROW, true, false>(g, tm, want_blocks, blocks, s);
+    }
   }
-  return run_power_k<T, N, ROW, false>(g, want_blocks, blocks, s);
+  return run_power_k<T, N, ROW, false, false>(g, tm, want_blocks, blocks, s);
 }
 
 template <typename T, bool ROW>
-cudaError_t run_power_n(int N, CovGeom g, int L0, int want_blocks, int* blocks, cudaStream_t s) {
+cudaError_t run_power_n(int N, CovGeom g, const int* L, int want_blocks, int* blocks, cudaStream_t s) {
   switch (N) {
-    case 4: return run_power<T, 4, ROW>(g, L0, want_blocks, blocks, s);
-    case 8: return run_power<T, 8, ROW>(g, L0, want_blocks, blocks, s);
-    case 16: return run_power<T, 16, ROW>(g, L0, want_blocks, blocks, s);
-    case 32: return run_power<T, 32, ROW>(g, L0, want_blocks, blocks, s);
-    case 64: return run_power<T, 64, ROW>(g, L0, want_blocks, blocks, s);
-    case 128: return run_power<T, 128, ROW>(g, L0, want_blocks, blocks, s);
-    case 256: return run_power<T, 256, ROW>(g, L0, want_blocks, blocks, s);
-    case 512: return run_power<T, 512, ROW>(g, L0, want_blocks, blocks, s);
-    case 1024: return run_power<T, 1024, ROW>(g, L0, want_blocks, blocks, s);
-    case 2048: return run_power<T, 2048, ROW>(g, L0, want_blocks, blocks, s);
-    case 320: return run_power<T, 320, ROW>(g, L0, want_blocks, blocks, s);
-    case 384: return run_power<T, 384, ROW>(g, L0, want_blocks, blocks, s);
-    case 640: return run_power<T, 640, ROW>(g, L0, want_blocks, blocks, s);
-    case 768: return run_power<T, 768, ROW>(g, L0, want_blocks, blocks, s);
-    case 1280: return run_power<T, 1280, ROW>(g, L0, want_blocks, blocks, s);
-    case 1536: return run_power<T, 1536, ROW>(g, L0, want_blocks, blocks, s);
+    case 4: return run_power<T, 4, ROW>(g, L, want_blocks, blocks, s);
+    case 8: return run_power<T, 8, ROW>(g, L, want_blocks, blocks, s);
+    case 16: return run_power<T, 16, ROW>(g, L, want_blocks, blocks, s);
+    case 32: return run_power<T, 32, ROW>(g, L, want_blocks, blocks, s);
+    case 64: return run_power<T, 64, ROW>(g, L, want_blocks, blocks, s);
+    case 128: return run_power<T, 128, ROW>(g, L, want_blocks, blocks, s);
+    case 256: return run_power<T, 256, ROW>(g, L, want_blocks, blocks, s);
+    case 512: return run_power<T, 512, ROW>(g, L, want_blocks, blocks, s);
+    case 1024: return run_power<T, 1024, ROW>(g, L, want_blocks, blocks, s);
+    case 2048: return run_power<T, 2048, ROW>(g, L, want_blocks, blocks, s);
+    case 320: return run_power<T, 320, ROW>(g, L, want_blocks, blocks, s);
+    case 384: return run_power<T, 384, ROW>(g, L, want_blocks, blocks, s);
+    case 640: return run_power<T, 640, ROW>(g, L, want_blocks, blocks, s);
+    case 768: return run_power<T, 768, ROW>(g, L, want_blocks, blocks, s);
+    case 1280: return run_power<T, 1280, ROW>(g, L, want_blocks, blocks, s);
+    case 1536: return run_power<T, 1536, ROW>(g, L, want_blocks, blocks, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -325,6 +468,9 @@ CovGeom geom(const void* f, const int L[3], int dir, double mu, const void* tw, 
   g.mu = mu;
   g.tw = tw;
   g.partial = partial;
+  g.status = nullptr;
+  g.dir = dir;
+  g.box = L[dir] < 256 ? L[dir] : 256;
   const int64_t L0 = L[0], L1 = L[1], L2 = L[2];
   if (dir == 0) {  // x lines, consecutive in memory
     g.na = L1; g.sa = L0; g.sb = L0 * L1; g.st = 1; g.nlines = L1 * L2;
@@ -336,11 +482,11 @@ CovGeom geom(const void* f, const int L[3], int dir, double mu, const void* tw, 
   return g;
 }
 
-cudaError_t dispatch(int dt, int dir, int N, CovGeom g, int L0, int want, int* blocks, cudaStream_t s) {
-  if (dt == 8) return dir == 0 ? run_power_n<double, true>(N, g, L0, want, blocks, s)
-                               : run_power_n<double, false>(N, g, L0, want, blocks, s);
-  return dir == 0 ? run_power_n<float, true>(N, g, L0, want, blocks, s)
-                  : run_power_n<float, false>(N, g, L0, want, blocks, s);
+cudaError_t dispatch(int dt, int dir, int N, CovGeom g, const int* L, int want, int* blocks, cudaStream_t s) {
+  if (dt == 8) return dir == 0 ? run_power_n<double, true>(N, g, L, want, blocks, s)
+                               : run_power_n<double, false>(N, g, L, want, blocks, s);
+  return dir == 0 ? run_power_n<float, true>(N, g, L, want, blocks, s)
+                  : run_power_n<float, false>(N, g, L, want, blocks, s);
 }
 
 // P_k = sum over blocks of the partial power (one thread per bin).
@@ -379,7 +525,7 @@ __global__ void k_cov_lags(const double* __restrict__ bins, int N, const double2
 int axis_power_blocks(int dt, const int L[3], int dir, int N) {
   int nb = -1;
   CovGeom g = geom(nullptr, L, dir, 0.0, nullptr, nullptr);
-  if (dispatch(dt, dir, N, g, L[0], -1, &nb, nullptr) != cudaSuccess) {
+  if (dispatch(dt, dir, N, g, L, -1, &nb, nullptr) != cudaSuccess) {
     cudaGetLastError();
     return -1;
   }
@@ -387,9 +533,10 @@ int axis_power_blocks(int dt, const int L[3], int dir, int N) {
 }
 
 cudaError_t launch_axis_power(int dt, const void* f, const int L[3], int dir, int N, double mu,
-                              const void* tw, double* partial, int nblocks, cudaStream_t s) {
+                              const void* tw, double* partial, int nblocks, cudaStream_t s, int* status) {
   CovGeom g = geom(f, L, dir, mu, tw, partial);
-  return dispatch(dt, dir, N, g, L[0], nblocks, nullptr, s);
+  g.status = status;
+  return dispatch(dt, dir, N, g, L, nblocks, nullptr, s);
 }
 
 cudaError_t launch_cov_lags(const double* partial, int nblocks, int N, int maxlag,

@@ -187,8 +187,11 @@ int lag_cov_parts(const int L[3], int dir);
 // zero-padded lines along axis dir (complex length N, padded length 2N),
 // then S(h) for h <= maxlag.  bins holds N + 1 doubles.
 int axis_power_blocks(int dt, const int L[3], int dir, int N);
+// status: the context's device status word (bit 0: a bounded copy wait of
+// the TMA form expired); null runs the forms without bulk copies.
 cudaError_t launch_axis_power(int dt, const void* f, const int L[3], int dir, int N, double mu,
-                              const void* tw, double* partial, int nblocks, cudaStream_t s);
+                              const void* tw, double* partial, int nblocks, cudaStream_t s,
+                              int* status = nullptr);
 cudaError_t launch_cov_lags(const double* partial, int nblocks, int N, int maxlag,
                             const double* tw64, double* bins, double* S, cudaStream_t s);
 
