@@ -490,6 +490,9 @@ def main():
     ap.add_argument("--profile-tile", action="store_true",
                     help="generate one field once (no timing) for profiler captures; launch "
                          "variants come from SCARL_TUNE_CACHE when set")
+    ap.add_argument("--split-x", action="store_true",
+                    help="with --profile-tile: pass 3's x DFT on the tensor cores too "
+                         "(SCARL_SPLIT_BF16_X)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -532,7 +535,8 @@ def main():
         sample, lay = layout_of(S)
         L = [int(v) for v in lay["L"]]
         field = torch.empty(L[0] * L[1] * L[2], dtype=torch.float32, device="cuda")
-        S.generate_sample(ctx, sample, generator=S.GEN_PADDED, dtype=S.F32 | S.SPLIT_BF16,
+        S.generate_sample(ctx, sample, generator=S.GEN_PADDED,
+                          dtype=S.F32 | (S.SPLIT_BF16_X if args.split_x else S.SPLIT_BF16),
                           nb_procs=8, topo=TOPO, pad_policy=S.PAD_SMOOTH, pad_tol=PAD_TOL, out=field)
         ctx.sync()
         print(json.dumps({"profile_tile": "ok", "launches": ctx.counters()["launches"]}))
