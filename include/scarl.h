@@ -394,7 +394,10 @@ int scarl_rebuild_sk(scarl_ctx* ctx, const void* field, int dtype, const int L[3
  * axis over the field.  No direct counterpart: rebuild_Sk_FFT
  * (statistics_RF.f90:258-462) windows and wraps each line; this is the
  * plain linear estimator a covariance model is checked against.  Needs
- * maxlag < L[d] and L[d] + maxlag <= 4096. */
+ * maxlag < L[d] and L[d] + maxlag <= 4096.  FP32 fields whose lines start on
+ * 16-byte boundaries stage their lines through TMA bulk copies with bounded
+ * waits: a wait that runs out returns SCARL_ETIMEOUT (the results are then
+ * invalid). */
 int scarl_axis_cov(scarl_ctx* ctx, const void* field, int dtype, const int L[3], int maxlag,
                    const double* known_mean, double* mean, double* var, double* cov);
 /* scarl_axis_cov with the field's sums already known: sums = (sum f,
